@@ -1,0 +1,477 @@
+// Linear FFT convolution on the B200: pruned 3D R2C / C2R FFTs with the OTF
+// product fused into the axial pass.
+//
+// Replaces deconlib's LinearFFTConvolver (deconvolution/linops_mlx.py:435-533)
+// and FFTConvolver (:384-432).  With signal N = (Nz, Ny, Nx) zero-padded to
+// the canvas F = (Fz, Fy, Fx), a convolution is five passes:
+//
+//   1. X R2C   N rows of x            -> S1[Nz][Ny][P]   (real FFT, length Fx)
+//   2. Y FFT   S1, Ny non-zero points -> S2[Nz][Fy][P]
+//   3. Z pass  S2 in place: FFT over Fz (Nz non-zero inputs), x OTF (or
+//              conj(OTF) for the adjoint), inverse FFT, keep the first Nz
+//   4. Y IFFT  S2 -> S1, keep the first Ny points
+//   5. X C2R   S1 -> out, keep x < Nx, scale 1/(Fz Fy Fx), fused epilogue
+//
+// Zero padding never exists in memory (the loads return zeros) and only the
+// Nz x Fy x (Fx/2+1) part of the spectrum that the crop can see is ever
+// formed ("pruned" FFT).  P is the spectrum row pitch: Fx/2 + 1 rounded up to
+// 16 complex values, so every 16-wide column tile of the strided passes
+// reads whole 128-byte lines.
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+#include <algorithm>
+
+#include "conv_impl.cuh"
+
+namespace dk {
+
+// ---------------------------------------------------------------------------
+// device value fetch for the X R2C prologue
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ bool kernel_src(int64_t c, int64_t F, int64_t m, int64_t npos,
+                                           int64_t& k) {
+    // Corner-origin embedding (utils/padding.py:142-190): canvas index c holds
+    // kernel index c (c < npos) or c - F + m (the wrapped negative offsets).
+    if (c < npos) {
+        k = c;
+        return c < m;
+    }
+    const int64_t nneg = m - npos;
+    if (c >= F - nneg) {
+        k = c - F + m;
+        return true;
+    }
+    return false;
+}
+
+struct RowSrc {
+    const float* p;  // row base (nullptr: row is outside the window)
+    bool ok;
+};
+
+template <int PRO>
+__device__ __forceinline__ RowSrc row_source(const XR2CArgs& a, int64_t z, int64_t y) {
+    RowSrc r{nullptr, false};
+    if constexpr (PRO == PRO_KERNEL) {
+        int64_t kz, ky;
+        if (kernel_src(z, a.Nz, a.Kz, a.pz, kz) && kernel_src(y, a.Ny, a.Ky, a.py, ky)) {
+            r.p = a.in + (kz * a.Ky + ky) * a.Kx;
+            r.ok = true;
+        }
+    } else {
+        const int64_t iz = z - a.win.oz, iy = y - a.win.oy;
+        if (iz >= 0 && iz < a.win.wz && iy >= 0 && iy < a.win.wy) {
+            r.ok = true;
+            if (a.in) r.p = a.in + (iz * a.win.wy + iy) * a.win.wx;
+        }
+    }
+    return r;
+}
+
+template <int PRO>
+__device__ __forceinline__ float fetch_x(const XR2CArgs& a, const RowSrc& r, int64_t x) {
+    if (!r.ok || x >= a.Nx) return 0.f;
+    if constexpr (PRO == PRO_KERNEL) {
+        int64_t kx;
+        if (!kernel_src(x, a.Nx, a.Kx, a.px, kx)) return 0.f;
+        return __ldg(r.p + kx) / a.kdiv;
+    } else {
+        const int64_t ix = x - a.win.ox;
+        if (ix < 0 || ix >= a.win.wx) return 0.f;
+        if constexpr (PRO == PRO_CONST) {
+            return a.cval;
+        } else if constexpr (PRO == PRO_RLINIT) {
+            return fmaxf(__ldg(r.p + ix) - a.bg, 1e-6f);
+        } else {
+            return __ldg(r.p + ix);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pass 1: X R2C
+// ---------------------------------------------------------------------------
+
+template <int PRO, int LS>
+__global__ void __launch_bounds__(kFftThreads) k_xr2c(XR2CArgs a) {
+    extern __shared__ float2 sm[];
+    const int T = a.T, L = a.ax.L, tid = threadIdx.x;
+    const int64_t row0 = (int64_t)blockIdx.x * T;
+    for (int q = tid; q < T * L; q += blockDim.x) {
+        const int t = q / L, n = q - t * L;
+        const int64_t row = row0 + t;
+        float2 v = make_float2(0.f, 0.f);
+        if (row < a.nrows) {
+            const int64_t z = row / a.Ny, y = row - z * a.Ny;
+            const RowSrc rs = row_source<PRO>(a, z, y);
+            if (a.odd) {
+                v.x = fetch_x<PRO>(a, rs, n);
+            } else {
+                v.x = fetch_x<PRO>(a, rs, 2 * (int64_t)n);
+                v.y = fetch_x<PRO>(a, rs, 2 * (int64_t)n + 1);
+            }
+        }
+        sm[phys(n, t, T)] = v;
+    }
+    __syncthreads();
+    fft_lines<-1, LS>(sm, T, tid % T, tid / T, a.ax);
+    const int H = a.Hx;
+    for (int q = tid; q < T * H; q += blockDim.x) {
+        const int t = q / H, k = q - t * H;
+        const int64_t row = row0 + t;
+        if (row >= a.nrows) continue;
+        float2 X;
+        if (a.odd) {
+            X = sm[phys(k, t, T)];
+        } else {
+            const int M = L;
+            const float2 zk = sm[phys(k == M ? 0 : k, t, T)];
+            const float2 zm = cconj(sm[phys(k == 0 ? 0 : M - k, t, T)]);
+            const float2 e = cscale(cadd(zk, zm), 0.5f);
+            const float2 o = rot90<-1>(cscale(csub(zk, zm), 0.5f));
+            X = cadd(e, cmul(__ldg(&a.twx[k]), o));
+        }
+        a.out[row * a.P + k] = X;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// passes 2-4: complex FFT along a strided axis over 16-wide column tiles
+// ---------------------------------------------------------------------------
+
+template <int LS>
+__global__ void __launch_bounds__(kFftThreads) k_colfft(ColArgs a) {
+    extern __shared__ float2 sm[];
+    const int T = a.T, L = a.ax.L, tid = threadIdx.x;
+    const int64_t o = blockIdx.x / a.ntiles;
+    const int64_t kx0 = (int64_t)(blockIdx.x - o * a.ntiles) * T;
+    const float2* src = a.src + o * a.src_os + kx0;
+    for (int q = tid; q < L * T; q += blockDim.x) {
+        const int j = q / T, t = q - j * T;
+        float2 v = make_float2(0.f, 0.f);
+        if (j < a.nin && kx0 + t < a.ncols) v = src[(int64_t)j * a.src_js + t];
+        sm[phys(j, t, T)] = v;
+    }
+    __syncthreads();
+    const int t = tid % T, jb = tid / T;
+    if (a.mode == COL_INV) {
+        fft_lines<+1, LS>(sm, T, t, jb, a.ax);
+    } else {
+        fft_lines<-1, LS>(sm, T, t, jb, a.ax);
+    }
+    if (a.mode == COL_OTF || a.mode == COL_OTF_CONJ) {
+        const float2* otf = a.otf + o * a.otf_os + kx0;
+        for (int q = tid; q < L * T; q += blockDim.x) {
+            const int j = q / T, tt = q - j * T;
+            if (kx0 + tt < a.ncols) {
+                const float2 w = __ldg(&otf[(int64_t)j * a.otf_js + tt]);
+                const int p = phys(j, tt, T);
+                sm[p] = a.mode == COL_OTF ? cmul(sm[p], w) : cmulc(sm[p], w);
+            }
+        }
+        __syncthreads();
+        fft_lines<+1, LS>(sm, T, t, jb, a.ax);
+    }
+    float2* dst = a.dst + o * a.dst_os + kx0;
+    for (int q = tid; q < a.nout * T; q += blockDim.x) {
+        const int j = q / T, tt = q - j * T;
+        if (kx0 + tt < a.ncols) dst[(int64_t)j * a.dst_js + tt] = sm[phys(j, tt, T)];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pass 5: X C2R with fused epilogues
+// ---------------------------------------------------------------------------
+
+template <int EPI, int LS>
+__global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
+    extern __shared__ float2 sm[];
+    const int T = a.T, L = a.ax.L, tid = threadIdx.x;
+    const int64_t row0 = (int64_t)blockIdx.x * T;
+    for (int q = tid; q < T * L; q += blockDim.x) {
+        const int t = q / L, k = q - t * L;
+        const int64_t row = row0 + t;
+        float2 Z = make_float2(0.f, 0.f);
+        if (row < a.nrows) {
+            const float2* rp = a.in + row * a.P;
+            if (a.odd) {
+                // Full Hermitian spectrum from the half: X[k] = conj(X[Fx - k]).
+                Z = k < a.Hx ? rp[k] : cconj(rp[L - k]);
+                if (k == 0) Z.y = 0.f;
+            } else {
+                const int M = L;
+                float2 xk = rp[k];
+                float2 xm = rp[M - k];
+                if (k == 0) {  // irfft ignores Im of the DC and Nyquist bins
+                    xk.y = 0.f;
+                    xm.y = 0.f;
+                }
+                xm = cconj(xm);
+                const float2 e = cadd(xk, xm);
+                const float2 od = cmulc(csub(xk, xm), __ldg(&a.twx[k]));
+                Z = cadd(e, rot90<+1>(od));
+            }
+        }
+        sm[phys(k, t, T)] = Z;
+    }
+    __syncthreads();
+    fft_lines<+1, LS>(sm, T, tid % T, tid / T, a.ax);
+
+    double acc = 0.0;
+    const int64_t Nx = a.Nx;
+    for (int64_t q = tid; q < (int64_t)T * Nx; q += blockDim.x) {
+        const int t = (int)(q / Nx);
+        const int64_t x = q - (int64_t)t * Nx;
+        const int64_t row = row0 + t;
+        if (row >= a.nrows) continue;
+        const int64_t z = row / a.Ny, y = row - z * a.Ny;
+        const int64_t iz = z - a.win.oz, iy = y - a.win.oy, ix = x - a.win.ox;
+        if (iz < 0 || iz >= a.win.wz || iy < 0 || iy >= a.win.wy || ix < 0 || ix >= a.win.wx)
+            continue;
+        float v;
+        if (a.odd) {
+            v = sm[phys((int)x, t, T)].x;
+        } else {
+            const float2 c = sm[phys((int)(x >> 1), t, T)];
+            v = (x & 1) ? c.y : c.x;
+        }
+        v *= a.scale;
+        const int64_t i = (iz * a.win.wy + iy) * a.win.wx + ix;
+        if constexpr (EPI == EPI_STORE) {
+            a.out[i] = v;
+        } else if constexpr (EPI == EPI_RL_RATIO || EPI == EPI_PRED) {
+            // rl_mlx.py:147-148  model = A x + b ; ratio = y / max(model, 1e-10)
+            const float m = v + a.bg;
+            const float yv = __ldg(a.aux0 + i);
+            if constexpr (EPI == EPI_RL_RATIO) {
+                a.out[i] = yv / fmaxf(m, 1e-10f);
+            } else {
+                a.out[i] = m;
+            }
+            if (a.partials) {
+                // rl_mlx.py:75-79: y log(max(y,eps)/max(m,eps)) - (y - max(m,eps))
+                const float ys = fmaxf(yv, 1e-6f), ms = fmaxf(m, 1e-6f);
+                acc += (double)(yv * logf(ys / ms) - (yv - ms));
+            }
+        } else if constexpr (EPI == EPI_RL_UPDATE) {
+            // rl_mlx.py:149-150  x = max(x * where(active, A^T ratio / sens, 0), 1e-10)
+            const float s = __ldg(a.aux1 + i);
+            const float c = s > 0.f ? v / s : 0.f;
+            a.out[i] = fmaxf(a.aux0[i] * c, 1e-10f);
+        }
+    }
+    if constexpr (EPI == EPI_RL_RATIO || EPI == EPI_PRED) {
+        if (a.partials) {
+            const double s = block_sum(acc);
+            if (tid == 0) a.partials[blockIdx.x] = s;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host: axis planning and launches
+// ---------------------------------------------------------------------------
+
+bool plan_axis(int L, Axis& ax) {
+    ax = Axis{};
+    ax.L = L;
+    int n = L, e2 = 0;
+    while (n % 2 == 0) {
+        n /= 2;
+        ++e2;
+    }
+    std::vector<int> r;
+    int n8 = e2 / 3, rem = e2 % 3;
+    if (rem == 1 && n8 > 0) {
+        --n8;
+        r.push_back(4);
+        r.push_back(4);
+    } else if (rem == 1) {
+        r.push_back(2);
+    } else if (rem == 2) {
+        r.push_back(4);
+    }
+    for (int i = 0; i < n8; ++i) r.insert(r.begin(), 8);
+    for (int p : {5, 3, 7}) {
+        while (n % p == 0) {
+            n /= p;
+            r.push_back(p);
+        }
+    }
+    if (n != 1 || (int)r.size() > kMaxStages) return false;
+    ax.nst = (int)r.size();
+    for (int i = 0; i < ax.nst; ++i) ax.rad |= (unsigned long long)r[i] << (4 * i);
+    ax.tpl = (L + 31) / 32;
+    return true;
+}
+
+static int threads_for(int T, const Axis& ax) {
+    int n = T * ax.tpl;
+    n = (int)round_up(n, 32);
+    return std::max(n, 64);
+}
+
+// Kernel selection: one instantiation per static length (0 = runtime radices).
+template <int PRO, int LS>
+static void* xr2c_ptr() { return (void*)k_xr2c<PRO, LS>; }
+template <int EPI, int LS>
+static void* xc2r_ptr() { return (void*)k_xc2r<EPI, LS>; }
+
+template <int PRO>
+static void* pick_xr2c(int L) {
+#define DK_CASE(n) if (L == n) return xr2c_ptr<PRO, n>();
+    DK_STATIC_LENGTHS(DK_CASE)
+#undef DK_CASE
+    return xr2c_ptr<PRO, 0>();
+}
+template <int EPI>
+static void* pick_xc2r(int L) {
+#define DK_CASE(n) if (L == n) return xc2r_ptr<EPI, n>();
+    DK_STATIC_LENGTHS(DK_CASE)
+#undef DK_CASE
+    return xc2r_ptr<EPI, 0>();
+}
+static void* pick_col(int L) {
+#define DK_CASE(n) if (L == n) return (void*)k_colfft<n>;
+    DK_STATIC_LENGTHS(DK_CASE)
+#undef DK_CASE
+    return (void*)k_colfft<0>;
+}
+
+static int launch(void* fn, int64_t nblk, int nthr, size_t smem, cudaStream_t st, void* args) {
+    if (smem > 48 * 1024) {
+        // idempotent; cheap compared with the launch
+        DK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    if (nblk <= 0) return DECON_OK;
+    if (nblk > 0x7fffffffLL) return fail(DECON_ERR_UNSUPPORTED, "grid too large");
+    void* params[] = {args};
+    DK_CUDA(cudaLaunchKernel(fn, dim3((unsigned)nblk), dim3(nthr), params, smem, st));
+    return DECON_OK;
+}
+
+int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cval, float bg,
+                int64_t nz_rows, float2* out, cudaStream_t st) {
+    XR2CArgs a{};
+    a.in = in;
+    a.cval = cval;
+    a.bg = bg;
+    a.Nz = nz_rows;
+    a.Ny = pro == PRO_KERNEL ? p.F[1] : p.N[1];
+    a.Nx = pro == PRO_KERNEL ? p.F[2] : p.N[2];
+    a.win = win;
+    a.Kz = p.K[0];
+    a.Ky = p.K[1];
+    a.Kx = p.K[2];
+    a.pz = (p.K[0] + 1) / 2;
+    a.py = (p.K[1] + 1) / 2;
+    a.px = (p.K[2] + 1) / 2;
+    a.kdiv = p.kdiv;
+    a.out = out;
+    a.P = p.P;
+    a.Hx = (int)p.Hx;
+    a.odd = p.odd;
+    a.ax = p.ax_x;
+    a.twx = p.twx;
+    a.T = p.T_x;
+    a.nrows = nz_rows * a.Ny;
+    const int nthr = threads_for(a.T, a.ax);
+    const int64_t nblk = cdiv(a.nrows, a.T);
+    const size_t smem = (size_t)a.T * a.ax.L * sizeof(float2);
+    void* fn = nullptr;
+    switch (pro) {
+        case PRO_ARRAY: fn = pick_xr2c<PRO_ARRAY>(a.ax.L); break;
+        case PRO_CONST: fn = pick_xr2c<PRO_CONST>(a.ax.L); break;
+        case PRO_KERNEL: fn = pick_xr2c<PRO_KERNEL>(a.ax.L); break;
+        case PRO_RLINIT: fn = pick_xr2c<PRO_RLINIT>(a.ax.L); break;
+        default: return fail(DECON_ERR_VALUE, "bad prologue %d", pro);
+    }
+    return launch(fn, nblk, nthr, smem, st, &a);
+}
+
+int launch_col(const ConvPlan& p, const Axis& ax, int T, int mode, const float2* src,
+               int64_t src_os, int64_t src_js, int nin, float2* dst, int64_t dst_os,
+               int64_t dst_js, int nout, int64_t nouter, cudaStream_t st) {
+    ColArgs a{};
+    a.src = src;
+    a.dst = dst;
+    a.src_os = src_os;
+    a.src_js = src_js;
+    a.dst_os = dst_os;
+    a.dst_js = dst_js;
+    a.nin = nin;
+    a.nout = nout;
+    a.ncols = (int)p.Hx;
+    a.T = T;
+    a.ax = ax;
+    a.mode = mode;
+    a.otf = p.otf;
+    a.otf_js = p.F[1] * p.P;
+    a.otf_os = p.P;
+    a.ntiles = (int)cdiv(p.Hx, T);
+    const int nthr = threads_for(T, ax);
+    const int64_t nblk = nouter * a.ntiles;
+    const size_t smem = (size_t)T * ax.L * sizeof(float2);
+    return launch(pick_col(ax.L), nblk, nthr, smem, st, &a);
+}
+
+int launch_xc2r(const ConvPlan& p, int epi, const float2* in, Win3 win, float* out,
+                const float* aux0, const float* aux1, float bg, double* partials, int* nblk_out,
+                cudaStream_t st) {
+    XC2RArgs a{};
+    a.in = in;
+    a.P = p.P;
+    a.Ny = p.N[1];
+    a.Nx = p.N[2];
+    a.nrows = p.N[0] * p.N[1];
+    a.Hx = (int)p.Hx;
+    a.odd = p.odd;
+    a.ax = p.ax_x;
+    a.twx = p.twx;
+    a.T = p.T_x;
+    a.scale = (float)(1.0 / ((double)p.F[0] * (double)p.F[1] * (double)p.F[2]));
+    a.win = win;
+    a.out = out;
+    a.aux0 = aux0;
+    a.aux1 = aux1;
+    a.bg = bg;
+    a.partials = partials;
+    const int nthr = threads_for(a.T, a.ax);
+    const int64_t nblk = cdiv(a.nrows, a.T);
+    if (nblk_out) *nblk_out = (int)nblk;
+    const size_t smem = (size_t)a.T * a.ax.L * sizeof(float2);
+    void* fn = nullptr;
+    switch (epi) {
+        case EPI_STORE: fn = pick_xc2r<EPI_STORE>(a.ax.L); break;
+        case EPI_RL_RATIO: fn = pick_xc2r<EPI_RL_RATIO>(a.ax.L); break;
+        case EPI_RL_UPDATE: fn = pick_xc2r<EPI_RL_UPDATE>(a.ax.L); break;
+        case EPI_PRED: fn = pick_xc2r<EPI_PRED>(a.ax.L); break;
+        default: return fail(DECON_ERR_VALUE, "bad epilogue %d", epi);
+    }
+    return launch(fn, nblk, nthr, smem, st, &a);
+}
+
+// Forward spectrum: x (window in N-space) -> S2 (after the Y pass).
+int spectrum_forward(const ConvPlan& p, int pro, const float* in, Win3 win, float cval, float bg,
+                     cudaStream_t st) {
+    const int64_t Nz = p.N[0], Ny = p.N[1], Fy = p.F[1], P = p.P;
+    DK_TRY(launch_xr2c(p, pro, in, win, cval, bg, Nz, p.s1, st));
+    DK_TRY(launch_col(p, p.ax_y, p.T_y, COL_FWD, p.s1, Ny * P, P, (int)Ny, p.s2, Fy * P, P,
+                      (int)Fy, Nz, st));
+    return DECON_OK;
+}
+
+// Z pass (x OTF or conj OTF) and the inverse Y pass: S2 -> S1.
+int spectrum_filter_back(const ConvPlan& p, bool adjoint, cudaStream_t st) {
+    const int64_t Nz = p.N[0], Ny = p.N[1], Fy = p.F[1], P = p.P;
+    DK_TRY(launch_col(p, p.ax_z, p.T_z, adjoint ? COL_OTF_CONJ : COL_OTF, p.s2, P, Fy * P,
+                      (int)Nz, p.s2, P, Fy * P, (int)Nz, Fy, st));
+    DK_TRY(launch_col(p, p.ax_y, p.T_y, COL_INV, p.s2, Fy * P, P, (int)Fy, p.s1, Ny * P, P,
+                      (int)Ny, Nz, st));
+    return DECON_OK;
+}
+
+}  // namespace dk

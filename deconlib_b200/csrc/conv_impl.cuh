@@ -1,0 +1,103 @@
+// Internal declarations of the convolution passes (conv.cu) shared with the
+// C ABI (capi.cu) and the solver kernels.
+#pragma once
+
+#include "common.cuh"
+#include "fft_engine.cuh"
+
+namespace dk {
+
+constexpr int kSmemElems = 8192;  // complex values per CTA (64 KB)
+// T lines x L points <= kSmemElems and ceil(L/32) threads per line bound a
+// CTA to kSmemElems / 32 threads.
+constexpr int kFftThreads = kSmemElems / 32;
+
+// A float32 array of shape (wz, wy, wx) placed at offset (oz, oy, ox) inside
+// the N-space volume; voxels outside the box read as zero / are not written.
+struct Win3 {
+    int64_t wz, wy, wx;
+    int64_t oz, oy, ox;
+};
+
+inline Win3 full_window(const int64_t* N) { return Win3{N[0], N[1], N[2], 0, 0, 0}; }
+
+enum Prologue { PRO_ARRAY = 0, PRO_CONST = 1, PRO_KERNEL = 2, PRO_RLINIT = 3 };
+enum Epilogue { EPI_STORE = 0, EPI_RL_RATIO = 1, EPI_RL_UPDATE = 2, EPI_PRED = 3 };
+enum ColMode { COL_FWD = 0, COL_INV = 1, COL_OTF = 2, COL_OTF_CONJ = 3 };
+
+struct XR2CArgs {
+    const float* in;
+    float cval, bg, kdiv;
+    int64_t Nz, Ny, Nx;  // rows = Nz * Ny, row length Nx (zero-padded to Fx)
+    Win3 win;
+    int64_t Kz, Ky, Kx, pz, py, px;  // kernel embedding (PRO_KERNEL)
+    float2* out;
+    int64_t P, nrows;
+    int Hx, odd, T;
+    Axis ax;            // length Fx/2 (even Fx) or Fx (odd)
+    const float2* twx;  // W_Fx table
+};
+
+struct ColArgs {
+    const float2* src;
+    float2* dst;
+    int64_t src_os, src_js, dst_os, dst_js;
+    int nin, nout, ncols, T, mode, ntiles;
+    Axis ax;
+    const float2* otf;
+    int64_t otf_js, otf_os;
+};
+
+struct XC2RArgs {
+    const float2* in;
+    int64_t P, Ny, Nx, nrows;
+    int Hx, odd, T;
+    Axis ax;
+    const float2* twx;
+    float scale;
+    Win3 win;
+    float* out;
+    const float* aux0;
+    const float* aux1;
+    float bg;
+    double* partials;
+};
+
+// Device-resident state of one LinearFFTConvolver.
+struct ConvPlan {
+    int64_t N[3], F[3], K[3];
+    int64_t Hx, P;
+    int odd;
+    Axis ax_x, ax_y, ax_z;
+    int T_x, T_y, T_z;
+    float2 *otf, *s1, *s2;
+    float2 *twx, *twy, *twz;
+    double* dscal;        // device scalars (kernel sum, reductions)
+    double* partials;     // per-CTA FP64 partial sums of fused reductions
+    int64_t npartials;
+    float kdiv;
+    double norm_sq;
+    int device;
+};
+
+int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cval, float bg,
+                int64_t nz_rows, float2* out, cudaStream_t st);
+int launch_col(const ConvPlan& p, const Axis& ax, int T, int mode, const float2* src,
+               int64_t src_os, int64_t src_js, int nin, float2* dst, int64_t dst_os,
+               int64_t dst_js, int nout, int64_t nouter, cudaStream_t st);
+int launch_xc2r(const ConvPlan& p, int epi, const float2* in, Win3 win, float* out,
+                const float* aux0, const float* aux1, float bg, double* partials, int* nblk_out,
+                cudaStream_t st);
+int spectrum_forward(const ConvPlan& p, int pro, const float* in, Win3 win, float cval, float bg,
+                     cudaStream_t st);
+int spectrum_filter_back(const ConvPlan& p, bool adjoint, cudaStream_t st);
+
+// FP64 reductions (reduce.cu)
+int reduce_f32(const float* a, const float* b, int64_t n, int op, double* out, double* partials,
+               int64_t npartials, cudaStream_t st);
+int finish_partials(const double* partials, int n, double* out, cudaStream_t st);
+int64_t reduce_partials_needed();
+
+}  // namespace dk
+
+struct decon_conv : dk::ConvPlan {};

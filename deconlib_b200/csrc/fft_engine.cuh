@@ -1,0 +1,257 @@
+// Shared-memory Stockham FFT engine for batches of lines.
+//
+// A CTA holds T lines of L complex points in shared memory, element (j, t)
+// (point j of line t) at phys(j, t) = j*T + (t ^ (j & (T-1))).  The XOR
+// swizzle keeps both access patterns conflict-free: consecutive lines at one
+// point (the butterflies and the strided-axis loads) and consecutive points
+// of one line (the contiguous-axis loads).  T is a power of two.
+//
+// Each radix-R stage of the self-sorting (Stockham) algorithm reads point
+// j + r*L/R, multiplies by the twiddle W_{Ns R}^{r (j mod Ns)}, applies a
+// radix-R DFT and writes point (j div Ns) Ns R + (j mod Ns) + r Ns.  Every
+// thread owns at most ceil(32/R) butterflies per stage, so it holds <= 35
+// complex values in registers; a stage is read-all / barrier / write-all / barrier,
+// which lets the transform run in place.  Threads per line: ceil(L / 32).
+//
+// Twiddles come from a table of exp(-2 pi i m / Lt) computed on the host in
+// double precision (W_L^m = tw[m * tws]); no sin/cos is evaluated on the GPU.
+// Radices 2, 3, 4, 5, 7 and 8 are implemented.
+#pragma once
+
+#include "common.cuh"
+
+namespace dk {
+
+constexpr int kMaxStages = 16;
+
+struct Axis {
+    int L;                  // complex points per line
+    int nst;                // radix stages
+    unsigned long long rad; // radix of stage s in bits [4s, 4s+4), product == L
+    int tpl;                // threads per line = ceil(L / 32)
+    int tws;                // table stride: W_L^m = tw[m * tws]
+    const float2* tw;       // twiddle table (device)
+    __host__ __device__ int radix(int s) const { return (int)((rad >> (4 * s)) & 15ull); }
+};
+
+__device__ __forceinline__ int phys(int j, int t, int T) { return j * T + (t ^ (j & (T - 1))); }
+
+// multiply by -i (DIR < 0, forward) or +i (DIR > 0, inverse)
+template <int DIR>
+__device__ __forceinline__ float2 rot90(float2 a) {
+    return DIR < 0 ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft2(float2& a, float2& b) {
+    float2 t = a;
+    a = cadd(t, b);
+    b = csub(t, b);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft4(float2* v) {
+    float2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    float2 t2 = cadd(v[1], v[3]), t3 = rot90<DIR>(csub(v[1], v[3]));
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft8(float2* v) {
+    constexpr float h = 0.7071067811865476f;  // sqrt(1/2)
+    float2 e[4] = {v[0], v[2], v[4], v[6]};
+    float2 o[4] = {v[1], v[3], v[5], v[7]};
+    dft4<DIR>(e);
+    dft4<DIR>(o);
+    // W8^1 = h (1 -+ i), W8^2 = -+ i, W8^3 = h (-1 -+ i)
+    float2 o1 = DIR < 0 ? make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x))
+                        : make_float2(h * (o[1].x - o[1].y), h * (o[1].y + o[1].x));
+    float2 o2 = rot90<DIR>(o[2]);
+    float2 o3 = DIR < 0 ? make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y))
+                        : make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y));
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], o1);
+    v[5] = csub(e[1], o1);
+    v[2] = cadd(e[2], o2);
+    v[6] = csub(e[2], o2);
+    v[3] = cadd(e[3], o3);
+    v[7] = csub(e[3], o3);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft3(float2* v) {
+    constexpr float s3 = 0.8660254037844386f;  // sin(2 pi / 3)
+    float2 s = cadd(v[1], v[2]);
+    float2 d = csub(v[1], v[2]);
+    float2 m = make_float2(v[0].x - 0.5f * s.x, v[0].y - 0.5f * s.y);
+    float2 r = rot90<DIR>(cscale(d, s3));
+    v[0] = cadd(v[0], s);
+    v[1] = cadd(m, r);
+    v[2] = csub(m, r);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft5(float2* v) {
+    constexpr float c1 = 0.30901699437494745f, c2 = -0.8090169943749473f;
+    constexpr float s1 = 0.9510565162951535f, s2 = 0.5877852522924732f;
+    float2 b1 = cadd(v[1], v[4]), b2 = cadd(v[2], v[3]);
+    float2 d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
+    float2 t1 = make_float2(v[0].x + c1 * b1.x + c2 * b2.x, v[0].y + c1 * b1.y + c2 * b2.y);
+    float2 t2 = make_float2(v[0].x + c2 * b1.x + c1 * b2.x, v[0].y + c2 * b1.y + c1 * b2.y);
+    float2 u1 = rot90<DIR>(make_float2(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y));
+    float2 u2 = rot90<DIR>(make_float2(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y));
+    v[0] = cadd(v[0], cadd(b1, b2));
+    v[1] = cadd(t1, u1);
+    v[4] = csub(t1, u1);
+    v[2] = cadd(t2, u2);
+    v[3] = csub(t2, u2);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft7(float2* v) {
+    // cos / sin (2 pi j / 7), j = 1..3
+    constexpr float C1 = 0.6234898018587336f, C2 = -0.22252093395631434f, C3 = -0.900968867902419f;
+    constexpr float S1 = 0.7818314824680298f, S2 = 0.9749279121818236f, S3 = 0.43388373911755823f;
+    float2 b1 = cadd(v[1], v[6]), b2 = cadd(v[2], v[5]), b3 = cadd(v[3], v[4]);
+    float2 d1 = csub(v[1], v[6]), d2 = csub(v[2], v[5]), d3 = csub(v[3], v[4]);
+    const float2 a0 = v[0];
+    // m = 1: cos(1,2,3) sin(1,2,3); m = 2: cos(2,4,6)=(C2,C3,C1) sin(2,4,6)=(S2,-S3,-S1)
+    // m = 3: cos(3,6,9)=(C3,C1,C2) sin(3,6,9)=(S3,-S1,S2)
+    float2 t1 = make_float2(a0.x + C1 * b1.x + C2 * b2.x + C3 * b3.x,
+                            a0.y + C1 * b1.y + C2 * b2.y + C3 * b3.y);
+    float2 t2 = make_float2(a0.x + C2 * b1.x + C3 * b2.x + C1 * b3.x,
+                            a0.y + C2 * b1.y + C3 * b2.y + C1 * b3.y);
+    float2 t3 = make_float2(a0.x + C3 * b1.x + C1 * b2.x + C2 * b3.x,
+                            a0.y + C3 * b1.y + C1 * b2.y + C2 * b3.y);
+    float2 u1 = rot90<DIR>(make_float2(S1 * d1.x + S2 * d2.x + S3 * d3.x,
+                                       S1 * d1.y + S2 * d2.y + S3 * d3.y));
+    float2 u2 = rot90<DIR>(make_float2(S2 * d1.x - S3 * d2.x - S1 * d3.x,
+                                       S2 * d1.y - S3 * d2.y - S1 * d3.y));
+    float2 u3 = rot90<DIR>(make_float2(S3 * d1.x - S1 * d2.x + S2 * d3.x,
+                                       S3 * d1.y - S1 * d2.y + S2 * d3.y));
+    v[0] = cadd(a0, cadd(b1, cadd(b2, b3)));
+    v[1] = cadd(t1, u1);
+    v[6] = csub(t1, u1);
+    v[2] = cadd(t2, u2);
+    v[5] = csub(t2, u2);
+    v[3] = cadd(t3, u3);
+    v[4] = csub(t3, u3);
+}
+
+template <int R, int DIR>
+__device__ __forceinline__ void dft(float2* v) {
+    if constexpr (R == 2) dft2<DIR>(v[0], v[1]);
+    else if constexpr (R == 3) dft3<DIR>(v);
+    else if constexpr (R == 4) dft4<DIR>(v);
+    else if constexpr (R == 5) dft5<DIR>(v);
+    else if constexpr (R == 7) dft7<DIR>(v);
+    else if constexpr (R == 8) dft8<DIR>(v);
+}
+
+// One Stockham stage.  (t, jb): this thread's line and first butterfly.
+template <int R, int DIR, int NS_STATIC>
+__device__ __forceinline__ void stage_body(float2* buf, int T, int L, int Ns_dyn, int t, int jb,
+                                           int tpl, const float2* __restrict__ tw, int tws) {
+    // ceil(32 / R) butterflies per thread cover L / R butterflies with
+    // ceil(L / 32) threads per line for every radix (<= 35 values held).
+    constexpr int K = (32 + R - 1) / R;
+    const int Ns = NS_STATIC > 0 ? NS_STATIC : Ns_dyn;
+    const int nb = L / R;
+    const int step = L / (Ns * R);  // twiddle index step in units of W_L
+    float2 v[K][R];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int j = jb + k * tpl;
+        if (jb < tpl && j < nb) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[k][r] = buf[phys(j + r * nb, t, T)];
+            if (Ns > 1) {
+                const int kk = j % Ns;
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    const float2 w = __ldg(&tw[(r * kk * step) * tws]);
+                    v[k][r] = DIR < 0 ? cmul(v[k][r], w) : cmulc(v[k][r], w);
+                }
+            }
+            dft<R, DIR>(v[k]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int j = jb + k * tpl;
+        if (jb < tpl && j < nb) {
+            const int base = (j / Ns) * Ns * R + (j % Ns);
+#pragma unroll
+            for (int r = 0; r < R; ++r) buf[phys(base + r * Ns, t, T)] = v[k][r];
+        }
+    }
+    __syncthreads();
+}
+
+// Runtime-dispatched stage for arbitrary 7-smooth lengths.  Not inlined, so
+// each radix keeps its own register allocation.
+template <int R, int DIR>
+__device__ __noinline__ void fft_stage_dyn(float2* buf, int T, int L, int Ns, int t, int jb,
+                                           int tpl, const float2* tw, int tws) {
+    stage_body<R, DIR, 0>(buf, T, L, Ns, t, jb, tpl, tw, tws);
+}
+
+template <int DIR>
+__device__ __forceinline__ void fft_lines_dyn(float2* buf, int T, int t, int jb, const Axis ax) {
+    int Ns = 1;
+    for (int s = 0; s < ax.nst; ++s) {
+        const int R = ax.radix(s);
+        switch (R) {
+            case 8: fft_stage_dyn<8, DIR>(buf, T, ax.L, Ns, t, jb, ax.tpl, ax.tw, ax.tws); break;
+            case 4: fft_stage_dyn<4, DIR>(buf, T, ax.L, Ns, t, jb, ax.tpl, ax.tw, ax.tws); break;
+            case 2: fft_stage_dyn<2, DIR>(buf, T, ax.L, Ns, t, jb, ax.tpl, ax.tw, ax.tws); break;
+            case 3: fft_stage_dyn<3, DIR>(buf, T, ax.L, Ns, t, jb, ax.tpl, ax.tw, ax.tws); break;
+            case 5: fft_stage_dyn<5, DIR>(buf, T, ax.L, Ns, t, jb, ax.tpl, ax.tw, ax.tws); break;
+            case 7: fft_stage_dyn<7, DIR>(buf, T, ax.L, Ns, t, jb, ax.tpl, ax.tw, ax.tws); break;
+            default: break;
+        }
+        Ns *= R;
+    }
+}
+
+// Power-of-two lengths with the radix sequence fixed at compile time
+// (8, 8, ..., then 4 / 4,4 / 2): straight-line stages, shifts for j div Ns.
+// Matches plan_axis() so both paths use the same radices and twiddles.
+constexpr int pow2_radix(int rem) { return rem == 2 ? 2 : (rem == 4 || rem == 16) ? 4 : 8; }
+
+template <int L, int DIR, int NS>
+__device__ __forceinline__ void fft_lines_pow2(float2* buf, int T, int t, int jb,
+                                               const float2* __restrict__ tw, int tws) {
+    if constexpr (NS < L) {
+        constexpr int R = pow2_radix(L / NS);
+        stage_body<R, DIR, NS>(buf, T, L, NS, t, jb, (L + 31) / 32, tw, tws);
+        fft_lines_pow2<L, DIR, NS * R>(buf, T, t, jb, tw, tws);
+    }
+}
+
+// Full transform of the T lines held in buf.  DIR = -1 forward
+// (exp(-2 pi i ...)), +1 inverse, both unnormalised.  All threads of the CTA
+// must call it (it contains barriers).  t = tid % T, jb = tid / T.
+// LS > 0 selects the compile-time path for length LS (== ax.L).
+template <int DIR, int LS>
+__device__ __forceinline__ void fft_lines(float2* buf, int T, int t, int jb, const Axis ax) {
+    if constexpr (LS > 0) {
+        fft_lines_pow2<LS, DIR, 1>(buf, T, t, jb, ax.tw, ax.tws);
+    } else {
+        fft_lines_dyn<DIR>(buf, T, t, jb, ax);
+    }
+}
+
+// Lengths with a compile-time path; others use the runtime radix switch.
+#define DK_STATIC_LENGTHS(X) X(64) X(128) X(256) X(512) X(1024)
+
+// Host: factor L into supported radices (8s first, then 4/2, 5, 3, 7).
+// Returns false if L has a prime factor other than 2, 3, 5, 7.
+bool plan_axis(int L, Axis& ax);
+
+}  // namespace dk

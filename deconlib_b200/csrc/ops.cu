@@ -1,0 +1,347 @@
+// Pad / crop, fractional-area resampling and finite-difference operators.
+//
+//   decon_window_copy      Pad and Crop, forward and adjoint (core_operators.py:29-137)
+//   decon_band_weights     _banded_overlap_weights_1d (core_operators.py:151-202)
+//   decon_banded_axis      _apply_banded_1d (core_operators.py:205-219)
+//   decon_hessian3d_*      Hessian3D (linops_mlx.py:182-262, linops_core_mlx.py:42-80)
+//   decon_gradient3d_*     Gradient3D (linops_mlx.py:92-122, linops_core_mlx.py:25-39)
+//
+// The stencils evaluate each difference in the same float32 operation order
+// as the reference so results agree to the last few ulps.
+#include <cmath>
+#include <vector>
+
+#include "conv_impl.cuh"
+
+namespace dk {
+
+static int grid1d(int64_t n, int threads) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, threads), (int64_t)sm_count() * 32));
+}
+
+struct Box4 {
+    int64_t ss[4], s0[4], ds[4], d0[4], ext[4];
+};
+
+__global__ void k_window_copy(const float* __restrict__ src, float* __restrict__ dst, Box4 b,
+                              int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = i, c[4];
+#pragma unroll
+        for (int d = 3; d >= 0; --d) {
+            c[d] = r % b.ds[d];
+            r /= b.ds[d];
+        }
+        bool in = true;
+        int64_t si = 0;
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            const int64_t k = c[d] - b.d0[d];
+            in = in && k >= 0 && k < b.ext[d];
+            si = si * b.ss[d] + (b.s0[d] + k);
+        }
+        dst[i] = in ? __ldg(src + si) : 0.f;
+    }
+}
+
+__global__ void k_banded(const float* __restrict__ in, float* __restrict__ out, int64_t outer,
+                         int64_t n_in, int64_t inner, int64_t n_out, const int32_t* __restrict__ idx,
+                         const float* __restrict__ w, int width) {
+    const int64_t n = outer * n_out * inner;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = i % inner;
+        const int64_t t = i / inner;
+        const int64_t o = t / n_out, j = t - o * n_out;
+        const float* base = in + o * n_in * inner + q;
+        float acc = 0.f;
+        // sum over the window in index order, as mx.sum(gathered * weight, -1)
+        for (int k = 0; k < width; ++k) {
+            const int64_t s = __ldg(idx + j * width + k);
+            acc += __ldg(w + j * width + k) * __ldg(base + s * inner);
+        }
+        out[i] = acc;
+    }
+}
+
+// ---- finite differences, Neumann boundary ----------------------------------
+
+struct Vol {
+    const float* p;
+    int64_t nz, ny, nx;
+    __device__ __forceinline__ float at(int64_t z, int64_t y, int64_t x) const {
+        return __ldg(p + (z * ny + y) * nx + x);
+    }
+};
+
+__device__ __forceinline__ int64_t clampi(int64_t v, int64_t n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
+
+// d2 along one axis (linops_core_mlx.py:66-76): (f[i-1] - 2 f[i]) + f[i+1], edge-replicated.
+__device__ __forceinline__ float d2v(float fm, float f0, float fp) { return fm - 2.f * f0 + fp; }
+
+__global__ void k_hessian_fwd(Vol f, float* __restrict__ h, float w0, float w1, float w2, float w3,
+                              float w4, float w5) {
+    const int64_t n = f.nz * f.ny * f.nx;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t x = i % f.nx, t = i / f.nx, y = t % f.ny, z = t / f.ny;
+        const int64_t zm = clampi(z - 1, f.nz), zp = clampi(z + 1, f.nz);
+        const int64_t ym = clampi(y - 1, f.ny), yp = clampi(y + 1, f.ny);
+        const int64_t xm = clampi(x - 1, f.nx), xp = clampi(x + 1, f.nx);
+        const float c = f.at(z, y, x);
+        const float hzz = d2v(f.at(zm, y, x), c, f.at(zp, y, x));
+        const float hyy = d2v(f.at(z, ym, x), c, f.at(z, yp, x));
+        const float hxx = d2v(f.at(z, y, xm), c, f.at(z, y, xp));
+        // d1_cen(d1_cen(f, z), y): Dz at y+-1, then (Dz[y+1] - Dz[y-1]) / 2
+        const float dz_yp = (f.at(zp, yp, x) - f.at(zm, yp, x)) / 2.f;
+        const float dz_ym = (f.at(zp, ym, x) - f.at(zm, ym, x)) / 2.f;
+        const float hyz = (dz_yp - dz_ym) / 2.f;
+        const float dz_xp = (f.at(zp, y, xp) - f.at(zm, y, xp)) / 2.f;
+        const float dz_xm = (f.at(zp, y, xm) - f.at(zm, y, xm)) / 2.f;
+        const float hxz = (dz_xp - dz_xm) / 2.f;
+        const float dy_xp = (f.at(z, yp, xp) - f.at(z, ym, xp)) / 2.f;
+        const float dy_xm = (f.at(z, yp, xm) - f.at(z, ym, xm)) / 2.f;
+        const float hxy = (dy_xp - dy_xm) / 2.f;
+        h[i] = hzz * w0;
+        h[n + i] = hyy * w1;
+        h[2 * n + i] = hxx * w2;
+        h[3 * n + i] = hyz * w3;
+        h[4 * n + i] = hxz * w4;
+        h[5 * n + i] = hxy * w5;
+    }
+}
+
+// d1_cen_adj (linops_core_mlx.py:53-58): out[i] = (G(i-1) - G(i+1)) / 2 with
+// G(-1) = -g[0], G(n) = -g[n-1].
+// Each element is first multiplied by its component weight (H_w = H * w,
+// linops_mlx.py:250), exactly the float32 product the reference forms.
+__device__ __forceinline__ float gext(const float* g, int64_t j, int64_t n, int64_t s, float w) {
+    return j < 0 ? -(__ldg(g) * w) : (j >= n ? -(__ldg(g + (n - 1) * s) * w) : __ldg(g + j * s) * w);
+}
+
+// d1_cen_adj along axis b of (d1_cen_adj along axis a of H) at index (ib, ia)
+// of a 2-D slice g (strides sb, sa).  The inner (axis a) adjoint is evaluated
+// at ib-1 and ib+1 first, then the outer one combines them.
+__device__ __forceinline__ float inner_adj(const float* g, int64_t ia, int64_t na, int64_t sa,
+                                           float w) {
+    return (gext(g, ia - 1, na, sa, w) - gext(g, ia + 1, na, sa, w)) / 2.f;
+}
+
+__device__ __forceinline__ float mixed_adj(const float* g, int64_t ib, int64_t nb, int64_t sb,
+                                           int64_t ia, int64_t na, int64_t sa, float w) {
+    // value of the inner adjoint on row jb of axis b
+    auto row = [&](int64_t jb) -> float {
+        if (jb < 0) return -inner_adj(g, ia, na, sa, w);
+        if (jb >= nb) return -inner_adj(g + (nb - 1) * sb, ia, na, sa, w);
+        return inner_adj(g + jb * sb, ia, na, sa, w);
+    };
+    return (row(ib - 1) - row(ib + 1)) / 2.f;
+}
+
+// d2 of a weighted component h * w along one axis with edge replication.
+__device__ __forceinline__ float d2w(const float* g, int64_t i, int64_t n, int64_t s, float w) {
+    const float fm = __ldg(g + clampi(i - 1, n) * s) * w;
+    const float f0 = __ldg(g + i * s) * w;
+    const float fp = __ldg(g + clampi(i + 1, n) * s) * w;
+    return d2v(fm, f0, fp);
+}
+
+// Hessian3D.adjoint (linops_mlx.py:244-259): weights applied per element,
+// then the six adjoint stencils summed in the reference's order.
+__global__ void k_hessian_adj(const float* __restrict__ hw, float* __restrict__ out, int64_t nz,
+                              int64_t ny, int64_t nx, float w0, float w1, float w2, float w3,
+                              float w4, float w5) {
+    const int64_t n = nz * ny * nx;
+    const int64_t sz = ny * nx, sy = nx, sx = 1;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t x = i % nx, t = i / nx, y = t % ny, z = t / ny;
+        const float azz = d2w(hw + y * sy + x, z, nz, sz, w0);
+        const float ayy = d2w(hw + n + z * sz + x, y, ny, sy, w1);
+        const float axx = d2w(hw + 2 * n + z * sz + y * sy, x, nx, sx, w2);
+        // adj_yz = d1_cen_adj(d1_cen_adj(H3, axis=y), axis=z)
+        const float ayz = mixed_adj(hw + 3 * n + x, z, nz, sz, y, ny, sy, w3);
+        // adj_xz = d1_cen_adj(d1_cen_adj(H4, axis=x), axis=z)
+        const float axz = mixed_adj(hw + 4 * n + y * sy, z, nz, sz, x, nx, sx, w4);
+        // adj_xy = d1_cen_adj(d1_cen_adj(H5, axis=x), axis=y)
+        const float axy = mixed_adj(hw + 5 * n + z * sz, y, ny, sy, x, nx, sx, w5);
+        out[i] = ((((azz + ayy) + axx) + ayz) + axz) + axy;
+    }
+}
+
+// Gradient3D: forward differences with f[n] = f[n-1] (linops_core_mlx.py:25-32).
+__global__ void k_gradient_fwd(Vol f, float* __restrict__ g, float r) {
+    const int64_t n = f.nz * f.ny * f.nx;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t x = i % f.nx, t = i / f.nx, y = t % f.ny, z = t / f.ny;
+        const float c = f.at(z, y, x);
+        g[i] = r * (f.at(clampi(z + 1, f.nz), y, x) - c);
+        g[n + i] = f.at(z, clampi(y + 1, f.ny), x) - c;
+        g[2 * n + i] = f.at(z, y, clampi(x + 1, f.nx)) - c;
+    }
+}
+
+// d1_fwd_adj (linops_core_mlx.py:35-39): [-g0, g[i-1] - g[i], g[n-2]]
+__device__ __forceinline__ float d1f_adj(const float* g, int64_t i, int64_t n, int64_t s, float sc) {
+    if (n == 1) return -(__ldg(g) * sc);
+    if (i == 0) return -(__ldg(g) * sc);
+    if (i == n - 1) return __ldg(g + (n - 2) * s) * sc;
+    return __ldg(g + (i - 1) * s) * sc - __ldg(g + i * s) * sc;
+}
+
+__global__ void k_gradient_adj(const float* __restrict__ g, float* __restrict__ out, int64_t nz,
+                               int64_t ny, int64_t nx, float r) {
+    const int64_t n = nz * ny * nx, sz = ny * nx, sy = nx;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t x = i % nx, t = i / nx, y = t % ny, z = t / ny;
+        const float az = d1f_adj(g + y * sy + x, z, nz, sz, r);
+        const float ay = d1f_adj(g + n + z * sz + x, y, ny, sy, 1.f);
+        const float ax = d1f_adj(g + 2 * n + z * sz + y * sy, x, nx, 1, 1.f);
+        out[i] = (az + ay) + ax;
+    }
+}
+
+static void hessian_weights(float r, float w[6]) {
+    // linops_mlx.py:237-239 (SQRT2 is a float32 device scalar there)
+    const float s2 = sqrtf(2.f);
+    w[0] = (float)((double)r * (double)r);
+    w[1] = 1.f;
+    w[2] = 1.f;
+    w[3] = r * s2;
+    w[4] = r * s2;
+    w[5] = s2;
+}
+
+}  // namespace dk
+
+using namespace dk;
+
+extern "C" {
+
+int decon_window_copy(const float* src, const int64_t* src_shape, const int64_t* src_start,
+                      float* dst, const int64_t* dst_shape, const int64_t* dst_start,
+                      const int64_t* ext, int ndim, void* stream) {
+    if (!src || !dst || !src_shape || !dst_shape || !ext) return fail(DECON_ERR_NULL, "null pointer");
+    if (ndim < 1 || ndim > 4) return fail(DECON_ERR_VALUE, "window copy supports 1-4 dims");
+    Box4 b;
+    const int off = 4 - ndim;
+    int64_t n = 1;
+    for (int d = 0; d < 4; ++d) {
+        if (d < off) {
+            b.ss[d] = b.ds[d] = b.ext[d] = 1;
+            b.s0[d] = b.d0[d] = 0;
+        } else {
+            const int k = d - off;
+            b.ss[d] = src_shape[k];
+            b.ds[d] = dst_shape[k];
+            b.ext[d] = ext[k];
+            b.s0[d] = src_start ? src_start[k] : 0;
+            b.d0[d] = dst_start ? dst_start[k] : 0;
+            if (b.ext[d] < 0 || b.s0[d] < 0 || b.d0[d] < 0 || b.s0[d] + b.ext[d] > b.ss[d] ||
+                b.d0[d] + b.ext[d] > b.ds[d])
+                return fail(DECON_ERR_VALUE, "window outside the array on axis %d", k);
+        }
+        n *= b.ds[d];
+    }
+    if (n == 0) return DECON_OK;
+    k_window_copy<<<grid1d(n, 256), 256, 0, as_stream(stream)>>>(src, dst, b, n);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_band_widths(int64_t n_large, int64_t n_small, int* w_fwd, int* w_adj) {
+    if (n_large < 1 || n_small < 1) return fail(DECON_ERR_VALUE, "band sizes must be positive");
+    const double s = (double)n_large / (double)n_small;
+    if (w_fwd) *w_fwd = (int)std::min<int64_t>(n_large, (int64_t)std::ceil(s) + 2);
+    if (w_adj) *w_adj = (int)std::min<int64_t>(n_small, (int64_t)std::ceil(1.0 / s) + 3);
+    return DECON_OK;
+}
+
+int decon_band_weights(int64_t n_large, int64_t n_small, int32_t* idx_f, float* w_f,
+                       int32_t* idx_a, float* w_a) {
+    int wf = 0, wa = 0;
+    DK_TRY(decon_band_widths(n_large, n_small, &wf, &wa));
+    const double s = (double)n_large / (double)n_small;
+    // large -> small: output cell [i s, (i+1) s) against unit cells [j, j+1)
+    for (int64_t i = 0; i < n_small; ++i) {
+        int64_t first = (int64_t)std::floor((double)i * s);
+        first = std::min<int64_t>(std::max<int64_t>(first, 0), n_large - wf);
+        const double lo = (double)i * s, hi = (double)(i + 1) * s;
+        for (int k = 0; k < wf; ++k) {
+            const int64_t j = first + k;
+            const double jd = (double)j;
+            if (idx_f) idx_f[i * wf + k] = (int32_t)j;
+            if (w_f) w_f[i * wf + k] = (float)std::max(0.0, std::min(hi, jd + 1) - std::max(lo, jd));
+        }
+    }
+    // small -> large (exact transpose derived independently)
+    for (int64_t j = 0; j < n_large; ++j) {
+        int64_t first = (int64_t)std::floor((double)j / s) - 1;
+        first = std::min<int64_t>(std::max<int64_t>(first, 0), n_small - wa);
+        const double b = (double)j;
+        for (int k = 0; k < wa; ++k) {
+            const int64_t i = first + k;
+            const double lo = (double)i * s, hi = ((double)i + 1) * s;
+            if (idx_a) idx_a[j * wa + k] = (int32_t)i;
+            if (w_a) w_a[j * wa + k] = (float)std::max(0.0, std::min(hi, b + 1) - std::max(lo, b));
+        }
+    }
+    return DECON_OK;
+}
+
+int decon_banded_axis(const float* in, float* out, int64_t outer, int64_t n_in, int64_t inner,
+                      int64_t n_out, const int32_t* idx, const float* w, int width, void* stream) {
+    if (!in || !out || !idx || !w) return fail(DECON_ERR_NULL, "null pointer");
+    if (outer < 0 || inner < 0 || n_in < 1 || n_out < 1 || width < 1)
+        return fail(DECON_ERR_VALUE, "bad banded shape");
+    const int64_t n = outer * n_out * inner;
+    if (n == 0) return DECON_OK;
+    k_banded<<<grid1d(n, 256), 256, 0, as_stream(stream)>>>(in, out, outer, n_in, inner, n_out, idx,
+                                                            w, width);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_hessian3d_forward(const float* x, float* h, const int64_t shape[3], float r, void* stream) {
+    if (!x || !h || !shape) return fail(DECON_ERR_NULL, "null pointer");
+    float w[6];
+    hessian_weights(r, w);
+    Vol f{x, shape[0], shape[1], shape[2]};
+    const int64_t n = shape[0] * shape[1] * shape[2];
+    k_hessian_fwd<<<grid1d(n, 256), 256, 0, as_stream(stream)>>>(f, h, w[0], w[1], w[2], w[3], w[4], w[5]);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_hessian3d_adjoint(const float* h, float* x, const int64_t shape[3], float r, void* stream) {
+    if (!h || !x || !shape) return fail(DECON_ERR_NULL, "null pointer");
+    float w[6];
+    hessian_weights(r, w);
+    const int64_t n = shape[0] * shape[1] * shape[2];
+    k_hessian_adj<<<grid1d(n, 256), 256, 0, as_stream(stream)>>>(h, x, shape[0], shape[1], shape[2],
+                                                                 w[0], w[1], w[2], w[3], w[4], w[5]);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_gradient3d_forward(const float* x, float* g, const int64_t shape[3], float r, void* stream) {
+    if (!x || !g || !shape) return fail(DECON_ERR_NULL, "null pointer");
+    Vol f{x, shape[0], shape[1], shape[2]};
+    const int64_t n = shape[0] * shape[1] * shape[2];
+    k_gradient_fwd<<<grid1d(n, 256), 256, 0, as_stream(stream)>>>(f, g, r);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_gradient3d_adjoint(const float* g, float* x, const int64_t shape[3], float r, void* stream) {
+    if (!g || !x || !shape) return fail(DECON_ERR_NULL, "null pointer");
+    const int64_t n = shape[0] * shape[1] * shape[2];
+    k_gradient_adj<<<grid1d(n, 256), 256, 0, as_stream(stream)>>>(g, x, shape[0], shape[1], shape[2], r);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,29 @@
+"""Drop-in B200 implementation of deconlib's deconvolution hot path.
+
+Same names and signatures as ``deconlib.deconvolution`` for the operator
+algebra (LinearFFTConvolver, FFTConvolver, Pad, Crop,
+FractionalAreaDownsample / Upsample, Hessian / Gradient, compose) and the
+solvers (richardson_lucy_with_operator, solve_pdhg_mlx,
+solve_pdhg_with_operator).  Arrays are CUDA ``torch.Tensor`` float32; NumPy
+input is copied to the device.
+"""
+
+from .base import MLXDeconvolutionResult
+from .composition import Compose, LinearOperator, as_numpy_op, compose
+from .core_operators import Crop, FractionalAreaDownsample, FractionalAreaUpsample, Pad
+from .linops import (FFTConvolver, Gradient1D, Gradient2D, Gradient3D, Hessian1D, Hessian2D,
+                     Hessian3D, LinearFFTConvolver, fast_padded_shape, pad_corner_origin_kernel)
+from .pdhg import (GradientRegularizer, HessianRegularizer, IdentityRegularizer,
+                   prox_gaussian_dual, prox_l1_2_dual, prox_l1_dual, prox_nonneg,
+                   prox_poisson_dual, solve_pdhg_mlx, solve_pdhg_with_operator)
+from .rl import RLResult, poisson_i_divergence, richardson_lucy_solver, richardson_lucy_with_operator
+
+__all__ = [
+    "MLXDeconvolutionResult", "Compose", "LinearOperator", "as_numpy_op", "compose", "Crop",
+    "FractionalAreaDownsample", "FractionalAreaUpsample", "Pad", "FFTConvolver", "Gradient1D",
+    "Gradient2D", "Gradient3D", "Hessian1D", "Hessian2D", "Hessian3D", "LinearFFTConvolver",
+    "fast_padded_shape", "pad_corner_origin_kernel", "GradientRegularizer", "HessianRegularizer",
+    "IdentityRegularizer", "prox_gaussian_dual", "prox_l1_2_dual", "prox_l1_dual", "prox_nonneg",
+    "prox_poisson_dual", "solve_pdhg_mlx", "solve_pdhg_with_operator", "RLResult",
+    "poisson_i_divergence", "richardson_lucy_solver", "richardson_lucy_with_operator",
+]

@@ -1,0 +1,238 @@
+/*
+ * decon_b200.h -- C ABI of the B200 (sm_100a) 3D deconvolution library.
+ *
+ * The library is the device side of deconlib's deconvolution hot path:
+ * linear FFT convolution, pad/crop, fractional-area resampling, Hessian and
+ * gradient stencils, Richardson-Lucy and adaptive-PDHG iterations.  Every
+ * entry point takes plain pointers, int64 shapes and a CUDA stream passed as
+ * ``void*`` (a ``cudaStream_t``; NULL is the legacy default stream).  Array
+ * pointers are DEVICE pointers to C-contiguous float32 data unless the
+ * comment says "host".  Volumes are (z, y, x); 1-D and 2-D problems are
+ * passed with leading extents of 1.
+ *
+ * Every function returns a status code (DECON_OK == 0).  On failure
+ * decon_last_error() returns a message for the calling host thread.  Launches
+ * are asynchronous: a status of DECON_OK means the work was queued.  Only the
+ * functions documented as "synchronises" wait for the device.
+ *
+ * The reference (deconlib 0.4.0) is pure Python on MLX; it has no native
+ * FFI.  Each entry point below names the Python interface it replaces
+ * (file:line inside the deconlib project).
+ */
+#ifndef DECON_B200_H
+#define DECON_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define DECON_OK 0
+#define DECON_ERR_VALUE 1       /* bad shape or argument (Python: ValueError) */
+#define DECON_ERR_UNSUPPORTED 2 /* size the kernels do not implement            */
+#define DECON_ERR_OOM 3         /* device allocation failed                    */
+#define DECON_ERR_CUDA 4        /* CUDA runtime error                          */
+#define DECON_ERR_TIMEOUT 5     /* a bounded device wait ran out               */
+#define DECON_ERR_NULL 6        /* null handle or pointer                      */
+
+/* Message for the last failing call on this host thread ("" if none). */
+const char* decon_last_error(void);
+/* Library ABI version (major * 10000 + minor * 100 + patch). */
+int decon_version(void);
+
+/* ---- FFT sizing (deconvolution/linops_mlx.py:956-1032) ---------------- */
+
+/* Smallest m >= n whose prime factors are 2, 3 and 5 only
+ * (linops_mlx.py:956 _next_smooth_number). */
+int64_t decon_next_smooth(int64_t n);
+
+/* Per-axis 5-smooth canvas >= max(N + pad, M); pad_or_minus1[i] < 0 means
+ * the default M - 1 (linops_mlx.py:975 fast_padded_shape).  Host arrays. */
+int decon_fast_padded_shape(int ndim, const int64_t* signal, const int64_t* kernel,
+                            const int64_t* pad_or_minus1, int64_t* out);
+
+/* ---- linear FFT convolution (deconvolution/linops_mlx.py:435-533) ------ */
+
+typedef struct decon_conv decon_conv; /* opaque plan: OTF, spectra, twiddles */
+
+/* LinearFFTConvolver.__init__ (linops_mlx.py:473-518): embeds the
+ * corner-origin kernel (utils/padding.py:142) in the canvas fft_shape,
+ * divides by its sum when normalize != 0 (FP64 sum) and stores
+ * OTF = rfftn(kernel) resident on the device.  kernel: device, shape kshape.
+ * Validates fft_shape >= signal + kernel - 1 (DECON_ERR_VALUE otherwise).
+ * Synchronises (the plan is ready on return). */
+int decon_conv_create(const float* kernel, const int64_t kshape[3], const int64_t signal_shape[3],
+                      const int64_t fft_shape[3], int normalize, void* stream, decon_conv** out);
+/* FFTConvolver.__init__ (linops_mlx.py:395-415): circular convolution on the
+ * kernel's own shape (canvas = signal = kernel shape, no corner embedding).
+ * Synchronises. */
+int decon_conv_create_circular(const float* kernel, const int64_t shape[3], int normalize,
+                               void* stream, decon_conv** out);
+int decon_conv_destroy(decon_conv* plan);
+/* operator_norm_sq = max |OTF|^2 (linops_mlx.py:415). */
+int decon_conv_norm_sq(const decon_conv* plan, double* out);
+/* Canvas fft_shape and the spectrum row pitch (complex elements). Host. */
+int decon_conv_shape(const decon_conv* plan, int64_t fft_shape[3], int64_t* pitch);
+/* Copies the OTF (fft_z, fft_y, fft_x/2+1) complex64 into out (device). */
+int decon_conv_get_otf(const decon_conv* plan, float* out_interleaved, void* stream);
+
+/* LinearFFTConvolver.forward: zero-pad, circular convolution, crop
+ * (linops_mlx.py:520-524).  x, y: signal_shape; y may alias x. */
+int decon_conv_forward(decon_conv* plan, const float* x, float* y, void* stream);
+/* LinearFFTConvolver.adjoint: correlation with conj(OTF)
+ * (linops_mlx.py:526-530). */
+int decon_conv_adjoint(decon_conv* plan, const float* y, float* x, void* stream);
+
+/* ---- Richardson-Lucy fused iterations (deconvolution/rl_mlx.py:83-185) - */
+
+/* RL set-up (rl_mlx.py:122-133): sens_raw = A^T 1, floor = max(max(sens)
+ * 1e-6, 1e-10); writes sens_masked = sens where sens > floor else 0 and
+ * x = active ? max(x_init, 1e-6) : 0.  If x_init is NULL, x0 = A^T max(y - b,
+ * 1e-6) as the reference does.  All arrays signal_shape.  Synchronises. */
+int decon_rl_setup(decon_conv* plan, const float* observed, float background, const float* x_init,
+                   float* x, float* sens_masked, void* stream);
+/* One RL iteration for blur_op = LinearFFTConvolver (rl_mlx.py:146-150):
+ * ratio = y / max(A x + b, 1e-10) fused into the forward pass epilogue and
+ * x = max(x * (sens>0 ? A^T ratio / sens : 0), 1e-10) fused into the adjoint
+ * pass epilogue.  ratio is caller scratch (signal_shape).  If loss_partials
+ * is non-NULL, the forward epilogue also accumulates the Poisson
+ * I-divergence of the INCOMING x (rl_mlx.py:58-80) into
+ * loss_partials[0] as an FP64 sum (see decon_rl_loss_finish). */
+int decon_rl_iteration(decon_conv* plan, const float* observed, float background,
+                       const float* sens_masked, float* x, float* ratio, double* loss_sum,
+                       void* stream);
+/* pred = A x + b and (if loss_sum != NULL) the FP64 I-divergence sum of
+ * (observed, pred) (rl_mlx.py:159-160,174). */
+int decon_rl_predict(decon_conv* plan, const float* observed, float background, const float* x,
+                     float* pred, double* loss_sum, void* stream);
+
+/* Element-wise RL steps for an arbitrary composed blur operator (the
+ * caller runs forward/adjoint through the operator entry points):
+ *   decon_rl_ratio:  ratio = y / max(model + b, 1e-10) (rl_mlx.py:147-148);
+ *                    ratio may be NULL; if loss_sum != NULL also the FP64
+ *                    I-divergence sum (rl_mlx.py:58-80), which needs a
+ *                    workspace of decon_reduce_workspace_bytes().
+ *   decon_rl_update: x = max(x * (sens>0 ? corr/sens : 0), 1e-10) (:149-150)
+ *   decon_rl_data_floor: out = max(y - b, 1e-6) (:123)
+ *   decon_rl_mask:   floor = max(max(sens) 1e-6, 1e-10); sens = active ? sens
+ *                    : 0; x = active ? max(x, 1e-6) : 0 (:125-133). */
+int decon_rl_ratio(const float* model, const float* observed, float background, float* ratio,
+                   int64_t n, double* loss_sum, void* workspace, void* stream);
+int decon_rl_update(float* x, const float* corr, const float* sens_masked, int64_t n, void* stream);
+int decon_rl_data_floor(const float* observed, float background, float* out, int64_t n, void* stream);
+int decon_rl_mask(float* x, float* sens, int64_t n, void* workspace, void* stream);
+int decon_fill(float* p, float value, int64_t n, void* stream);
+int decon_clamp_min(const float* a, float lo, float* out, int64_t n, void* stream);
+/* out = alpha a + beta (pred = A x + b, rl_mlx.py:174). */
+int decon_affine(const float* a, float alpha, float beta, float* out, int64_t n, void* stream);
+
+/* ---- adaptive PDHG (deconvolution/pdhg_mlx.py:507-1242) ------------------ */
+
+typedef struct decon_pdhg decon_pdhg; /* device-resident tau/sigma/theta + histories */
+
+/* State for one solve: tau = sigma = step_scale, theta = 1 (pdhg_mlx.py:693-701).
+ * Every kernel below reads the step sizes from this state and returns at
+ * once after the stop flag is set (convergence or num_iter reached), so a
+ * host can queue iterations without synchronising. */
+int decon_pdhg_create(int num_iter, double step_scale, double delta, double eta, double tol,
+                      int min_iter, int patience, decon_pdhg** out);
+int decon_pdhg_destroy(decon_pdhg* h);
+/* y1 = prox_{sigma F*}(y1 + sigma ((1+theta) Ax_cur - theta Ax_prev)),
+ * loss_type 0 Poisson (pdhg_mlx.py:115-166), 1 Gaussian (:169-189). */
+int decon_pdhg_dual_data(decon_pdhg* h, float* y1, const float* ax_cur, const float* ax_prev,
+                         const float* data, float background, int loss_type, int64_t m,
+                         void* stream);
+/* y2 = proj(y2 + sigma L xbar); norm 0 L1 clip, 1 L1,2 ball (pdhg_mlx.py:197-233).
+ * y2, lxbar: (ncomp, n). */
+int decon_pdhg_dual_reg(decon_pdhg* h, float* y2, const float* lxbar, float alpha, int norm,
+                        int ncomp, int64_t n, void* stream);
+/* xbar = x_cur + theta (x_cur - x_prev) (pdhg_mlx.py:841). */
+int decon_pdhg_xbar(decon_pdhg* h, const float* xc, const float* xp, float* xbar, int64_t n,
+                    void* stream);
+/* x_new = max(0, x - tau (aty + lty)) plus FP64 ||dx||^2, ||x||^2, ||x_new||^2
+ * (pdhg_mlx.py:741-750, 805-806); lty may be NULL. */
+int decon_pdhg_primal(decon_pdhg* h, const float* xc, const float* aty, const float* lty,
+                      float* xn, int64_t n, void* stream);
+int decon_pdhg_sub(decon_pdhg* h, const float* a, const float* b, float* d, int64_t n, void* stream);
+/* ||A x_new - A x||^2 and (l_dx != NULL) ||L (x_new - x)||^2 (pdhg_mlx.py:753-759). */
+int decon_pdhg_dk(decon_pdhg* h, const float* ax_new, const float* ax_cur, int64_t m,
+                  const float* l_dx, int64_t nl, void* stream);
+/* Malitsky-Pock step-size update and convergence test in FP64 (pdhg_mlx.py:761-857). */
+int decon_pdhg_step(decon_pdhg* h, void* stream);
+/* Objective at iteration k (pdhg_mlx.py:860-881): data term of (ax + b, data)
+ * plus alpha times the L1 / L1,2 norm of lx (ncomp, n). */
+int decon_pdhg_loss(decon_pdhg* h, const float* ax, const float* data, float background,
+                    int loss_type, int64_t m, const float* lx, int norm, int ncomp, int64_t n,
+                    double alpha, int k, void* stream);
+/* Reads the state (synchronises): iteration counter, final iteration,
+ * converged and stop flags, (tau, sigma, theta) and the histories (host
+ * arrays of num_iter doubles; any may be NULL). */
+int decon_pdhg_read(decon_pdhg* h, int* k, int* final_iter, int* converged, int* stop,
+                    double* scalars3, double* tau_hist, double* sigma_hist, double* loss_hist,
+                    double* rel_hist, void* stream);
+/* Host-requested stop (a callback returned truthy). Synchronises. */
+int decon_pdhg_set_stop(decon_pdhg* h, int final_iter, void* stream);
+
+/* ---- pad / crop (deconvolution/core_operators.py:29-137) ---------------- */
+
+/* Copies the box [start, start + ext) of src (shape src_shape) to dst at
+ * dst_start inside dst_shape; every other dst element is set to zero.  One
+ * kernel serves Pad.forward/adjoint and Crop.forward/adjoint. ndim <= 4. */
+int decon_window_copy(const float* src, const int64_t* src_shape, const int64_t* src_start,
+                      float* dst, const int64_t* dst_shape, const int64_t* dst_start,
+                      const int64_t* ext, int ndim, void* stream);
+
+/* ---- fractional-area resampling (core_operators.py:151-450) ------------- */
+
+/* Band tables of _banded_overlap_weights_1d (core_operators.py:151-202),
+ * computed on the host in FP64 and rounded to float32.  widths via
+ * decon_band_widths.  Host arrays. */
+int decon_band_widths(int64_t n_large, int64_t n_small, int* w_fwd, int* w_adj);
+int decon_band_weights(int64_t n_large, int64_t n_small, int32_t* idx_fwd, float* w_fwd,
+                       int32_t* idx_adj, float* w_adj);
+/* out[o, i, q] = sum_k w[i,k] * in[o, idx[i,k], q] along one axis
+ * (_apply_banded_1d, core_operators.py:205-219).  in: (outer, n_in, inner),
+ * out: (outer, n_out, inner); idx/w: device (n_out, width). */
+int decon_banded_axis(const float* in, float* out, int64_t outer, int64_t n_in, int64_t inner,
+                      int64_t n_out, const int32_t* idx, const float* w, int width, void* stream);
+
+/* ---- finite-difference operators (linops_mlx.py:92-262) ----------------- */
+
+/* Hessian3D.forward: h[6, z, y, x] = [r^2 zz, yy, xx, sqrt2 r yz, sqrt2 r xz,
+ * sqrt2 xy] with Neumann boundaries (linops_mlx.py:224-242). */
+int decon_hessian3d_forward(const float* x, float* h, const int64_t shape[3], float r,
+                            void* stream);
+/* Hessian3D.adjoint (linops_mlx.py:244-259). */
+int decon_hessian3d_adjoint(const float* h, float* x, const int64_t shape[3], float r,
+                            void* stream);
+/* Gradient3D.forward / adjoint (linops_mlx.py:107-119). */
+int decon_gradient3d_forward(const float* x, float* g, const int64_t shape[3], float r,
+                             void* stream);
+int decon_gradient3d_adjoint(const float* g, float* x, const int64_t shape[3], float r,
+                             void* stream);
+
+/* ---- reductions (FP64, deterministic) ----------------------------------- */
+
+#define DECON_RED_SUM 0      /* sum a                          */
+#define DECON_RED_SUMSQ 1    /* sum a^2                        */
+#define DECON_RED_DIFFSQ 2   /* sum (a - b)^2                  */
+#define DECON_RED_MAX 3      /* max a                          */
+#define DECON_RED_DOT 4      /* sum a b                        */
+/* Bytes of device workspace decon_reduce needs (per concurrent call). */
+int64_t decon_reduce_workspace_bytes(void);
+/* out[0] (device double) = reduction over n elements of a (and b).  Two
+ * fixed-shape passes, so the result is bitwise reproducible run to run.
+ * workspace: caller-owned device buffer of decon_reduce_workspace_bytes();
+ * calls that share a workspace must be ordered on one stream.  This is the
+ * FP64 reduction the solvers use for norms, flux and step sizes
+ * (pdhg_mlx.py:750,759,805-809; rl_mlx.py:77-80,130). */
+int decon_reduce(const float* a, const float* b, int64_t n, int op, double* out, void* workspace,
+                 void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DECON_B200_H */

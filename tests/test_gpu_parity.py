@@ -1,0 +1,248 @@
+"""GPU parity: the CUDA path (through libdecon_b200's C ABI) against the
+golden vectors of the reference and against the CPU oracle.
+
+Tolerances (relative L2 unless stated):
+  * operators (conv, resampling, stencils): 2e-6 vs the float32 reference
+    (both are float32 evaluations of the same formulas; only FFT rounding
+    differs) and 1e-6 against the float64 oracle for the convolution;
+  * Pad / Crop: bit-exact;
+  * Richardson-Lucy trajectories: 1e-5 after 8-12 iterations;
+  * PDHG trajectories: max(1e-4, 2 x the float32-vs-float64 reference spread),
+    because the GPU computes step sizes and reductions in FP64 while the
+    float32 reference rounds them to float32 (the stated tolerance rule).
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.fixture(scope="module")
+def g32():
+    return np.load(os.path.join(HERE, "golden", "golden_fp32.npz"))
+
+
+@pytest.fixture(scope="module")
+def g64():
+    return np.load(os.path.join(HERE, "golden", "golden_fp64.npz"))
+
+
+@pytest.fixture(scope="module")
+def D():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import deconlib_b200.deconvolution as d
+
+    return d
+
+
+def rel(a, b):
+    a = np.asarray(a.detach().cpu().numpy() if hasattr(a, "detach") else a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def cpu(t):
+    return t.detach().cpu().numpy()
+
+
+def test_conv_forward_adjoint(D, g32, g64):
+    c = D.LinearFFTConvolver(g32["psf16"], (16, 32, 32))
+    assert c.fft_shape == tuple(g32["conv_fft_shape"])
+    assert abs(c.operator_norm_sq - float(g32["conv_norm"])) < 1e-5
+    x = g32["conv_x"]
+    assert rel(c.forward(x), g32["conv_fwd"]) < 2e-6
+    assert rel(c.adjoint(x), g32["conv_adj"]) < 2e-6
+    assert rel(c.forward(x), g64["conv_fwd"]) < 1e-6
+    assert rel(c.adjoint(x), g64["conv_adj"]) < 1e-6
+
+
+def test_conv_odd_and_explicit_canvas(D, g32, g64):
+    co = D.LinearFFTConvolver(g32["kodd"], (9, 11, 13))
+    assert co.fft_shape == tuple(g32["convodd_fft_shape"])
+    xo = g32["convodd_x"]
+    assert rel(co.forward(xo), g64["convodd_fwd"]) < 1e-6
+    assert rel(co.adjoint(xo), g64["convodd_adj"]) < 1e-6
+    assert abs(co.operator_norm_sq - float(g64["convodd_norm"])) < 1e-6 * float(g64["convodd_norm"])
+    cx = D.LinearFFTConvolver(g32["kodd"], (9, 11, 13), normalize=False, fft_shape=(15, 18, 25))
+    assert rel(cx.forward(xo), g64["convx_fwd"]) < 1e-6
+    assert rel(cx.adjoint(xo), g64["convx_adj"]) < 1e-6
+
+
+def test_conv_2d(D, g64):
+    c = D.LinearFFTConvolver(g64["k2d"].astype(np.float32), (20, 30))
+    x = g64["conv2d_x"].astype(np.float32)
+    assert rel(c.forward(x), g64["conv2d_fwd"]) < 1e-6
+    assert rel(c.adjoint(x), g64["conv2d_adj"]) < 1e-6
+
+
+def test_otf_matches_oracle(D, g32):
+    from oracle import ops
+
+    c = D.LinearFFTConvolver(g32["psf16"], (16, 32, 32))
+    o = ops.LinearFFTConvolver(g32["psf16"], (16, 32, 32), dtype=np.float64)
+    err = np.linalg.norm(cpu(c.otf) - o.otf) / np.linalg.norm(o.otf)
+    assert err < 1e-6
+
+
+@pytest.mark.parametrize("shape,kshape", [((64, 128, 128), (64, 128, 128)),
+                                          ((40, 96, 72), (17, 33, 25)),
+                                          ((30, 50, 45), (9, 15, 12))])
+def test_conv_sizes_vs_fp64_oracle(D, shape, kshape):
+    from oracle import ops
+
+    rng = np.random.default_rng(sum(shape))
+    k = rng.random(kshape).astype(np.float32)
+    x = rng.random(shape).astype(np.float32)
+    c = D.LinearFFTConvolver(k, shape)
+    o = ops.LinearFFTConvolver(k, shape, dtype=np.float64)
+    assert rel(c.forward(x), o.forward(x.astype(np.float64))) < 2e-6
+    assert rel(c.adjoint(x), o.adjoint(x.astype(np.float64))) < 2e-6
+
+
+def test_conv_adjoint_identity(D):
+    # <A x, y> == <x, A^T y>  (tests/test_composition.py:66-73, rtol 1e-4)
+    rng = np.random.default_rng(3)
+    k = rng.random((7, 9, 11)).astype(np.float32)
+    c = D.LinearFFTConvolver(k, (20, 24, 28))
+    x = rng.random((20, 24, 28)).astype(np.float32)
+    y = rng.random((20, 24, 28)).astype(np.float32)
+    lhs = float(np.sum(cpu(c.forward(x)).astype(np.float64) * y))
+    rhs = float(np.sum(x.astype(np.float64) * cpu(c.adjoint(y))))
+    assert abs(lhs - rhs) <= 1e-5 * abs(lhs)
+
+
+def test_pad_crop_exact(D, g32):
+    x = g32["pad_x"]
+    np.testing.assert_array_equal(cpu(D.Pad(((1, 2), (0, 3), (4, 0))).forward(x)), g32["pad_fwd"])
+    c = D.Crop((9, 10, 11), (5, 6, 7))
+    np.testing.assert_array_equal(cpu(c.forward(x)), g32["crop_fwd"])
+    np.testing.assert_array_equal(cpu(c.adjoint(g32["crop_y"])), g32["crop_adj"])
+    c2 = D.Crop((9, 10, 11), (5, 6, 7), start=(4, 0, 3))
+    np.testing.assert_array_equal(cpu(c2.forward(x)), g32["crop2_fwd"])
+    np.testing.assert_array_equal(cpu(c2.adjoint(g32["crop_y"])), g32["crop2_adj"])
+    p = D.Pad(((1, 2), (0, 3), (4, 0)))
+    np.testing.assert_array_equal(cpu(p.adjoint(p.forward(x))), x)
+
+
+def test_resampling(D, g32):
+    x, y = g32["rs_x"], g32["rs_y"]
+    d2 = D.FractionalAreaDownsample(2.0, in_shape=(12, 20, 18))
+    assert rel(d2.forward(x), g32["down2_fwd"]) < 2e-7
+    assert rel(d2.adjoint(y), g32["down2_adj"]) < 2e-7
+    d15 = D.FractionalAreaDownsample((1.5, 1.25, 2.5), in_shape=(12, 20, 18))
+    assert rel(d15.forward(x), g32["down15_fwd"]) < 2e-7
+    assert rel(d15.adjoint(g32["down15_y"]), g32["down15_adj"]) < 2e-7
+    assert rel(D.FractionalAreaDownsample(2.0).forward(x), g32["down2np_fwd"]) < 2e-7
+    up = D.FractionalAreaUpsample(2.0)
+    assert rel(up.forward(y), g32["up2_fwd"]) < 2e-7
+    assert rel(up.adjoint(x), g32["up2_adj"]) < 2e-7
+    up3 = D.FractionalAreaUpsample((1.5, 2.0, 3.0))
+    assert rel(up3.forward(y), g32["up3_fwd"]) < 2e-7
+    assert rel(D.FractionalAreaDownsample(3.0).forward(g32["rs2d_x"]), g32["down2d_fwd"]) < 2e-7
+    assert rel(D.FractionalAreaDownsample(2.5).forward(g32["rs1d_x"]), g32["down1d_fwd"]) < 2e-7
+
+
+def test_stencils(D, g32):
+    x, y = g32["hess_x"], g32["hess_y"]
+    h = D.Hessian3D(0.7)
+    assert rel(h.forward(x), g32["hess_fwd"]) < 2e-7
+    assert rel(h.adjoint(y), g32["hess_adj"]) < 2e-7
+    gr = D.Gradient3D(0.7)
+    assert rel(gr.forward(x), g32["grad_fwd"]) < 2e-7
+    assert rel(gr.adjoint(y[:3]), g32["grad_adj"]) < 2e-7
+
+
+def test_prox(D, g32):
+    y, d = g32["prox_y"], g32["prox_d"]
+    assert rel(D.prox_poisson_dual(y, 0.3, d, 2.0), g32["prox_poisson"]) < 1e-6
+    assert rel(D.prox_gaussian_dual(y, 0.3, d, 2.0), g32["prox_gauss"]) < 1e-6
+    np.testing.assert_array_equal(cpu(D.prox_l1_dual(y, 0.5)), g32["prox_l1"])
+    assert rel(D.prox_l1_2_dual(g32["prox_l12_y"], 0.5), g32["prox_l12"]) < 1e-6
+
+
+def test_rl_fused(D, g32, g64):
+    c = D.LinearFFTConvolver(g32["psf16"], (16, 32, 32))
+    r = D.richardson_lucy_with_operator(g32["rl_obs"], c, num_iter=12, background=10.0,
+                                        eval_interval=5)
+    assert r.iterations == int(g32["rl_iters"])
+    assert rel(r.restored, g32["rl_x"]) < 1e-5
+    assert rel(r.restored, g64["rl_x"]) < 1e-5
+    assert rel(r.pred, g64["rl_pred"]) < 1e-6
+    np.testing.assert_allclose(r.loss_history, g64["rl_loss"], rtol=1e-5)
+
+
+def test_rl_composed_crop(D, g32, g64):
+    c = D.LinearFFTConvolver(g32["psf16"], (16, 32, 32))
+    op = D.compose(D.Crop((16, 32, 32), (12, 26, 28), start=(2, 3, 2)), c)
+    r = D.richardson_lucy_with_operator(g32["rlc_obs"], op, num_iter=8, background=10.0,
+                                        eval_interval=3)
+    assert rel(r.restored, g64["rlc_x"]) < 1e-5
+    assert rel(r.pred, g64["rlc_pred"]) < 1e-6
+    np.testing.assert_allclose(r.loss_history, g64["rlc_loss"], rtol=1e-5)
+
+
+def test_rl_callback_stops(D, g32):
+    c = D.LinearFFTConvolver(g32["psf16"], (16, 32, 32))
+    seen = []
+    r = D.richardson_lucy_with_operator(g32["rl_obs"], c, num_iter=12, background=10.0,
+                                        callback=lambda k, x: seen.append(k) or k == 4)
+    assert r.iterations == 5 and seen == [0, 1, 2, 3, 4]
+
+
+PD_CASES = {
+    "pd_h_l1": dict(regularization="hessian", norm="L1"),
+    "pd_h_l12": dict(regularization="hessian", norm="L1_2"),
+    "pd_g_l1": dict(regularization="gradient", norm="L1"),
+    "pd_i_l1": dict(regularization="identity", norm="L1"),
+    "pd_h_gauss": dict(regularization="hessian", norm="L1", loss_type="gaussian"),
+}
+
+
+def _pd_tol(g32, g64, name):
+    spread = rel(g32[name + "_x"], g64[name + "_x"])
+    return max(1e-4, 2 * spread)
+
+
+@pytest.mark.parametrize("name", list(PD_CASES))
+def test_pdhg_sampling(D, g32, g64, name):
+    r = D.solve_pdhg_mlx(g32["pd_obs"], g32["psf_hr"], alpha=1e-3, sampling_factors=2.0,
+                         spacing=(0.05, 0.0425, 0.0425), background=5.0, num_iter=30,
+                         eval_interval=10, **PD_CASES[name])
+    t = _pd_tol(g32, g64, name)
+    assert r.iterations == int(g64[name + "_iters"])
+    assert rel(r.restored, g64[name + "_x"]) < t
+    np.testing.assert_allclose(r.tau_history, g64[name + "_tau"], rtol=max(t, 1e-4))
+    np.testing.assert_allclose(r.sigma_history, g64[name + "_sigma"], rtol=max(t, 1e-4))
+    np.testing.assert_allclose(r.loss_history, g64[name + "_loss"], rtol=1e-4)
+
+
+def test_pdhg_convergence_bin_plain_operator(D, g32, g64):
+    r = D.solve_pdhg_mlx(g32["pd_obs"], g32["psf_hr"], alpha=5.0, sampling_factors=2.0,
+                         background=5.0, num_iter=60, tol=5e-2, min_iter=3, patience=2)
+    assert r.iterations == int(g64["pd_conv_iters"])
+    assert r.converged == bool(g64["pd_conv_converged"])
+    assert rel(r.restored, g64["pd_conv_x"]) < 1e-4
+    r = D.solve_pdhg_mlx(g32["pd_obs"], g32["psf_hr"], alpha=1e-3, bin_factors=2,
+                         background=5.0, num_iter=15)
+    assert rel(r.restored, g64["pd_bin_x"]) < 1e-4
+    r = D.solve_pdhg_mlx(g32["rl_obs"], g32["psf16"], alpha=1e-3, background=10.0, num_iter=15,
+                         spacing=(0.1, 0.085, 0.085))
+    assert rel(r.restored, g64["pd_plain_x"]) < 1e-4
+    np.testing.assert_allclose(r.loss_history, g64["pd_plain_loss"], rtol=1e-4)
+    op = D.LinearFFTConvolver(g32["psf16"], (16, 32, 32))
+    seen = []
+    r = D.solve_pdhg_with_operator(g32["rl_obs"], op, alpha=1e-3, regularization="hessian",
+                                   background=10.0, num_iter=15,
+                                   callback=lambda k, x, loss: seen.append(loss))
+    assert rel(r.restored, g64["pdo_x"]) < 1e-4
+    np.testing.assert_allclose(r.tau_history, g64["pdo_tau"], rtol=1e-4)
+    np.testing.assert_allclose(r.loss_history, g64["pdo_loss"], rtol=1e-4)
+    assert len(seen) == 15
