@@ -1,0 +1,424 @@
+"""Benchmark: voxel-iterations/s of Hessian-PDHG and Richardson-Lucy at 128x256x256.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (seeded synthetic inputs, no dataset exists for it): the
+super-resolved Hessian-PDHG solve of a 128x256x256 object through
+compose(FractionalAreaDownsample(2), LinearFFTConvolver) against a
+64x128x128 Poisson observation (500 peak photons, background 5, PSF with a
+10 um index mismatch, 0.5 rad spherical and -0.2 rad coma, filament + bead
+phantom), alpha = 1e-3, L1 Hessian with r = dy/dz.  A step is one PDHG
+iteration over the whole volume.  The same line carries Richardson-Lucy at
+128x256x256 (beads + shells, 1000 photons, background 10) under "rl".
+
+``value``: object voxels x timed iterations / device time (CUDA events, max
+over ranks), inputs resident in HBM.  ``e2e``: the same metric through the
+public API (``solve_pdhg_mlx`` with NumPy host arrays: host->device copies,
+OTF set-up, iterations and the device->host copy of the result all inside the
+timed region).  ``roofline``: the axial FFT x OTF pass (the largest FFT pass),
+algorithmic bytes per launch / its average CUDA-event launch time.
+``cpu_baseline``: the NumPy oracle port of the reference on this host.
+
+Multi-GPU: the path does not shard; ``--gpus N`` runs N independent replicas
+(one process per GPU, torchrun), value = all replicas' voxel-iterations /
+max device time.  Timed iterations use tol = 0 so every one does full work.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+OBJ = (128, 256, 256)
+DATA = (64, 128, 128)
+SPACING_PD = (0.05, 0.0425, 0.0425)
+SPACING_RL = (0.1, 0.085, 0.085)
+METRIC = "voxel-iter/s RL & PDHG at 128x256^2 vs plain GPU; %HBM roofline; serve p50/p99"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], [], set()
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+                for nm, v in zip(names, r[4:8]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# inputs
+# ---------------------------------------------------------------------------
+
+
+def pdhg_inputs(D):
+    from deconlib_b200 import synth
+
+    psf, truth = synth.pdhg_workload(OBJ, SPACING_PD, seed=2)
+    fwd = D.compose(D.FractionalAreaDownsample(2.0, in_shape=OBJ), D.LinearFFTConvolver(psf, OBJ))
+    blur = fwd.forward(truth).cpu().numpy()
+    obs = synth.poisson_observation(blur, 500.0, 5.0, np.random.default_rng(3))
+    return psf, obs
+
+
+def rl_inputs(D):
+    from deconlib_b200 import synth
+
+    psf, truth = synth.rl_workload(OBJ, SPACING_RL, seed=0)
+    blur = D.LinearFFTConvolver(psf, OBJ).forward(truth).cpu().numpy()
+    obs = synth.poisson_observation(blur, 1000.0, 10.0, np.random.default_rng(1))
+    return psf, obs
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes of the axial pass (per launch)
+# ---------------------------------------------------------------------------
+
+
+def zpass_bytes(n_shape, f_shape):
+    nz = n_shape[0]
+    fz, fy, fx = f_shape
+    hx = fx // 2 + 1
+    hs = nz * fy * hx
+    hf = fz * fy * hx
+    return 8 * (2 * hs + hf)  # read S2, read OTF, write S2
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch from a committed ncu summary (profiles/<name>.json)."""
+    p = os.path.join(ROOT, "profiles", name + ".json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    import ctypes as C
+
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import deconlib_b200.deconvolution as D
+    from deconlib_b200 import _lib
+    from deconlib_b200.deconvolution.pdhg import HessianRegularizer, PDHGRunner, _compute_spacing_ratio
+
+    lib = _lib.load()
+    K, W = args.steps, args.warmup
+    psf, obs = pdhg_inputs(D)
+    n_obj = int(np.prod(OBJ))
+
+    # --- PDHG, resident inputs ---------------------------------------------
+    from deconlib_b200.deconvolution._device import to_device
+
+    data = to_device(obs)
+    conv = D.LinearFFTConvolver(psf, OBJ)
+    A = D.compose(D.FractionalAreaDownsample((2.0, 2.0, 2.0)), conv)
+    reg = HessianRegularizer(3, _compute_spacing_ratio(SPACING_PD, 3), "L1")
+    x0 = D.prox_nonneg(A.adjoint(data))
+    runner = PDHGRunner(data, A, reg, x0, 1e-3, "poisson", W + K, 5.0, 0.99, 0.5, 10, 0.0, 20, 5)
+    for _ in range(W):
+        runner.iterate()
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = lib.decon_launch_count()
+    lib.decon_profile_start(_lib.PROF_ZOTF)
+    e0.record(st)
+    for _ in range(K):
+        runner.iterate()
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms_z, nz_launch = C.c_double(), C.c_int64()
+    lib.decon_profile_stop(C.byref(ms_z), C.byref(nz_launch))
+    launches = lib.decon_launch_count() - n0
+    ms = e0.elapsed_time(e1)
+    if ws > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    clk = clocks.stop()
+    info = runner.result()
+    value = n_obj * K * ws / (ms / 1e3)
+
+    # roofline of the axial pass
+    z_bytes = zpass_bytes(OBJ, conv.fft_shape)
+    z_ms = ms_z.value / max(nz_launch.value, 1)
+    hbm, src = peaks()
+    achieved = z_bytes / (z_ms / 1e3) / 1e9
+    traffic = profile_traffic("zotf_pdhg_128x256x256")
+
+    # --- RL at the same size (fused path) -----------------------------------
+    psf_rl, obs_rl = rl_inputs(D)
+    y = to_device(obs_rl)
+    c_rl = D.LinearFFTConvolver(psf_rl, OBJ)
+    x = torch.empty_like(y)
+    sens = torch.empty_like(y)
+    ratio = torch.empty_like(y)
+    s = _lib.stream_ptr()
+    _lib.call("decon_rl_setup", c_rl.plan, _lib.ptr(y), C.c_float(10.0), None, _lib.ptr(x),
+              _lib.ptr(sens), s)
+    for _ in range(W):
+        _lib.call("decon_rl_iteration", c_rl.plan, _lib.ptr(y), C.c_float(10.0), _lib.ptr(sens),
+                  _lib.ptr(x), _lib.ptr(ratio), None, s)
+    torch.cuda.synchronize()
+    r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lib.decon_profile_start(_lib.PROF_ZOTF)
+    r0.record(st)
+    for _ in range(K):
+        _lib.call("decon_rl_iteration", c_rl.plan, _lib.ptr(y), C.c_float(10.0), _lib.ptr(sens),
+                  _lib.ptr(x), _lib.ptr(ratio), None, s)
+    r1.record(st)
+    torch.cuda.synchronize()
+    ms_rz, n_rz = C.c_double(), C.c_int64()
+    lib.decon_profile_stop(C.byref(ms_rz), C.byref(n_rz))
+    ms_rl = r0.elapsed_time(r1)
+    rl_value = n_obj * K * ws / (ms_rl / 1e3)
+    fz, fy, fx = c_rl.fft_shape
+    hx = fx // 2 + 1
+    rl_model_bytes = 28 * n_obj + 8 * 8 * OBJ[0] * fy * hx + 2 * 8 * fz * fy * hx
+
+    # --- e2e through the public API with host buffers ------------------------
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = D.solve_pdhg_mlx(obs, psf, alpha=1e-3, regularization="hessian", sampling_factors=2.0,
+                           spacing=SPACING_PD, background=5.0, num_iter=K, tol=0.0)
+    out = res.restored.cpu().numpy()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_value = n_obj * res.iterations * ws / e2e_s
+
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "voxel-iter/s",
+        "n_gpus": ws,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": ms / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded filament+bead phantom, widefield PSF with aberrations, Poisson)",
+        "config": {
+            "workload": "hessian_pdhg_sampling2_object128x256x256_data64x128x128",
+            "object_shape": list(OBJ), "data_shape": list(DATA),
+            "fft_shape": list(conv.fft_shape), "alpha": 1e-3, "norm": "L1",
+            "step": "one PDHG iteration (1 forward + 1 adjoint A, Hessian dual/primal, FP64 step)",
+            "l2": "inputs larger than L2 (OTF 285 MB, Hessian dual 201 MB per iteration)",
+            "parallelism": f"replicas x{ws}",
+        },
+        "roofline": {
+            "bound": "hbm", "kernel": "k_colfft axial FFT x OTF x IFFT",
+            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "peak_source": src, "traffic": traffic, "algorithmic_bytes_per_launch": z_bytes,
+            "launch_ms": z_ms, "launches": nz_launch.value,
+        },
+        "e2e": {"value": e2e_value, "unit": "voxel-iter/s",
+                "h2d_bytes_per_step": int((obs.nbytes + psf.nbytes) / max(res.iterations, 1)),
+                "d2h_bytes_per_step": int(out.nbytes / max(res.iterations, 1)),
+                "seconds": e2e_s, "iterations": res.iterations,
+                "note": "solve_pdhg_mlx(numpy in, numpy out) incl. OTF set-up; bytes amortised per iteration"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "rl": {"value": rl_value, "unit": "voxel-iter/s", "ms_per_iter": ms_rl / K,
+               "model_bytes_per_iter": rl_model_bytes,
+               "hbm_frac_model": rl_model_bytes / (ms_rl / K / 1e3) / 1e9 / hbm,
+               "zpass_ms": ms_rz.value / max(n_rz.value, 1),
+               "workload": "rl_object128x256x256_beads_shells"},
+        "pdhg_iterations_run": info[1],
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_pdhg(psf, obs, iters=1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle (reference restatement) timing
+# ---------------------------------------------------------------------------
+
+
+def _oracle_pdhg_setup(psf, obs, workers):
+    from oracle import ops, solvers
+
+    ops.set_fft_workers(workers)
+    y = obs.astype(np.float32)
+    conv = ops.LinearFFTConvolver(psf, OBJ, dtype=np.float32)
+    A = ops.compose(ops.FractionalAreaDownsample(2.0, dtype=np.float32), conv)
+    reg = solvers.Regularizer("hessian", 3, solvers.spacing_ratio(SPACING_PD, 3), "L1", np.float32)
+    x0 = np.maximum(A.adjoint(y), np.float32(0))
+    return solvers, y, A, reg, x0
+
+
+def _oracle_iter(solvers, y, A, reg, x0):
+    return solvers._pdhg_loop(y, A, reg, x0, 1e-3, "poisson", 1, 5.0, 0.99, 0.5, 10, 0.0, 20, 5,
+                              np.float32, generic=False)
+
+
+def cpu_baseline_pdhg(psf, obs, iters=1):
+    workers = len(os.sched_getaffinity(0))
+    solvers, y, A, reg, x0 = _oracle_pdhg_setup(psf, obs, workers)
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        _oracle_iter(solvers, y, A, reg, x0)
+    dt = (time.perf_counter() - t0) / iters
+    return {"value": int(np.prod(OBJ)) / dt, "unit": "voxel-iter/s", "cores": workers,
+            "kind": "port",
+            "sample": f"{iters} full PDHG iteration(s) of the NumPy oracle at 128x256x256 "
+                      f"(3 forward + 1 adjoint convolution, as the reference), scipy.fft with "
+                      f"{workers} threads; set-up excluded", "seconds_per_iter": dt}
+
+
+def run_reference(args, ws, rank, local):
+    if rank != 0:
+        return
+    import torch
+    import deconlib_b200.deconvolution as D
+
+    if torch.cuda.is_available():
+        psf, obs = pdhg_inputs(D)
+    else:  # inputs only; the reference arm itself is CPU
+        from deconlib_b200 import synth
+        from oracle import ops
+
+        psf, truth = synth.pdhg_workload(OBJ, SPACING_PD, seed=2)
+        fwd = ops.compose(ops.FractionalAreaDownsample(2.0, in_shape=OBJ),
+                          ops.LinearFFTConvolver(psf, OBJ))
+        obs = synth.poisson_observation(fwd.forward(truth), 500.0, 5.0, np.random.default_rng(3))
+    workers = len(os.sched_getaffinity(0))
+    solvers, y, A, reg, x0 = _oracle_pdhg_setup(psf, obs, workers)
+    W = min(args.warmup, 1)
+    K = max(1, min(args.steps, 3))
+    for _ in range(W):
+        _oracle_iter(solvers, y, A, reg, x0)
+    t0 = time.perf_counter()
+    for _ in range(K):
+        _oracle_iter(solvers, y, A, reg, x0)
+    dt = time.perf_counter() - t0
+    value = int(np.prod(OBJ)) * K / dt
+    sample = (f"{K} timed PDHG iteration(s) (+{W} warm-up) of the NumPy restatement of the "
+              f"reference at 128x256x256, scipy.fft with {workers} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "voxel-iter/s",
+            "n_gpus": ws, "steps": K, "warmup": W, "ms_per_step": dt / K * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": "hessian_pdhg_sampling2_object128x256x256_data64x128x128"},
+            "cpu_baseline": {"value": value, "unit": "voxel-iter/s", "cores": workers,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "voxel-iter/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, ws, rank, local)
+    else:
+        run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -29,6 +29,7 @@ _dp = C.POINTER(C.c_double)
 _SIGS = {
     "decon_last_error": (C.c_char_p, []),
     "decon_version": (C.c_int, []),
+    "decon_launch_count": (_i64, []),
     "decon_next_smooth": (_i64, [_i64]),
     "decon_fast_padded_shape": (C.c_int, [C.c_int, _i64p, _i64p, _i64p, _i64p]),
     "decon_conv_create": (C.c_int, [_p, _i64p, _i64p, _i64p, C.c_int, _p, C.POINTER(_p)]),
@@ -75,7 +76,11 @@ _SIGS = {
                                   C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _dp, _dp, _dp,
                                   _dp, _p]),
     "decon_pdhg_set_stop": (C.c_int, [_p, C.c_int, _p]),
+    "decon_profile_start": (C.c_int, [C.c_int]),
+    "decon_profile_stop": (C.c_int, [_dp, _i64p]),
 }
+
+PROF_XR2C, PROF_COL, PROF_ZOTF, PROF_XC2R = 1, 2, 4, 8
 
 _lib = None
 _lock = threading.Lock()

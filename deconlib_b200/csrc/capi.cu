@@ -1,5 +1,6 @@
 // C ABI: error state, FFT sizing, convolution plans and the fused
 // Richardson-Lucy entry points (include/decon_b200.h).
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -12,6 +13,9 @@
 namespace dk {
 
 static thread_local std::string g_err;
+static std::atomic<long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_error(const char* fmt, ...) {
     char buf[1024];
@@ -110,6 +114,8 @@ extern "C" {
 const char* decon_last_error(void) { return g_err.c_str(); }
 
 int decon_version(void) { return 100; }
+
+int64_t decon_launch_count(void) { return (int64_t)g_launches.load(); }
 
 int64_t decon_next_smooth(int64_t n) {
     int64_t m = n < 1 ? 1 : n;

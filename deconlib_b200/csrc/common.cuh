@@ -25,8 +25,13 @@ int fail(int code, const char* fmt, ...);
                               cudaGetErrorString(e_), __FILE__, __LINE__);                \
     } while (0)
 
+// Count of kernels launched by the library (decon_launch_count), for the
+// benchmark's launch accounting.
+void count_launch();
+
 #define DK_LAUNCHED()                                                                     \
     do {                                                                                  \
+        ::dk::count_launch();                                                             \
         cudaError_t e_ = cudaGetLastError();                                              \
         if (e_ != cudaSuccess)                                                            \
             return ::dk::fail(DECON_ERR_CUDA, "kernel launch failed: %s (%s:%d)",         \

@@ -341,7 +341,17 @@ static void* pick_col(int L) {
     return (void*)k_colfft<0>;
 }
 
-static int launch(void* fn, int64_t nblk, int nthr, size_t smem, cudaStream_t st, void* args) {
+// Kernel-class timing (decon_profile_start / _stop): CUDA events recorded
+// on the launching stream around every launch of the selected classes.
+struct ProfState {
+    int mask = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+    size_t used = 0;
+};
+static ProfState g_prof;
+
+static int launch(void* fn, int64_t nblk, int nthr, size_t smem, cudaStream_t st, void* args,
+                  int cls) {
     if (smem > 48 * 1024) {
         // idempotent; cheap compared with the launch
         DK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -349,9 +359,50 @@ static int launch(void* fn, int64_t nblk, int nthr, size_t smem, cudaStream_t st
     if (nblk <= 0) return DECON_OK;
     if (nblk > 0x7fffffffLL) return fail(DECON_ERR_UNSUPPORTED, "grid too large");
     void* params[] = {args};
+    const bool prof = (g_prof.mask & cls) != 0;
+    if (prof) {
+        if (g_prof.used == g_prof.ev.size()) {
+            cudaEvent_t a, b;
+            DK_CUDA(cudaEventCreate(&a));
+            DK_CUDA(cudaEventCreate(&b));
+            g_prof.ev.emplace_back(a, b);
+        }
+        DK_CUDA(cudaEventRecord(g_prof.ev[g_prof.used].first, st));
+    }
     DK_CUDA(cudaLaunchKernel(fn, dim3((unsigned)nblk), dim3(nthr), params, smem, st));
+    count_launch();
+    if (prof) {
+        DK_CUDA(cudaEventRecord(g_prof.ev[g_prof.used].second, st));
+        ++g_prof.used;
+    }
     return DECON_OK;
 }
+
+}  // namespace dk
+
+extern "C" int decon_profile_start(int class_mask) {
+    dk::g_prof.mask = class_mask;
+    dk::g_prof.used = 0;
+    return DECON_OK;
+}
+
+extern "C" int decon_profile_stop(double* ms_total, int64_t* launches) {
+    using namespace dk;
+    double tot = 0.0;
+    for (size_t i = 0; i < g_prof.used; ++i) {
+        DK_CUDA(cudaEventSynchronize(g_prof.ev[i].second));
+        float ms = 0.f;
+        DK_CUDA(cudaEventElapsedTime(&ms, g_prof.ev[i].first, g_prof.ev[i].second));
+        tot += ms;
+    }
+    if (ms_total) *ms_total = tot;
+    if (launches) *launches = (int64_t)g_prof.used;
+    g_prof.mask = 0;
+    g_prof.used = 0;
+    return DECON_OK;
+}
+
+namespace dk {
 
 int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cval, float bg,
                 int64_t nz_rows, float2* out, cudaStream_t st) {
@@ -389,7 +440,7 @@ int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cva
         case PRO_RLINIT: fn = pick_xr2c<PRO_RLINIT>(a.ax.L); break;
         default: return fail(DECON_ERR_VALUE, "bad prologue %d", pro);
     }
-    return launch(fn, nblk, nthr, smem, st, &a);
+    return launch(fn, nblk, nthr, smem, st, &a, PROF_XR2C);
 }
 
 int launch_col(const ConvPlan& p, const Axis& ax, int T, int mode, const float2* src,
@@ -415,7 +466,8 @@ int launch_col(const ConvPlan& p, const Axis& ax, int T, int mode, const float2*
     const int nthr = threads_for(T, ax);
     const int64_t nblk = nouter * a.ntiles;
     const size_t smem = (size_t)T * ax.L * sizeof(float2);
-    return launch(pick_col(ax.L), nblk, nthr, smem, st, &a);
+    return launch(pick_col(ax.L), nblk, nthr, smem, st, &a,
+                  (mode == COL_OTF || mode == COL_OTF_CONJ) ? PROF_ZOTF : PROF_COL);
 }
 
 int launch_xc2r(const ConvPlan& p, int epi, const float2* in, Win3 win, float* out,
@@ -451,7 +503,7 @@ int launch_xc2r(const ConvPlan& p, int epi, const float2* in, Win3 win, float* o
         case EPI_PRED: fn = pick_xc2r<EPI_PRED>(a.ax.L); break;
         default: return fail(DECON_ERR_VALUE, "bad epilogue %d", epi);
     }
-    return launch(fn, nblk, nthr, smem, st, &a);
+    return launch(fn, nblk, nthr, smem, st, &a, PROF_XC2R);
 }
 
 // Forward spectrum: x (window in N-space) -> S2 (after the Y pass).

@@ -24,6 +24,8 @@ inline Win3 full_window(const int64_t* N) { return Win3{N[0], N[1], N[2], 0, 0, 
 enum Prologue { PRO_ARRAY = 0, PRO_CONST = 1, PRO_KERNEL = 2, PRO_RLINIT = 3 };
 enum Epilogue { EPI_STORE = 0, EPI_RL_RATIO = 1, EPI_RL_UPDATE = 2, EPI_PRED = 3 };
 enum ColMode { COL_FWD = 0, COL_INV = 1, COL_OTF = 2, COL_OTF_CONJ = 3 };
+// kernel classes for decon_profile_start (bit mask)
+enum ProfClass { PROF_XR2C = 1, PROF_COL = 2, PROF_ZOTF = 4, PROF_XC2R = 8 };
 
 struct XR2CArgs {
     const float* in;

@@ -299,96 +299,130 @@ def _norm_code(norm):
     return 0 if norm == "L1" else 1
 
 
-def _pdhg_loop(data, A, reg, x0, alpha, loss_type, num_iter, background, delta, eta,
-               eval_interval, tol, min_iter, patience, verbose, callback, generic):
-    s = stream()
-    bg = float(background)
-    lcode = 0 if loss_type == "poisson" else 1
-    ncode = _norm_code(reg.norm)
-    step_scale = 0.99 / (A.operator_norm_sq + reg.operator_norm_sq) ** 0.5
-    st = _State(num_iter, step_scale, delta, eta, tol, min_iter, patience)
-    h = st.h
-    ncomp = reg.output_components
-    X = [x0.contiguous(), x0.clone()]
-    ax0 = to_device(A.forward(X[0])).clone()
-    if tuple(ax0.shape) != tuple(data.shape):
-        raise ValueError(
-            f"blur_op maps the solution to {tuple(ax0.shape)} but observed is {tuple(data.shape)}"
-        )
-    AX = [ax0, ax0.clone()]
-    m = data.numel()
-    n = x0.numel()
-    y1 = zeros(data.shape)
-    y2 = zeros((ncomp,) + tuple(x0.shape))
-    xbar = empty(x0.shape)
-    dxb = empty(x0.shape)
-    want_loss_each = generic and (verbose or callback is not None)
-    stopped_at = None
-    for k in range(num_iter):
-        xc, xp = X[k % 2], X[(k + 1) % 2]
-        axc, axp = AX[k % 2], AX[(k + 1) % 2]
-        _lib.call("decon_pdhg_dual_data", h, _lib.ptr(y1), _lib.ptr(axc), _lib.ptr(axp),
-                  _lib.ptr(data), C.c_float(bg), lcode, m, s)
-        aty = to_device(A.adjoint(y1))
-        _lib.call("decon_pdhg_xbar", h, _lib.ptr(xc), _lib.ptr(xp), _lib.ptr(xbar), n, s)
-        lxb = to_device(reg.forward(xbar))
-        _lib.call("decon_pdhg_dual_reg", h, _lib.ptr(y2), _lib.ptr(lxb), C.c_float(alpha), ncode,
-                  ncomp, n, s)
-        lty = to_device(reg.adjoint(y2))
+class PDHGRunner:
+    """The shared iteration of both entry points (pdhg_mlx.py:717-900 and
+    :1066-1221), split into set-up / ``iterate`` / ``result`` so a caller
+    (the benchmark, the serving loop) can time or interleave iterations.
+
+    Buffers: x and A x are double-buffered (slot k % 2 holds x_k, the other
+    x_{k-1}); iteration k writes x_{k+1} over x_{k-1}.  x_bar and A x_bar are
+    never stored: they are formed from the two slots inside the kernels."""
+
+    def __init__(self, data, A, reg, x0, alpha, loss_type, num_iter, background, delta, eta,
+                 eval_interval, tol, min_iter, patience, verbose=False, callback=None,
+                 generic=False):
+        self.s = stream()
+        self.data, self.A, self.reg = data, A, reg
+        self.alpha = float(alpha)
+        self.bg = float(background)
+        self.lcode = 0 if loss_type == "poisson" else 1
+        self.ncode = _norm_code(reg.norm)
+        self.num_iter, self.eval_interval = int(num_iter), int(eval_interval)
+        self.tol, self.patience = tol, patience
+        self.verbose, self.callback, self.generic = verbose, callback, generic
+        step_scale = 0.99 / (A.operator_norm_sq + reg.operator_norm_sq) ** 0.5
+        self.state = _State(num_iter, step_scale, delta, eta, tol, min_iter, patience)
+        self.h = self.state.h
+        self.ncomp = reg.output_components
+        self.X = [x0.contiguous(), x0.clone()]
+        ax0 = to_device(A.forward(self.X[0])).clone()
+        if tuple(ax0.shape) != tuple(data.shape):
+            raise ValueError(
+                f"blur_op maps the solution to {tuple(ax0.shape)} but observed is "
+                f"{tuple(data.shape)}"
+            )
+        self.AX = [ax0, ax0.clone()]
+        self.m = data.numel()
+        self.n = x0.numel()
+        self.y1 = zeros(data.shape)
+        self.y2 = zeros((self.ncomp,) + tuple(x0.shape))
+        self.xbar = empty(x0.shape)
+        self.dxb = empty(x0.shape)
+        self.want_loss_each = generic and (verbose or callback is not None)
+        self.stopped_at = None
+        self.k = 0
+
+    def iterate(self) -> bool:
+        """Queue iteration k; returns False once the solve has stopped."""
+        k, s, h, A, reg = self.k, self.s, self.h, self.A, self.reg
+        if k >= self.num_iter or self.stopped_at is not None:
+            return False
+        m, n = self.m, self.n
+        xc, xp = self.X[k % 2], self.X[(k + 1) % 2]
+        axc, axp = self.AX[k % 2], self.AX[(k + 1) % 2]
+        _lib.call("decon_pdhg_dual_data", h, _lib.ptr(self.y1), _lib.ptr(axc), _lib.ptr(axp),
+                  _lib.ptr(self.data), C.c_float(self.bg), self.lcode, m, s)
+        aty = to_device(A.adjoint(self.y1))
+        _lib.call("decon_pdhg_xbar", h, _lib.ptr(xc), _lib.ptr(xp), _lib.ptr(self.xbar), n, s)
+        lxb = to_device(reg.forward(self.xbar))
+        _lib.call("decon_pdhg_dual_reg", h, _lib.ptr(self.y2), _lib.ptr(lxb), C.c_float(self.alpha),
+                  self.ncode, self.ncomp, n, s)
+        lty = to_device(reg.adjoint(self.y2))
         _lib.call("decon_pdhg_primal", h, _lib.ptr(xc), _lib.ptr(aty), _lib.ptr(lty), _lib.ptr(xp),
                   n, s)
         xn = xp
         axn = to_device(A.forward(xn))
-        _lib.call("decon_pdhg_sub", h, _lib.ptr(xn), _lib.ptr(xc), _lib.ptr(dxb), n, s)
-        ldx = to_device(reg.forward(dxb))
+        _lib.call("decon_pdhg_sub", h, _lib.ptr(xn), _lib.ptr(xc), _lib.ptr(self.dxb), n, s)
+        ldx = to_device(reg.forward(self.dxb))
         _lib.call("decon_pdhg_dk", h, _lib.ptr(axn), _lib.ptr(axc), m, _lib.ptr(ldx), ldx.numel(), s)
         _lib.call("decon_pdhg_step", h, s)
-        AX[(k + 1) % 2] = axn
-        do_loss = want_loss_each or ((not generic) and (k + 1) % eval_interval == 0)
+        self.AX[(k + 1) % 2] = axn
+        do_loss = self.want_loss_each or ((not self.generic) and (k + 1) % self.eval_interval == 0)
         if do_loss:
             lx = to_device(reg.forward(xn))
-            _lib.call("decon_pdhg_loss", h, _lib.ptr(axn), _lib.ptr(data), C.c_float(bg), lcode, m,
-                      _lib.ptr(lx), ncode, ncomp, n, C.c_double(alpha), k, s)
-        sync_now = callback is not None or (verbose and do_loss) or (k + 1) % _CHUNK == 0
-        if sync_now:
-            info = st.read(hist=bool(verbose and do_loss) or (generic and callback is not None))
+            _lib.call("decon_pdhg_loss", h, _lib.ptr(axn), _lib.ptr(self.data), C.c_float(self.bg),
+                      self.lcode, m, _lib.ptr(lx), self.ncode, self.ncomp, n,
+                      C.c_double(self.alpha), k, s)
+        self.k = k + 1
+        cb, verbose = self.callback, self.verbose
+        if cb is not None or (verbose and do_loss) or self.k % _CHUNK == 0:
+            info = self.state.read(hist=bool(verbose and do_loss) or (self.generic and cb is not None))
             # Stop here if the solve ended before this iteration, or broke on
             # convergence at it (the reference breaks before the loss and the
             # callback, pdhg_mlx.py:812-833); reaching num_iter still runs them.
             ended_before = info["stop"] and info["final_iter"] < k + 1
             converged_here = info["converged"] and info["final_iter"] == k + 1
             if ended_before or converged_here:
-                stopped_at = info["final_iter"]
+                self.stopped_at = info["final_iter"]
                 if verbose and info["converged"]:
-                    print(f"Converged at iteration {stopped_at}: rel_change="
-                          f"{info['rel_hist'][stopped_at - 1] if info['rel_hist'] is not None else float('nan'):.2e}"
-                          f" < tol={tol:.2e} for {patience} consecutive iterations")
-                break
-            if verbose and do_loss and (not generic or (k + 1) % eval_interval == 0):
+                    rel = info["rel_hist"][self.stopped_at - 1] if info["rel_hist"] is not None else float("nan")
+                    print(f"Converged at iteration {self.stopped_at}: rel_change={rel:.2e} "
+                          f"< tol={self.tol:.2e} for {self.patience} consecutive iterations")
+                return False
+            if verbose and do_loss and (not self.generic or self.k % self.eval_interval == 0):
                 print(f"Iter {k + 1:4d}: loss={info['loss_hist'][k]:.4e}, "
                       f"tau={info['tau']:.4e}, sigma={info['sigma']:.4e}")
-            if callback is not None:
-                if generic:
-                    callback(k, xn, float(info["loss_hist"][k]))
-                elif callback(k, xn):
+            if cb is not None:
+                if self.generic:
+                    cb(k, xn, float(info["loss_hist"][k]))
+                elif cb(k, xn):
                     _lib.call("decon_pdhg_set_stop", h, k + 1, s)
-                    stopped_at = k + 1
-                    break
-    info = st.read(hist=True)
-    final_iter = info["final_iter"] if stopped_at is None else stopped_at
-    converged = info["converged"]
-    x = X[final_iter % 2] if num_iter > 0 else X[0]
-    taus = [float(v) for v in info["tau_hist"][:final_iter]]
-    sigmas = [float(v) for v in info["sigma_hist"][:final_iter]]
-    lh = info["loss_hist"]
-    if generic:
-        loss_k = [k for k in range(final_iter)] if want_loss_each else []
-    else:
-        loss_k = [k for k in range(final_iter) if (k + 1) % eval_interval == 0]
-    if converged:
-        loss_k = [k for k in loss_k if k != final_iter - 1]
-    losses = [float(lh[k]) for k in loss_k]
-    return x, final_iter, converged, taus, sigmas, losses, y1, y2
+                    self.stopped_at = k + 1
+                    return False
+        return True
+
+    def run(self):
+        while self.iterate():
+            pass
+        return self
+
+    def result(self):
+        info = self.state.read(hist=True)
+        final_iter = info["final_iter"] if self.stopped_at is None else self.stopped_at
+        final_iter = min(final_iter, self.k) if self.num_iter > 0 else 0
+        converged = info["converged"]
+        x = self.X[final_iter % 2]
+        taus = [float(v) for v in info["tau_hist"][:final_iter]]
+        sigmas = [float(v) for v in info["sigma_hist"][:final_iter]]
+        lh = info["loss_hist"]
+        if self.generic:
+            loss_k = list(range(final_iter)) if self.want_loss_each else []
+        else:
+            loss_k = [k for k in range(final_iter) if (k + 1) % self.eval_interval == 0]
+        if converged:
+            loss_k = [k for k in loss_k if k != final_iter - 1]
+        losses = [float(lh[k]) for k in loss_k]
+        return x, final_iter, converged, taus, sigmas, losses
 
 
 def solve_pdhg_mlx(observed, psf, alpha: float = 0.01,
@@ -446,9 +480,9 @@ def solve_pdhg_mlx(observed, psf, alpha: float = 0.01,
     else:
         x0 = to_device(blur_op.adjoint(data)) if (sampling_factors is not None or bin_factors is not None) else data.clone()
         x0 = prox_nonneg(x0)
-    x, fi, cv, taus, sigmas, losses, _, _ = _pdhg_loop(
+    x, fi, cv, taus, sigmas, losses = PDHGRunner(
         data, blur_op, reg, x0, alpha, loss_type, num_iter, background, delta, eta, eval_interval,
-        tol, min_iter, patience, verbose, callback, generic=False)
+        tol, min_iter, patience, verbose, callback, generic=False).run().result()
     return MLXDeconvolutionResult(
         restored=x, iterations=fi, loss_history=losses, converged=cv, tau_history=taus,
         sigma_history=sigmas,
@@ -487,9 +521,9 @@ def solve_pdhg_with_operator(observed, blur_op: LinearOperator, alpha: float = 0
     else:
         x0 = fill(empty(solution_shape), 0.01)
     x0 = prox_nonneg(x0)
-    x, fi, cv, taus, sigmas, losses, _, _ = _pdhg_loop(
+    x, fi, cv, taus, sigmas, losses = PDHGRunner(
         data, blur_op, reg, x0, alpha, loss_type, num_iter, background, delta, eta, eval_interval,
-        tol, min_iter, patience, verbose, callback, generic=True)
+        tol, min_iter, patience, verbose, callback, generic=True).run().result()
     return MLXDeconvolutionResult(
         restored=x, iterations=fi, loss_history=losses, converged=cv, tau_history=taus,
         sigma_history=sigmas,

@@ -41,6 +41,8 @@ extern "C" {
 const char* decon_last_error(void);
 /* Library ABI version (major * 10000 + minor * 100 + patch). */
 int decon_version(void);
+/* Kernels launched by this library since load (benchmark accounting). */
+int64_t decon_launch_count(void);
 
 /* ---- FFT sizing (deconvolution/linops_mlx.py:956-1032) ---------------- */
 
@@ -230,6 +232,19 @@ int64_t decon_reduce_workspace_bytes(void);
  * (pdhg_mlx.py:750,759,805-809; rl_mlx.py:77-80,130). */
 int decon_reduce(const float* a, const float* b, int64_t n, int op, double* out, void* workspace,
                  void* stream);
+
+/* ---- kernel timing (no reference counterpart: measurement support) ------ */
+
+#define DECON_PROF_XR2C 1 /* X R2C pass              */
+#define DECON_PROF_COL 2  /* Y / inverse-Y passes    */
+#define DECON_PROF_ZOTF 4 /* axial FFT x OTF x IFFT  */
+#define DECON_PROF_XC2R 8 /* X C2R pass + epilogue   */
+/* Records CUDA events on the launching stream around every launch of the
+ * selected FFT pass classes until decon_profile_stop, which synchronises,
+ * returns the summed kernel time (ms) and launch count, and disables timing.
+ * Process-wide, not thread-safe; for benchmarks. */
+int decon_profile_start(int class_mask);
+int decon_profile_stop(double* ms_total, int64_t* launches);
 
 #ifdef __cplusplus
 }

@@ -23,6 +23,32 @@ import numpy as np
 
 SQRT2 = math.sqrt(2.0)
 
+# FFT backend: NumPy's pocketfft (single thread) by default; set_fft_workers(n)
+# switches to scipy.fft (the same pocketfft algorithm) with n host threads,
+# which the timed CPU baseline uses to give the reference every core.
+_WORKERS = 1
+
+
+def set_fft_workers(n: int) -> None:
+    global _WORKERS
+    _WORKERS = max(1, int(n))
+
+
+def _rfftn(x):
+    if _WORKERS > 1:
+        import scipy.fft as sf
+
+        return sf.rfftn(x, workers=_WORKERS)
+    return np.fft.rfftn(x)
+
+
+def _irfftn(x, s):
+    if _WORKERS > 1:
+        import scipy.fft as sf
+
+        return sf.irfftn(x, s=s, workers=_WORKERS)
+    return np.fft.irfftn(x, s=s)
+
 
 def _c(dtype):
     return np.complex64 if np.dtype(dtype) == np.float32 else np.complex128
@@ -327,14 +353,14 @@ class FFTConvolver:
         self.dtype = dtype
         if normalize:
             k = k / np.sum(k)
-        self.otf = np.fft.rfftn(k).astype(_c(dtype))
+        self.otf = _rfftn(k).astype(_c(dtype))
         self.operator_norm_sq = float(np.max(np.abs(self.otf) ** 2))
 
     def forward(self, x):
-        return np.fft.irfftn(np.fft.rfftn(x) * self.otf, s=self.shape).astype(self.dtype)
+        return _irfftn(_rfftn(x) * self.otf, self.shape).astype(self.dtype)
 
     def adjoint(self, y):
-        return np.fft.irfftn(np.fft.rfftn(y) * np.conj(self.otf), s=self.shape).astype(self.dtype)
+        return _irfftn(_rfftn(y) * np.conj(self.otf), self.shape).astype(self.dtype)
 
 
 class LinearFFTConvolver:
