@@ -403,6 +403,32 @@ def run_reference(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_conv_only(args):
+    """Forward + adjoint LinearFFTConvolver at 128x256x256 (canvas 256x512x512), seeded
+    random PSF-like kernel; prints the device time per convolution pair."""
+    import torch
+
+    import deconlib_b200.deconvolution as D
+
+    rng = np.random.default_rng(0)
+    k = (rng.random(OBJ, dtype=np.float32) ** 8).astype(np.float32)
+    from deconlib_b200.deconvolution._device import to_device
+
+    x = to_device(rng.random(OBJ, dtype=np.float32))
+    c = D.LinearFFTConvolver(k, OBJ)
+    for _ in range(args.warmup):
+        c.adjoint(c.forward(x))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        c.adjoint(c.forward(x))
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "conv", "fft_shape": list(c.fft_shape),
+                      "ms_per_fwd_adj_pair": e0.elapsed_time(e1) / args.steps}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -410,10 +436,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", choices=["full", "conv"], default="full",
+                    help="conv: only warm-up + steps forward/adjoint convolutions of the PDHG "
+                         "operator (a small, fixed launch sequence for ncu captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     ws, rank, local = dist_setup()
+    if args.mode == "conv":
+        run_conv_only(args)
+        return
     if args.impl == "reference":
         run_reference(args, ws, rank, local)
     else:

@@ -30,6 +30,7 @@ _SIGS = {
     "decon_last_error": (C.c_char_p, []),
     "decon_version": (C.c_int, []),
     "decon_launch_count": (_i64, []),
+    "decon_device_status": (C.c_int, [_p]),
     "decon_next_smooth": (_i64, [_i64]),
     "decon_fast_padded_shape": (C.c_int, [C.c_int, _i64p, _i64p, _i64p, _i64p]),
     "decon_conv_create": (C.c_int, [_p, _i64p, _i64p, _i64p, C.c_int, _p, C.POINTER(_p)]),

@@ -1,6 +1,7 @@
 // C ABI: error state, FFT sizing, convolution plans and the fused
 // Richardson-Lucy entry points (include/decon_b200.h).
 #include <atomic>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -217,6 +218,22 @@ static int conv_create_impl(const float* kernel, const int64_t kshape[3],
         free_plan(p);
         delete p;
         return st;
+    }
+    // TMA tensor maps for the strided column passes (power-of-two lengths
+    // <= 512, 16-column tiles).  DECON_NO_TMA=1 selects the plain-load kernels.
+    {
+        const bool allow = getenv("DECON_NO_TMA") == nullptr;
+        const int64_t P = p->P;
+        p->s1_box = (int)std::min<int64_t>(ny, 256);
+        p->s2y_box = (int)std::min<int64_t>(Fy, 256);
+        p->s2z_box = (int)std::min<int64_t>(nz, 256);
+        p->otf_box = (int)std::min<int64_t>(Fz, 256);
+        p->tma_y = allow && tma_length_ok(p->ax_y.L) && p->T_y == 16 &&
+                   encode_spectrum_map(&p->tm_s1_j1, p->s1, P, ny, nz, p->s1_box, 1) &&
+                   encode_spectrum_map(&p->tm_s2_j1, p->s2, P, Fy, nz, p->s2y_box, 1);
+        p->tma_z = allow && tma_length_ok(p->ax_z.L) && p->T_z == 16 &&
+                   encode_spectrum_map(&p->tm_s2_j2, p->s2, P, Fy, nz, 1, p->s2z_box) &&
+                   encode_spectrum_map(&p->tm_otf_z, p->otf, P, Fy, Fz, 1, p->otf_box);
     }
     // Kernel sum (FP64) for normalisation (linops_mlx.py:408-409).
     p->kdiv = 1.f;

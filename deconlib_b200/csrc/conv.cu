@@ -24,6 +24,7 @@
 #include <algorithm>
 
 #include "conv_impl.cuh"
+#include "tma.cuh"
 
 namespace dk {
 
@@ -179,6 +180,71 @@ __global__ void __launch_bounds__(kFftThreads) k_colfft(ColArgs a) {
     for (int q = tid; q < a.nout * T; q += blockDim.x) {
         const int j = q / T, tt = q - j * T;
         if (kx0 + tt < a.ncols) dst[(int64_t)j * a.dst_js + tt] = sm[phys(j, tt, T)];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// passes 2-4 on TMA: the same column transform with the tile moved by
+// cp.async.bulk.tensor (one elected thread issues the boxes; an mbarrier with
+// a bounded wait signals arrival; results leave through a TMA store).
+// Power-of-two lengths L <= 512 with 16-column tiles (128-byte rows), so the
+// shared-memory tile uses the TMA 128-byte swizzle layout (physw<1>).
+// ---------------------------------------------------------------------------
+
+
+template <int LS>
+__global__ void __launch_bounds__(kFftThreads, (LS >= 512 ? 1 : 2)) k_colfft_tma(const __grid_constant__ ColTmaArgs a) {
+    extern __shared__ unsigned char smraw[];
+    float2* sm = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
+    float2* so = sm + LS * 16;
+    __shared__ uint64_t bar;
+    const int tid = threadIdx.x;
+    const int o = blockIdx.x / a.ntiles;
+    const int c0 = (blockIdx.x - o * a.ntiles) * 32;  // float coordinate of the tile
+    const bool otf = a.mode == COL_OTF || a.mode == COL_OTF_CONJ;
+    const int nbox = (a.nin + a.src_box - 1) / a.src_box;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        fence_proxy_async_smem();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const uint32_t bytes = (uint32_t)(nbox * a.src_box * 128) + (otf ? (uint32_t)(LS * 128) : 0u);
+        mbar_expect_tx(&bar, bytes);
+        for (int i = 0; i < nbox; ++i) {
+            const int r0 = i * a.src_box;
+            if (a.src_jdim == 1) tma_load_3d(sm + r0 * 16, &a.src, c0, r0, o, &bar);
+            else tma_load_3d(sm + r0 * 16, &a.src, c0, o, r0, &bar);
+        }
+        if (otf)
+            for (int r0 = 0; r0 < LS; r0 += a.otf_box) tma_load_3d(so + r0 * 16, &a.otf, c0, o, r0, &bar);
+    }
+    // rows the boxes do not cover are the implicit zero padding
+    for (int q = nbox * a.src_box * 16 + tid; q < LS * 16; q += blockDim.x) sm[q] = make_float2(0.f, 0.f);
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0));
+    if (!ok) return;
+    const int t = tid & 15, jb = tid >> 4;
+    if (a.mode == COL_INV) {
+        fft_lines_pow2<LS, +1, 1, 1>(sm, 16, t, jb, a.tw, a.tws);
+    } else {
+        fft_lines_pow2<LS, -1, 1, 1>(sm, 16, t, jb, a.tw, a.tws);
+    }
+    if (otf) {
+        for (int q = tid; q < LS * 16; q += blockDim.x) {
+            const float2 w = so[q];
+            sm[q] = a.mode == COL_OTF ? cmul(sm[q], w) : cmulc(sm[q], w);
+        }
+        __syncthreads();
+        fft_lines_pow2<LS, +1, 1, 1>(sm, 16, t, jb, a.tw, a.tws);
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+        for (int r0 = 0; r0 < a.nout; r0 += a.dst_box) {
+            if (a.dst_jdim == 1) tma_store_3d(&a.dst, c0, r0, o, sm + r0 * 16);
+            else tma_store_3d(&a.dst, c0, o, r0, sm + r0 * 16);
+        }
+        tma_store_commit_and_wait();
     }
 }
 
@@ -380,6 +446,15 @@ static int launch(void* fn, int64_t nblk, int nthr, size_t smem, cudaStream_t st
 
 }  // namespace dk
 
+extern "C" int decon_device_status(void* stream) {
+    using namespace dk;
+    DK_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    int flag = 0;
+    DK_CUDA(cudaMemcpyFromSymbol(&flag, g_wait_timeout, sizeof(int)));
+    if (flag) return fail(DECON_ERR_TIMEOUT, "a bounded TMA wait gave up; results are invalid");
+    return DECON_OK;
+}
+
 extern "C" int decon_profile_start(int class_mask) {
     dk::g_prof.mask = class_mask;
     dk::g_prof.used = 0;
@@ -506,23 +581,106 @@ int launch_xc2r(const ConvPlan& p, int epi, const float2* in, Win3 win, float* o
     return launch(fn, nblk, nthr, smem, st, &a, PROF_XC2R);
 }
 
+static void* pick_col_tma(int L) {
+    switch (L) {
+        case 64: return (void*)k_colfft_tma<64>;
+        case 128: return (void*)k_colfft_tma<128>;
+        case 256: return (void*)k_colfft_tma<256>;
+        case 512: return (void*)k_colfft_tma<512>;
+        default: return nullptr;
+    }
+}
+
+bool tma_length_ok(int L) { return L == 64 || L == 128 || L == 256 || L == 512; }
+
+bool encode_spectrum_map(CUtensorMap* map, const float2* base, int64_t pitch, int64_t d1, int64_t d2,
+                         int b1, int b2) {
+    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        else
+            cudaGetLastError();
+    }
+    if (!enc) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)(2 * pitch), (cuuint64_t)d1, (cuuint64_t)d2};
+    cuuint64_t strides[2] = {(cuuint64_t)(2 * pitch * sizeof(float)),
+                             (cuuint64_t)(2 * pitch * sizeof(float) * d1)};
+    cuuint32_t box[3] = {32u, (cuuint32_t)b1, (cuuint32_t)b2};
+    cuuint32_t estr[3] = {1u, 1u, 1u};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float2*>(base), dims, strides,
+                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// One column pass on TMA.  src/dst/otf maps come from the plan.
+static int launch_col_tma(const ConvPlan& p, const Axis& ax, int mode, const CUtensorMap& src,
+                          int src_jdim, int src_box, int nin, const CUtensorMap& dst, int dst_jdim,
+                          int dst_box, int nout, int64_t nouter, cudaStream_t st) {
+    ColTmaArgs a;
+    memset(&a, 0, sizeof(a));
+    a.src = src;
+    a.dst = dst;
+    if (mode == COL_OTF || mode == COL_OTF_CONJ) a.otf = p.tm_otf_z;
+    a.nin = nin;
+    a.nout = nout;
+    a.ntiles = (int)cdiv(p.Hx, 16);
+    a.mode = mode;
+    a.src_jdim = src_jdim;
+    a.dst_jdim = dst_jdim;
+    a.src_box = src_box;
+    a.dst_box = dst_box;
+    a.otf_box = p.otf_box;
+    a.tw = ax.tw;
+    a.tws = ax.tws;
+    const int L = ax.L;
+    const int nthr = std::max(64, L / 2);
+    const bool otf = mode == COL_OTF || mode == COL_OTF_CONJ;
+    const size_t smem = 1024 + (size_t)L * 16 * sizeof(float2) * (otf ? 2 : 1);
+    return launch(pick_col_tma(L), nouter * a.ntiles, nthr, smem, st, &a,
+                  otf ? PROF_ZOTF : PROF_COL);
+}
+
 // Forward spectrum: x (window in N-space) -> S2 (after the Y pass).
 int spectrum_forward(const ConvPlan& p, int pro, const float* in, Win3 win, float cval, float bg,
                      cudaStream_t st) {
     const int64_t Nz = p.N[0], Ny = p.N[1], Fy = p.F[1], P = p.P;
     DK_TRY(launch_xr2c(p, pro, in, win, cval, bg, Nz, p.s1, st));
-    DK_TRY(launch_col(p, p.ax_y, p.T_y, COL_FWD, p.s1, Ny * P, P, (int)Ny, p.s2, Fy * P, P,
-                      (int)Fy, Nz, st));
+    if (p.tma_y) {
+        DK_TRY(launch_col_tma(p, p.ax_y, COL_FWD, p.tm_s1_j1, 1, p.s1_box, (int)Ny, p.tm_s2_j1, 1,
+                              p.s2y_box, (int)Fy, Nz, st));
+    } else {
+        DK_TRY(launch_col(p, p.ax_y, p.T_y, COL_FWD, p.s1, Ny * P, P, (int)Ny, p.s2, Fy * P, P,
+                          (int)Fy, Nz, st));
+    }
     return DECON_OK;
 }
 
 // Z pass (x OTF or conj OTF) and the inverse Y pass: S2 -> S1.
 int spectrum_filter_back(const ConvPlan& p, bool adjoint, cudaStream_t st) {
     const int64_t Nz = p.N[0], Ny = p.N[1], Fy = p.F[1], P = p.P;
-    DK_TRY(launch_col(p, p.ax_z, p.T_z, adjoint ? COL_OTF_CONJ : COL_OTF, p.s2, P, Fy * P,
-                      (int)Nz, p.s2, P, Fy * P, (int)Nz, Fy, st));
-    DK_TRY(launch_col(p, p.ax_y, p.T_y, COL_INV, p.s2, Fy * P, P, (int)Fy, p.s1, Ny * P, P,
-                      (int)Ny, Nz, st));
+    const int mode = adjoint ? COL_OTF_CONJ : COL_OTF;
+    if (p.tma_z) {
+        DK_TRY(launch_col_tma(p, p.ax_z, mode, p.tm_s2_j2, 2, p.s2z_box, (int)Nz, p.tm_s2_j2, 2,
+                              p.s2z_box, (int)Nz, Fy, st));
+    } else {
+        DK_TRY(launch_col(p, p.ax_z, p.T_z, mode, p.s2, P, Fy * P, (int)Nz, p.s2, P, Fy * P,
+                          (int)Nz, Fy, st));
+    }
+    if (p.tma_y) {
+        DK_TRY(launch_col_tma(p, p.ax_y, COL_INV, p.tm_s2_j1, 1, p.s2y_box, (int)Fy, p.tm_s1_j1, 1,
+                              p.s1_box, (int)Ny, Nz, st));
+    } else {
+        DK_TRY(launch_col(p, p.ax_y, p.T_y, COL_INV, p.s2, Fy * P, P, (int)Fy, p.s1, Ny * P, P,
+                          (int)Ny, Nz, st));
+    }
     return DECON_OK;
 }
 

@@ -2,6 +2,8 @@
 // C ABI (capi.cu) and the solver kernels.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 #include "fft_engine.cuh"
 
@@ -50,6 +52,14 @@ struct ColArgs {
     int64_t otf_js, otf_os;
 };
 
+struct ColTmaArgs {
+    CUtensorMap src, dst, otf;  // 64-byte aligned descriptors
+    int nin, nout, ntiles, mode;
+    int src_jdim, dst_jdim, src_box, dst_box, otf_box;
+    int tws;
+    const float2* tw;
+};
+
 struct XC2RArgs {
     const float2* in;
     int64_t P, Ny, Nx, nrows;
@@ -80,7 +90,15 @@ struct ConvPlan {
     float kdiv;
     double norm_sq;
     int device;
+    // TMA descriptors of the column passes (valid when tma_y / tma_z)
+    bool tma_y = false, tma_z = false;
+    CUtensorMap tm_s1_j1, tm_s2_j1, tm_s2_j2, tm_otf_z;
+    int s1_box = 0, s2y_box = 0, s2z_box = 0, otf_box = 0;
 };
+
+bool tma_length_ok(int L);
+bool encode_spectrum_map(CUtensorMap* map, const float2* base, int64_t pitch, int64_t d1, int64_t d2,
+                         int b1, int b2);
 
 int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cval, float bg,
                 int64_t nz_rows, float2* out, cudaStream_t st);

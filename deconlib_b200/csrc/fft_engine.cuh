@@ -36,6 +36,19 @@ struct Axis {
 
 __device__ __forceinline__ int phys(int j, int t, int T) { return j * T + (t ^ (j & (T - 1))); }
 
+// Layout selector.  SW = 0: the XOR swizzle above (any power-of-two T).
+// SW = 1: T = 16 lines whose rows are exactly 128 bytes, laid out as the TMA
+// 128-byte swizzle writes them: 16-byte chunk (t / 2) XOR (j mod 8).  Both
+// keep a warp's accesses to consecutive lines at one point conflict-free.
+template <int SW>
+__device__ __forceinline__ int physw(int j, int t, int T) {
+    if constexpr (SW == 0) {
+        return phys(j, t, T);
+    } else {
+        return j * 16 + ((((t >> 1) ^ (j & 7)) << 1) | (t & 1));
+    }
+}
+
 // multiply by -i (DIR < 0, forward) or +i (DIR > 0, inverse)
 template <int DIR>
 __device__ __forceinline__ float2 rot90(float2 a) {
@@ -142,9 +155,51 @@ __device__ __forceinline__ void dft7(float2* v) {
     v[4] = csub(t3, u3);
 }
 
+// v * W16^m for the fixed twiddles of the radix-16 codelet (c = cos, s = sin
+// of 2 pi m / 16); forward multiplies by c - i s, inverse by c + i s.
+template <int DIR>
+__device__ __forceinline__ float2 rot16(float2 v, float c, float s) {
+    return DIR < 0 ? make_float2(v.x * c + v.y * s, v.y * c - v.x * s)
+                   : make_float2(v.x * c - v.y * s, v.y * c + v.x * s);
+}
+
+// Radix-16 as 4 x 4: DFT4 over n2 of a[n1 + 4 n2], twiddle W16^(n1 k2),
+// DFT4 over n1; output X[k2 + 4 k1].
+template <int DIR>
+__device__ __forceinline__ void dft16(float2* v) {
+    constexpr float c1 = 0.9238795325112867f, s1 = 0.3826834323650898f;
+    constexpr float h = 0.7071067811865476f;
+    float2 y[4][4];
+#pragma unroll
+    for (int n1 = 0; n1 < 4; ++n1) {
+        float2 t[4] = {v[n1], v[n1 + 4], v[n1 + 8], v[n1 + 12]};
+        dft4<DIR>(t);
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) y[n1][k2] = t[k2];
+    }
+    // twiddles W16^(n1 k2), n1, k2 in 1..3: m = 1,2,3 / 2,4,6 / 3,6,9
+    y[1][1] = rot16<DIR>(y[1][1], c1, s1);
+    y[1][2] = rot16<DIR>(y[1][2], h, h);
+    y[1][3] = rot16<DIR>(y[1][3], s1, c1);
+    y[2][1] = rot16<DIR>(y[2][1], h, h);
+    y[2][2] = rot90<DIR>(y[2][2]);
+    y[2][3] = rot16<DIR>(y[2][3], -h, h);
+    y[3][1] = rot16<DIR>(y[3][1], s1, c1);
+    y[3][2] = rot16<DIR>(y[3][2], -h, h);
+    y[3][3] = rot16<DIR>(y[3][3], -c1, -s1);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) {
+        float2 t[4] = {y[0][k2], y[1][k2], y[2][k2], y[3][k2]};
+        dft4<DIR>(t);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) v[k2 + 4 * k1] = t[k1];
+    }
+}
+
 template <int R, int DIR>
 __device__ __forceinline__ void dft(float2* v) {
-    if constexpr (R == 2) dft2<DIR>(v[0], v[1]);
+    if constexpr (R == 16) dft16<DIR>(v);
+    else if constexpr (R == 2) dft2<DIR>(v[0], v[1]);
     else if constexpr (R == 3) dft3<DIR>(v);
     else if constexpr (R == 4) dft4<DIR>(v);
     else if constexpr (R == 5) dft5<DIR>(v);
@@ -153,7 +208,7 @@ __device__ __forceinline__ void dft(float2* v) {
 }
 
 // One Stockham stage.  (t, jb): this thread's line and first butterfly.
-template <int R, int DIR, int NS_STATIC>
+template <int R, int DIR, int NS_STATIC, int SW = 0>
 __device__ __forceinline__ void stage_body(float2* buf, int T, int L, int Ns_dyn, int t, int jb,
                                            int tpl, const float2* __restrict__ tw, int tws) {
     // ceil(32 / R) butterflies per thread cover L / R butterflies with
@@ -168,7 +223,7 @@ __device__ __forceinline__ void stage_body(float2* buf, int T, int L, int Ns_dyn
         const int j = jb + k * tpl;
         if (jb < tpl && j < nb) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[k][r] = buf[phys(j + r * nb, t, T)];
+            for (int r = 0; r < R; ++r) v[k][r] = buf[physw<SW>(j + r * nb, t, T)];
             if (Ns > 1) {
                 const int kk = j % Ns;
 #pragma unroll
@@ -187,7 +242,7 @@ __device__ __forceinline__ void stage_body(float2* buf, int T, int L, int Ns_dyn
         if (jb < tpl && j < nb) {
             const int base = (j / Ns) * Ns * R + (j % Ns);
 #pragma unroll
-            for (int r = 0; r < R; ++r) buf[phys(base + r * Ns, t, T)] = v[k][r];
+            for (int r = 0; r < R; ++r) buf[physw<SW>(base + r * Ns, t, T)] = v[k][r];
         }
     }
     __syncthreads();
@@ -220,17 +275,21 @@ __device__ __forceinline__ void fft_lines_dyn(float2* buf, int T, int t, int jb,
 }
 
 // Power-of-two lengths with the radix sequence fixed at compile time
-// (8, 8, ..., then 4 / 4,4 / 2): straight-line stages, shifts for j div Ns.
-// Matches plan_axis() so both paths use the same radices and twiddles.
-constexpr int pow2_radix(int rem) { return rem == 2 ? 2 : (rem == 4 || rem == 16) ? 4 : 8; }
+// (pow2_radix): straight-line stages, shifts for j div Ns.  The runtime
+// path (plan_axis, for non-instantiated lengths) uses radices <= 8.
+// Radix-16 stages first (fewest shared-memory round trips), then 8 / 4 / 2:
+// 64 = 16.4, 128 = 16.8, 256 = 16.16, 512 = 16.8.4, 1024 = 16.16.4.
+constexpr int pow2_radix(int rem) {
+    return rem >= 16 && rem != 32 ? 16 : (rem == 32 ? 8 : rem);
+}
 
-template <int L, int DIR, int NS>
+template <int L, int DIR, int NS, int SW = 0>
 __device__ __forceinline__ void fft_lines_pow2(float2* buf, int T, int t, int jb,
                                                const float2* __restrict__ tw, int tws) {
     if constexpr (NS < L) {
         constexpr int R = pow2_radix(L / NS);
-        stage_body<R, DIR, NS>(buf, T, L, NS, t, jb, (L + 31) / 32, tw, tws);
-        fft_lines_pow2<L, DIR, NS * R>(buf, T, t, jb, tw, tws);
+        stage_body<R, DIR, NS, SW>(buf, T, L, NS, t, jb, (L + 31) / 32, tw, tws);
+        fft_lines_pow2<L, DIR, NS * R, SW>(buf, T, t, jb, tw, tws);
     }
 }
 

@@ -41,6 +41,9 @@ extern "C" {
 const char* decon_last_error(void);
 /* Library ABI version (major * 10000 + minor * 100 + patch). */
 int decon_version(void);
+/* Synchronises the stream and reports DECON_ERR_TIMEOUT if any kernel's
+ * bounded TMA/mbarrier wait gave up since load (its results are invalid). */
+int decon_device_status(void* stream);
 /* Kernels launched by this library since load (benchmark accounting). */
 int64_t decon_launch_count(void);
 

@@ -246,3 +246,20 @@ def test_pdhg_convergence_bin_plain_operator(D, g32, g64):
     np.testing.assert_allclose(r.tau_history, g64["pdo_tau"], rtol=1e-4)
     np.testing.assert_allclose(r.loss_history, g64["pdo_loss"], rtol=1e-4)
     assert len(seen) == 15
+
+
+def test_tma_and_plain_column_passes_agree(D, monkeypatch):
+    # Power-of-two canvases run the column passes on TMA; DECON_NO_TMA=1 at
+    # plan creation selects the plain-load kernels.  Same radices, twiddles
+    # and operation order, so the two must agree bit for bit.
+    rng = np.random.default_rng(11)
+    k = rng.random((33, 65, 65)).astype(np.float32)
+    x = rng.random((64, 128, 128)).astype(np.float32)
+    c_tma = D.LinearFFTConvolver(k, (64, 128, 128), fft_shape=(128, 256, 256))
+    monkeypatch.setenv("DECON_NO_TMA", "1")
+    c_ld = D.LinearFFTConvolver(k, (64, 128, 128), fft_shape=(128, 256, 256))
+    monkeypatch.delenv("DECON_NO_TMA")
+    np.testing.assert_array_equal(cpu(c_tma.forward(x)), cpu(c_ld.forward(x)))
+    np.testing.assert_array_equal(cpu(c_tma.adjoint(x)), cpu(c_ld.adjoint(x)))
+    from deconlib_b200 import _lib
+    _lib.call("decon_device_status", _lib.stream_ptr())
