@@ -1,0 +1,195 @@
+// Persistent, software-pipelined column FFT pass (Y and axial passes).
+//
+// Each CTA loops over 16-column tiles (tile i, i + grid, ...).  Tiles arrive
+// through an NS-deep ring of TMA loads (one mbarrier per ring slot, bounded
+// waits), so the next tiles stream in while the current one is transformed.
+// The transform of a line of L = SPLIT * R * R points runs as two radix-R
+// Stockham stages with K = 1 butterfly per thread per stage: thread (t, j)
+// owns column t and butterfly j in both stages, so the second-stage twiddles
+// W_{R^2}^{r j} are computed once per thread and stay in registers.
+//
+// SPLIT = 2 uses the half-zero structure of the canvas (the signal occupies at
+// most half of the axis):
+//   forward, x[n] = 0 for n >= L/2:  X[2m] = FFT_{L/2}(x)[m],
+//                                     X[2m+1] = FFT_{L/2}(x[n] W_L^n)[m];
+//   inverse, only y[n], n < L/2, kept: y[n] = IFFT_{L/2}(X[2m])[n]
+//                                     + W_L^{-n} IFFT_{L/2}(X[2m+1])[n].
+// The axial pass (MODE = COL_OTF / COL_OTF_CONJ) multiplies by the OTF in
+// registers between the forward and inverse transforms: after the forward
+// second stage a thread holds X at m = j + R r, exactly the points the inverse
+// first stage needs, so that product costs no shared-memory round trip.  The
+// OTF values are prefetched from global memory into registers before the
+// tile's barrier wait.
+#pragma once
+
+#include "conv_impl.cuh"
+#include "tma.cuh"
+
+namespace dk {
+
+__device__ __forceinline__ int p1(int row, int t) { return physw<1>(row, t, 16); }
+
+template <int R, int SPLIT, int MODE>
+__global__ void __launch_bounds__(16 * R, 1) k_col_pipe(const __grid_constant__ PipeArgs a) {
+    constexpr int LH = R * R;          // sub-transform length
+    constexpr int L = LH * SPLIT;      // axis length
+    constexpr int NS = (L >= 512) ? 2 : 3;
+    constexpr bool OTF = (MODE == COL_OTF || MODE == COL_OTF_CONJ);
+    constexpr bool INV_FIRST = (MODE == COL_INV);
+    constexpr int D1 = INV_FIRST ? +1 : -1;  // direction of the first transform
+    extern __shared__ unsigned char smraw[];
+    float2* base = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
+    __shared__ uint64_t full[NS];
+    const int tid = threadIdx.x, t = tid & 15, j = tid >> 4;
+    const int total = a.nouter * a.ntiles;
+
+    // second-stage twiddles W_LH^(r j) = W_L^(SPLIT r j)
+    float2 w2[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) w2[r] = __ldg(&a.tw[(SPLIT * r * j) * a.tws]);
+    // split twiddles W_L^n, n = j + R r
+    float2 ws[SPLIT == 2 ? R : 1];
+    if constexpr (SPLIT == 2) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) ws[r] = __ldg(&a.tw[(j + R * r) * a.tws]);
+    }
+
+    if (tid == 0) {
+        for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
+        fence_proxy_async_smem();
+    }
+    __syncthreads();
+    const int nbox = (a.nin + a.src_box - 1) / a.src_box;
+    auto issue = [&](int tile, int s) {
+        const int o = tile / a.ntiles;
+        const int c0 = (tile - o * a.ntiles) * 32;
+        float2* buf = base + s * L * 16;
+        mbar_expect_tx(&full[s], (uint32_t)(nbox * a.src_box * 128));
+        for (int i = 0; i < nbox; ++i) {
+            const int r0 = i * a.src_box;
+            if (a.src_jdim == 1) tma_load_3d(buf + r0 * 16, &a.src, c0, r0, o, &full[s]);
+            else tma_load_3d(buf + r0 * 16, &a.src, c0, o, r0, &full[s]);
+        }
+    };
+    if (tid == 0)
+        for (int s = 0; s < NS; ++s) {
+            const int tile = blockIdx.x + s * gridDim.x;
+            if (tile < total) issue(tile, s);
+        }
+
+    for (int it = 0;; ++it) {
+        const int tile = blockIdx.x + it * gridDim.x;
+        if (tile >= total) break;
+        const int s = it % NS;
+        const uint32_t ph = (uint32_t)((it / NS) & 1);
+        float2* buf = base + s * L * 16;
+        const int o = tile / a.ntiles;
+        const int c0 = (tile - o * a.ntiles) * 32;
+
+        float2 ov[OTF ? SPLIT : 1][OTF ? R : 1];
+        if constexpr (OTF) {
+            const float2* op = a.otf + o * a.otf_os + (c0 >> 1) + t;
+#pragma unroll
+            for (int h = 0; h < SPLIT; ++h)
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    ov[h][r] = __ldg(op + (int64_t)(SPLIT * (j + R * r) + h) * a.otf_js);
+        }
+        if (!__syncthreads_and(mbar_wait_bounded(&full[s], ph))) return;
+
+        float2 v[SPLIT][R];
+        // ---- stage 1 of the first transform (Ns = 1) ----
+        if constexpr (!INV_FIRST) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int n = j + R * r;
+                const float2 x = n < a.nin ? buf[p1(n, t)] : make_float2(0.f, 0.f);
+                v[0][r] = x;
+                if constexpr (SPLIT == 2) v[1][r] = cmul(x, ws[r]);
+            }
+        } else {
+#pragma unroll
+            for (int h = 0; h < SPLIT; ++h)
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[h][r] = buf[p1(SPLIT * (j + R * r) + h, t)];
+        }
+#pragma unroll
+        for (int h = 0; h < SPLIT; ++h) dft<R, D1>(v[h]);
+        __syncthreads();
+#pragma unroll
+        for (int h = 0; h < SPLIT; ++h)
+#pragma unroll
+            for (int r = 0; r < R; ++r) buf[p1(h * LH + j * R + r, t)] = v[h][r];
+        __syncthreads();
+        // ---- stage 2 (Ns = R): reads and writes point j + R r ----
+#pragma unroll
+        for (int h = 0; h < SPLIT; ++h) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const float2 x = buf[p1(h * LH + j + R * r, t)];
+                v[h][r] = r == 0 ? x : (D1 < 0 ? cmul(x, w2[r]) : cmulc(x, w2[r]));
+            }
+            dft<R, D1>(v[h]);
+        }
+        if constexpr (OTF) {
+            // X at m = j + R r  ->  x OTF  ->  inverse stage 1 in registers
+#pragma unroll
+            for (int h = 0; h < SPLIT; ++h) {
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    v[h][r] = MODE == COL_OTF ? cmul(v[h][r], ov[h][r]) : cmulc(v[h][r], ov[h][r]);
+                dft<R, +1>(v[h]);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int h = 0; h < SPLIT; ++h)
+#pragma unroll
+                for (int r = 0; r < R; ++r) buf[p1(h * LH + j * R + r, t)] = v[h][r];
+            __syncthreads();
+#pragma unroll
+            for (int h = 0; h < SPLIT; ++h) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const float2 x = buf[p1(h * LH + j + R * r, t)];
+                    v[h][r] = r == 0 ? x : cmulc(x, w2[r]);
+                }
+                dft<R, +1>(v[h]);
+            }
+        }
+        // ---- outputs in natural order ----
+        if constexpr (MODE == COL_FWD) {
+            // X[SPLIT m + h], m = j + R r
+            if constexpr (SPLIT == 2) __syncthreads();  // other threads still read rows h LH + m
+#pragma unroll
+            for (int h = 0; h < SPLIT; ++h)
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int k = SPLIT * (j + R * r) + h;
+                    if (k < a.nout) buf[p1(k, t)] = v[h][r];
+                }
+        } else {
+            // y[n] = y0[n] (+ W_L^-n y1[n]), n = j + R r; this thread alone
+            // read rows n and LH + n, so no barrier is needed before writing.
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int n = j + R * r;
+                float2 y = v[0][r];
+                if constexpr (SPLIT == 2) y = cadd(y, cmulc(v[1][r], ws[r]));
+                if (n < a.nout) buf[p1(n, t)] = y;
+            }
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            for (int r0 = 0; r0 < a.nout; r0 += a.dst_box) {
+                if (a.dst_jdim == 1) tma_store_3d(&a.dst, c0, r0, o, buf + r0 * 16);
+                else tma_store_3d(&a.dst, c0, o, r0, buf + r0 * 16);
+            }
+            tma_store_commit_and_wait();
+            const int next = tile + NS * gridDim.x;
+            if (next < total) issue(next, s);
+        }
+    }
+}
+
+}  // namespace dk

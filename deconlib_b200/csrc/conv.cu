@@ -25,6 +25,7 @@
 
 #include "conv_impl.cuh"
 #include "tma.cuh"
+#include "colpipe.cuh"
 
 namespace dk {
 
@@ -621,9 +622,85 @@ bool encode_spectrum_map(CUtensorMap* map, const float2* base, int64_t pitch, in
 }
 
 // One column pass on TMA.  src/dst/otf maps come from the plan.
+// Pipelined kernel for (L, mode, nin, nout), or nullptr.  R x R (SPLIT 1) for
+// L = 64, 256; the half-zero split (SPLIT 2) for L = 128, 512 when the
+// non-zero input / kept output fits in half the axis.
+static void* pick_pipe(int L, int mode, int nin, int nout, int* R, int* split) {
+    const bool otf = mode == COL_OTF || mode == COL_OTF_CONJ;
+    const bool half_ok = (mode == COL_FWD && nin <= L / 2) || (mode == COL_INV && nout <= L / 2) ||
+                         (otf && nin <= L / 2 && nout <= L / 2);
+#define DK_PIPE(RR, SS)                                                      \
+    do {                                                                     \
+        *R = RR;                                                             \
+        *split = SS;                                                         \
+        switch (mode) {                                                      \
+            case COL_FWD: return (void*)k_col_pipe<RR, SS, COL_FWD>;         \
+            case COL_INV: return (void*)k_col_pipe<RR, SS, COL_INV>;         \
+            case COL_OTF: return (void*)k_col_pipe<RR, SS, COL_OTF>;         \
+            case COL_OTF_CONJ: return (void*)k_col_pipe<RR, SS, COL_OTF_CONJ>; \
+        }                                                                    \
+    } while (0)
+    if (L == 256) DK_PIPE(16, 1);
+    if (L == 64) DK_PIPE(8, 1);
+    if (L == 128 && half_ok) DK_PIPE(8, 2);
+#undef DK_PIPE
+    if (L == 512 && half_ok && !otf) {
+        *R = 16;
+        *split = 2;
+        return mode == COL_FWD ? (void*)k_col_pipe<16, 2, COL_FWD> : (void*)k_col_pipe<16, 2, COL_INV>;
+    }
+    return nullptr;
+}
+
+static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const CUtensorMap& src,
+                            int src_jdim, int src_box, int nin, const CUtensorMap& dst, int dst_jdim,
+                            int dst_box, int nout, int64_t nouter, cudaStream_t st, int* status) {
+    int R = 0, split = 0;
+    void* fn = getenv("DECON_NO_PIPE") ? nullptr : pick_pipe(ax.L, mode, nin, nout, &R, &split);
+    if (!fn) return false;
+    PipeArgs a;
+    memset(&a, 0, sizeof(a));
+    a.src = src;
+    a.dst = dst;
+    a.otf = p.otf;
+    a.otf_js = p.F[1] * p.P;
+    a.otf_os = p.P;
+    a.tw = ax.tw;
+    a.tws = ax.tws;
+    a.nin = nin;
+    a.nout = nout;
+    a.ntiles = (int)cdiv(p.Hx, 16);
+    a.nouter = (int)nouter;
+    a.src_jdim = src_jdim;
+    a.dst_jdim = dst_jdim;
+    a.src_box = src_box;
+    a.dst_box = dst_box;
+    const int L = ax.L;
+    const int ns = L >= 512 ? 2 : 3;
+    const size_t smem = 1024 + (size_t)ns * L * 16 * sizeof(float2);
+    const int nthr = 16 * R;
+    *status = DECON_OK;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        *status = fail(DECON_ERR_CUDA, "smem attribute failed");
+        return true;
+    }
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nthr, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int64_t total = nouter * a.ntiles;
+    const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count() * per_sm);
+    *status = launch(fn, grid, nthr, smem, st, &a,
+                     (mode == COL_OTF || mode == COL_OTF_CONJ) ? PROF_ZOTF : PROF_COL);
+    return true;
+}
+
 static int launch_col_tma(const ConvPlan& p, const Axis& ax, int mode, const CUtensorMap& src,
                           int src_jdim, int src_box, int nin, const CUtensorMap& dst, int dst_jdim,
                           int dst_box, int nout, int64_t nouter, cudaStream_t st) {
+    int pst = DECON_OK;
+    if (launch_col_pipe(p, ax, mode, src, src_jdim, src_box, nin, dst, dst_jdim, dst_box, nout,
+                        nouter, st, &pst))
+        return pst;
     ColTmaArgs a;
     memset(&a, 0, sizeof(a));
     a.src = src;

@@ -60,6 +60,17 @@ struct ColTmaArgs {
     const float2* tw;
 };
 
+// Persistent pipelined column pass (k_col_pipe).
+struct PipeArgs {
+    CUtensorMap src, dst;
+    const float2* otf;      // OTF base for the axial pass
+    int64_t otf_js, otf_os; // complex-element strides of OTF rows (kz) and planes (ky)
+    const float2* tw;       // W_L table, W_L^m = tw[m * tws]
+    int tws;
+    int nin, nout, ntiles, nouter;
+    int src_jdim, dst_jdim, src_box, dst_box;
+};
+
 struct XC2RArgs {
     const float2* in;
     int64_t P, Ny, Nx, nrows;

@@ -248,18 +248,30 @@ def test_pdhg_convergence_bin_plain_operator(D, g32, g64):
     assert len(seen) == 15
 
 
-def test_tma_and_plain_column_passes_agree(D, monkeypatch):
-    # Power-of-two canvases run the column passes on TMA; DECON_NO_TMA=1 at
-    # plan creation selects the plain-load kernels.  Same radices, twiddles
-    # and operation order, so the two must agree bit for bit.
+@pytest.mark.parametrize("shape,fft", [((64, 128, 128), (128, 256, 256)),
+                                       ((128, 256, 256), (256, 512, 512)),
+                                       ((20, 60, 40), (64, 128, 128)),
+                                       ((30, 100, 90), (64, 256, 256))])
+def test_column_pass_variants_agree(D, monkeypatch, shape, fft):
+    # The pipelined column kernel (R x R Stockham, half-zero split for 128 /
+    # 512), the one-tile TMA kernel (DECON_NO_PIPE) and the plain-load kernel
+    # (DECON_NO_TMA) compute the same transforms with different factorings.
     rng = np.random.default_rng(11)
-    k = rng.random((33, 65, 65)).astype(np.float32)
-    x = rng.random((64, 128, 128)).astype(np.float32)
-    c_tma = D.LinearFFTConvolver(k, (64, 128, 128), fft_shape=(128, 256, 256))
-    monkeypatch.setenv("DECON_NO_TMA", "1")
-    c_ld = D.LinearFFTConvolver(k, (64, 128, 128), fft_shape=(128, 256, 256))
-    monkeypatch.delenv("DECON_NO_TMA")
-    np.testing.assert_array_equal(cpu(c_tma.forward(x)), cpu(c_ld.forward(x)))
-    np.testing.assert_array_equal(cpu(c_tma.adjoint(x)), cpu(c_ld.adjoint(x)))
+    kshape = tuple(f - n + 1 for n, f in zip(shape, fft))
+    k = rng.random(kshape).astype(np.float32)
+    x = rng.random(shape).astype(np.float32)
+    outs = []
+    for env in ({}, {"DECON_NO_PIPE": "1"}, {"DECON_NO_TMA": "1"}):
+        for key in ("DECON_NO_PIPE", "DECON_NO_TMA"):
+            monkeypatch.delenv(key, raising=False)
+        for key, val in env.items():
+            monkeypatch.setenv(key, val)
+        c = D.LinearFFTConvolver(k, shape, fft_shape=fft)
+        outs.append((cpu(c.forward(x)), cpu(c.adjoint(x))))
+    for key in ("DECON_NO_PIPE", "DECON_NO_TMA"):
+        monkeypatch.delenv(key, raising=False)
+    for f, a in outs[1:]:
+        assert rel(f, outs[0][0]) < 1e-6
+        assert rel(a, outs[0][1]) < 1e-6
     from deconlib_b200 import _lib
     _lib.call("decon_device_status", _lib.stream_ptr())
