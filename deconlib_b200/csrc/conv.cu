@@ -26,119 +26,9 @@
 #include "conv_impl.cuh"
 #include "tma.cuh"
 #include "colpipe.cuh"
+#include "xpass.cuh"
 
 namespace dk {
-
-// ---------------------------------------------------------------------------
-// device value fetch for the X R2C prologue
-// ---------------------------------------------------------------------------
-
-__device__ __forceinline__ bool kernel_src(int64_t c, int64_t F, int64_t m, int64_t npos,
-                                           int64_t& k) {
-    // Corner-origin embedding (utils/padding.py:142-190): canvas index c holds
-    // kernel index c (c < npos) or c - F + m (the wrapped negative offsets).
-    if (c < npos) {
-        k = c;
-        return c < m;
-    }
-    const int64_t nneg = m - npos;
-    if (c >= F - nneg) {
-        k = c - F + m;
-        return true;
-    }
-    return false;
-}
-
-struct RowSrc {
-    const float* p;  // row base (nullptr: row is outside the window)
-    bool ok;
-};
-
-template <int PRO>
-__device__ __forceinline__ RowSrc row_source(const XR2CArgs& a, int64_t z, int64_t y) {
-    RowSrc r{nullptr, false};
-    if constexpr (PRO == PRO_KERNEL) {
-        int64_t kz, ky;
-        if (kernel_src(z, a.Nz, a.Kz, a.pz, kz) && kernel_src(y, a.Ny, a.Ky, a.py, ky)) {
-            r.p = a.in + (kz * a.Ky + ky) * a.Kx;
-            r.ok = true;
-        }
-    } else {
-        const int64_t iz = z - a.win.oz, iy = y - a.win.oy;
-        if (iz >= 0 && iz < a.win.wz && iy >= 0 && iy < a.win.wy) {
-            r.ok = true;
-            if (a.in) r.p = a.in + (iz * a.win.wy + iy) * a.win.wx;
-        }
-    }
-    return r;
-}
-
-template <int PRO>
-__device__ __forceinline__ float fetch_x(const XR2CArgs& a, const RowSrc& r, int64_t x) {
-    if (!r.ok || x >= a.Nx) return 0.f;
-    if constexpr (PRO == PRO_KERNEL) {
-        int64_t kx;
-        if (!kernel_src(x, a.Nx, a.Kx, a.px, kx)) return 0.f;
-        return __ldg(r.p + kx) / a.kdiv;
-    } else {
-        const int64_t ix = x - a.win.ox;
-        if (ix < 0 || ix >= a.win.wx) return 0.f;
-        if constexpr (PRO == PRO_CONST) {
-            return a.cval;
-        } else if constexpr (PRO == PRO_RLINIT) {
-            return fmaxf(__ldg(r.p + ix) - a.bg, 1e-6f);
-        } else {
-            return __ldg(r.p + ix);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// pass 1: X R2C
-// ---------------------------------------------------------------------------
-
-template <int PRO, int LS>
-__global__ void __launch_bounds__(kFftThreads) k_xr2c(XR2CArgs a) {
-    extern __shared__ float2 sm[];
-    const int T = a.T, L = a.ax.L, tid = threadIdx.x;
-    const int64_t row0 = (int64_t)blockIdx.x * T;
-    for (int q = tid; q < T * L; q += blockDim.x) {
-        const int t = q / L, n = q - t * L;
-        const int64_t row = row0 + t;
-        float2 v = make_float2(0.f, 0.f);
-        if (row < a.nrows) {
-            const int64_t z = row / a.Ny, y = row - z * a.Ny;
-            const RowSrc rs = row_source<PRO>(a, z, y);
-            if (a.odd) {
-                v.x = fetch_x<PRO>(a, rs, n);
-            } else {
-                v.x = fetch_x<PRO>(a, rs, 2 * (int64_t)n);
-                v.y = fetch_x<PRO>(a, rs, 2 * (int64_t)n + 1);
-            }
-        }
-        sm[phys(n, t, T)] = v;
-    }
-    __syncthreads();
-    fft_lines<-1, LS>(sm, T, tid % T, tid / T, a.ax);
-    const int H = a.Hx;
-    for (int q = tid; q < T * H; q += blockDim.x) {
-        const int t = q / H, k = q - t * H;
-        const int64_t row = row0 + t;
-        if (row >= a.nrows) continue;
-        float2 X;
-        if (a.odd) {
-            X = sm[phys(k, t, T)];
-        } else {
-            const int M = L;
-            const float2 zk = sm[phys(k == M ? 0 : k, t, T)];
-            const float2 zm = cconj(sm[phys(k == 0 ? 0 : M - k, t, T)]);
-            const float2 e = cscale(cadd(zk, zm), 0.5f);
-            const float2 o = rot90<-1>(cscale(csub(zk, zm), 0.5f));
-            X = cadd(e, cmul(__ldg(&a.twx[k]), o));
-        }
-        a.out[row * a.P + k] = X;
-    }
-}
 
 // ---------------------------------------------------------------------------
 // passes 2-4: complex FFT along a strided axis over 16-wide column tiles
@@ -246,95 +136,6 @@ __global__ void __launch_bounds__(kFftThreads, (LS >= 512 ? 1 : 2)) k_colfft_tma
             else tma_store_3d(&a.dst, c0, o, r0, sm + r0 * 16);
         }
         tma_store_commit_and_wait();
-    }
-}
-
-// ---------------------------------------------------------------------------
-// pass 5: X C2R with fused epilogues
-// ---------------------------------------------------------------------------
-
-template <int EPI, int LS>
-__global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
-    extern __shared__ float2 sm[];
-    const int T = a.T, L = a.ax.L, tid = threadIdx.x;
-    const int64_t row0 = (int64_t)blockIdx.x * T;
-    for (int q = tid; q < T * L; q += blockDim.x) {
-        const int t = q / L, k = q - t * L;
-        const int64_t row = row0 + t;
-        float2 Z = make_float2(0.f, 0.f);
-        if (row < a.nrows) {
-            const float2* rp = a.in + row * a.P;
-            if (a.odd) {
-                // Full Hermitian spectrum from the half: X[k] = conj(X[Fx - k]).
-                Z = k < a.Hx ? rp[k] : cconj(rp[L - k]);
-                if (k == 0) Z.y = 0.f;
-            } else {
-                const int M = L;
-                float2 xk = rp[k];
-                float2 xm = rp[M - k];
-                if (k == 0) {  // irfft ignores Im of the DC and Nyquist bins
-                    xk.y = 0.f;
-                    xm.y = 0.f;
-                }
-                xm = cconj(xm);
-                const float2 e = cadd(xk, xm);
-                const float2 od = cmulc(csub(xk, xm), __ldg(&a.twx[k]));
-                Z = cadd(e, rot90<+1>(od));
-            }
-        }
-        sm[phys(k, t, T)] = Z;
-    }
-    __syncthreads();
-    fft_lines<+1, LS>(sm, T, tid % T, tid / T, a.ax);
-
-    double acc = 0.0;
-    const int64_t Nx = a.Nx;
-    for (int64_t q = tid; q < (int64_t)T * Nx; q += blockDim.x) {
-        const int t = (int)(q / Nx);
-        const int64_t x = q - (int64_t)t * Nx;
-        const int64_t row = row0 + t;
-        if (row >= a.nrows) continue;
-        const int64_t z = row / a.Ny, y = row - z * a.Ny;
-        const int64_t iz = z - a.win.oz, iy = y - a.win.oy, ix = x - a.win.ox;
-        if (iz < 0 || iz >= a.win.wz || iy < 0 || iy >= a.win.wy || ix < 0 || ix >= a.win.wx)
-            continue;
-        float v;
-        if (a.odd) {
-            v = sm[phys((int)x, t, T)].x;
-        } else {
-            const float2 c = sm[phys((int)(x >> 1), t, T)];
-            v = (x & 1) ? c.y : c.x;
-        }
-        v *= a.scale;
-        const int64_t i = (iz * a.win.wy + iy) * a.win.wx + ix;
-        if constexpr (EPI == EPI_STORE) {
-            a.out[i] = v;
-        } else if constexpr (EPI == EPI_RL_RATIO || EPI == EPI_PRED) {
-            // rl_mlx.py:147-148  model = A x + b ; ratio = y / max(model, 1e-10)
-            const float m = v + a.bg;
-            const float yv = __ldg(a.aux0 + i);
-            if constexpr (EPI == EPI_RL_RATIO) {
-                a.out[i] = yv / fmaxf(m, 1e-10f);
-            } else {
-                a.out[i] = m;
-            }
-            if (a.partials) {
-                // rl_mlx.py:75-79: y log(max(y,eps)/max(m,eps)) - (y - max(m,eps))
-                const float ys = fmaxf(yv, 1e-6f), ms = fmaxf(m, 1e-6f);
-                acc += (double)(yv * logf(ys / ms) - (yv - ms));
-            }
-        } else if constexpr (EPI == EPI_RL_UPDATE) {
-            // rl_mlx.py:149-150  x = max(x * where(active, A^T ratio / sens, 0), 1e-10)
-            const float s = __ldg(a.aux1 + i);
-            const float c = s > 0.f ? v / s : 0.f;
-            a.out[i] = fmaxf(a.aux0[i] * c, 1e-10f);
-        }
-    }
-    if constexpr (EPI == EPI_RL_RATIO || EPI == EPI_PRED) {
-        if (a.partials) {
-            const double s = block_sum(acc);
-            if (tid == 0) a.partials[blockIdx.x] = s;
-        }
     }
 }
 
@@ -503,6 +304,9 @@ int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cva
     a.odd = p.odd;
     a.ax = p.ax_x;
     a.twx = p.twx;
+    a.vec4 = pro == PRO_ARRAY && in != nullptr && !p.odd && (a.Nx % 4) == 0 && win.oz == 0 &&
+             win.oy == 0 && win.ox == 0 && win.wz == p.N[0] && win.wy == p.N[1] &&
+             win.wx == p.N[2] && (reinterpret_cast<uintptr_t>(in) & 15) == 0;
     a.T = p.T_x;
     a.nrows = nz_rows * a.Ny;
     const int nthr = threads_for(a.T, a.ax);
@@ -559,6 +363,12 @@ int launch_xc2r(const ConvPlan& p, int epi, const float2* in, Win3 win, float* o
     a.odd = p.odd;
     a.ax = p.ax_x;
     a.twx = p.twx;
+    {
+        const bool full = win.oz == 0 && win.oy == 0 && win.ox == 0 && win.wz == p.N[0] &&
+                          win.wy == p.N[1] && win.wx == p.N[2];
+        auto al = [](const void* q) { return q == nullptr || (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+        a.vec4 = full && !p.odd && (p.N[2] % 4) == 0 && al(out) && al(aux0) && al(aux1);
+    }
     a.T = p.T_x;
     a.scale = (float)(1.0 / ((double)p.F[0] * (double)p.F[1] * (double)p.F[2]));
     a.win = win;

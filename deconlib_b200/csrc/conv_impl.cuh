@@ -37,7 +37,7 @@ struct XR2CArgs {
     int64_t Kz, Ky, Kx, pz, py, px;  // kernel embedding (PRO_KERNEL)
     float2* out;
     int64_t P, nrows;
-    int Hx, odd, T;
+    int Hx, odd, T, vec4;
     Axis ax;            // length Fx/2 (even Fx) or Fx (odd)
     const float2* twx;  // W_Fx table
 };
@@ -74,7 +74,7 @@ struct PipeArgs {
 struct XC2RArgs {
     const float2* in;
     int64_t P, Ny, Nx, nrows;
-    int Hx, odd, T;
+    int Hx, odd, T, vec4;
     Axis ax;
     const float2* twx;
     float scale;

@@ -15,7 +15,7 @@
 //
 // Twiddles come from a table of exp(-2 pi i m / Lt) computed on the host in
 // double precision (W_L^m = tw[m * tws]); no sin/cos is evaluated on the GPU.
-// Radices 2, 3, 4, 5, 7 and 8 are implemented.
+// Radices 2, 3, 4, 5, 7, 8 and 16 are implemented.
 #pragma once
 
 #include "common.cuh"
@@ -210,7 +210,11 @@ __device__ __forceinline__ void dft(float2* v) {
 // One Stockham stage.  (t, jb): this thread's line and first butterfly.
 template <int R, int DIR, int NS_STATIC, int SW = 0>
 __device__ __forceinline__ void stage_body(float2* buf, int T, int L, int Ns_dyn, int t, int jb,
-                                           int tpl, const float2* __restrict__ tw, int tws) {
+                                           int tpl, const float2* __restrict__ tw, int tws,
+                                           int nin = 1 << 30, int nout = 1 << 30) {
+    // nin: points >= nin are known zeros (only meaningful in a first stage,
+    // where point index = input index); nout: points >= nout are not stored
+    // (only in a last stage, where point index = output index).
     // ceil(32 / R) butterflies per thread cover L / R butterflies with
     // ceil(L / 32) threads per line for every radix (<= 35 values held).
     constexpr int K = (32 + R - 1) / R;
@@ -223,7 +227,8 @@ __device__ __forceinline__ void stage_body(float2* buf, int T, int L, int Ns_dyn
         const int j = jb + k * tpl;
         if (jb < tpl && j < nb) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[k][r] = buf[physw<SW>(j + r * nb, t, T)];
+            for (int r = 0; r < R; ++r)
+                v[k][r] = (j + r * nb < nin) ? buf[physw<SW>(j + r * nb, t, T)] : make_float2(0.f, 0.f);
             if (Ns > 1) {
                 const int kk = j % Ns;
 #pragma unroll
@@ -242,7 +247,8 @@ __device__ __forceinline__ void stage_body(float2* buf, int T, int L, int Ns_dyn
         if (jb < tpl && j < nb) {
             const int base = (j / Ns) * Ns * R + (j % Ns);
 #pragma unroll
-            for (int r = 0; r < R; ++r) buf[physw<SW>(base + r * Ns, t, T)] = v[k][r];
+            for (int r = 0; r < R; ++r)
+                if (base + r * Ns < nout) buf[physw<SW>(base + r * Ns, t, T)] = v[k][r];
         }
     }
     __syncthreads();
@@ -285,11 +291,13 @@ constexpr int pow2_radix(int rem) {
 
 template <int L, int DIR, int NS, int SW = 0>
 __device__ __forceinline__ void fft_lines_pow2(float2* buf, int T, int t, int jb,
-                                               const float2* __restrict__ tw, int tws) {
+                                               const float2* __restrict__ tw, int tws,
+                                               int nin = 1 << 30, int nout = 1 << 30) {
     if constexpr (NS < L) {
         constexpr int R = pow2_radix(L / NS);
-        stage_body<R, DIR, NS, SW>(buf, T, L, NS, t, jb, (L + 31) / 32, tw, tws);
-        fft_lines_pow2<L, DIR, NS * R, SW>(buf, T, t, jb, tw, tws);
+        stage_body<R, DIR, NS, SW>(buf, T, L, NS, t, jb, (L + 31) / 32, tw, tws,
+                                   NS == 1 ? nin : (1 << 30), NS * R == L ? nout : (1 << 30));
+        fft_lines_pow2<L, DIR, NS * R, SW>(buf, T, t, jb, tw, tws, nin, nout);
     }
 }
 
@@ -298,9 +306,10 @@ __device__ __forceinline__ void fft_lines_pow2(float2* buf, int T, int t, int jb
 // must call it (it contains barriers).  t = tid % T, jb = tid / T.
 // LS > 0 selects the compile-time path for length LS (== ax.L).
 template <int DIR, int LS>
-__device__ __forceinline__ void fft_lines(float2* buf, int T, int t, int jb, const Axis ax) {
+__device__ __forceinline__ void fft_lines(float2* buf, int T, int t, int jb, const Axis ax,
+                                          int nin = 1 << 30, int nout = 1 << 30) {
     if constexpr (LS > 0) {
-        fft_lines_pow2<LS, DIR, 1>(buf, T, t, jb, ax.tw, ax.tws);
+        fft_lines_pow2<LS, DIR, 1>(buf, T, t, jb, ax.tw, ax.tws, nin, nout);
     } else {
         fft_lines_dyn<DIR>(buf, T, t, jb, ax);
     }
