@@ -429,6 +429,33 @@ def run_conv_only(args):
                       "ms_per_fwd_adj_pair": e0.elapsed_time(e1) / args.steps}), flush=True)
 
 
+def run_pdhg_only(args):
+    """The PDHG iterations of the headline workload only; prints ms per iteration."""
+    import torch
+
+    import deconlib_b200.deconvolution as D
+    from deconlib_b200.deconvolution._device import to_device
+    from deconlib_b200.deconvolution.pdhg import HessianRegularizer, PDHGRunner, _compute_spacing_ratio
+
+    psf, obs = pdhg_inputs(D)
+    data = to_device(obs)
+    A = D.compose(D.FractionalAreaDownsample((2.0, 2.0, 2.0)), D.LinearFFTConvolver(psf, OBJ))
+    reg = HessianRegularizer(3, _compute_spacing_ratio(SPACING_PD, 3), "L1")
+    x0 = D.prox_nonneg(A.adjoint(data))
+    run = PDHGRunner(data, A, reg, x0, 1e-3, "poisson", args.warmup + args.steps, 5.0, 0.99, 0.5,
+                     10, 0.0, 20, 5)
+    for _ in range(args.warmup):
+        run.iterate()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        run.iterate()
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "pdhg", "ms_per_iter": e0.elapsed_time(e1) / args.steps}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -436,15 +463,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", choices=["full", "conv"], default="full",
+    ap.add_argument("--mode", choices=["full", "conv", "pdhg"], default="full",
                     help="conv: only warm-up + steps forward/adjoint convolutions of the PDHG "
-                         "operator (a small, fixed launch sequence for ncu captures)")
+                         "operator; pdhg: only the timed PDHG iterations (small, fixed launch "
+                         "sequences for ncu captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     ws, rank, local = dist_setup()
     if args.mode == "conv":
         run_conv_only(args)
+        return
+    if args.mode == "pdhg":
+        run_pdhg_only(args)
         return
     if args.impl == "reference":
         run_reference(args, ws, rank, local)

@@ -77,6 +77,11 @@ _SIGS = {
                                   C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _dp, _dp, _dp,
                                   _dp, _p]),
     "decon_pdhg_set_stop": (C.c_int, [_p, C.c_int, _p]),
+    "decon_pdhg_hess_dual": (C.c_int, [_p, _p, _p, _p, _i64p, C.c_float, C.c_float, C.c_int, _p]),
+    "decon_pdhg_hess_primal": (C.c_int, [_p, _p, _p, _p, _p, _i64p, C.c_float, _p]),
+    "decon_pdhg_hess_dk": (C.c_int, [_p, _p, _p, _i64, _p, _p, _i64p, C.c_float, _p]),
+    "decon_pdhg_hess_loss": (C.c_int, [_p, _p, _p, C.c_float, C.c_int, _i64, _p, _i64p, C.c_float,
+                                       C.c_int, C.c_double, C.c_int, _p]),
     "decon_profile_start": (C.c_int, [C.c_int]),
     "decon_profile_stop": (C.c_int, [_dp, _i64p]),
 }

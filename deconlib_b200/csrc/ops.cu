@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "conv_impl.cuh"
+#include "stencil.cuh"
 
 namespace dk {
 
@@ -73,104 +74,35 @@ struct Vol {
     __device__ __forceinline__ float at(int64_t z, int64_t y, int64_t x) const {
         return __ldg(p + (z * ny + y) * nx + x);
     }
+    __device__ __forceinline__ float operator()(int64_t z, int64_t y, int64_t x) const {
+        return at(z, y, x);
+    }
 };
 
-__device__ __forceinline__ int64_t clampi(int64_t v, int64_t n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
-
-// d2 along one axis (linops_core_mlx.py:66-76): (f[i-1] - 2 f[i]) + f[i+1], edge-replicated.
-__device__ __forceinline__ float d2v(float fm, float f0, float fp) { return fm - 2.f * f0 + fp; }
-
-__global__ void k_hessian_fwd(Vol f, float* __restrict__ h, float w0, float w1, float w2, float w3,
-                              float w4, float w5) {
+// Hessian3D.forward (linops_mlx.py:224-242): six weighted components.
+__global__ void k_hessian_fwd(Vol f, float* __restrict__ h, W6 w) {
+    const Dims d{f.nz, f.ny, f.nx};
     const int64_t n = f.nz * f.ny * f.nx;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t x = i % f.nx, t = i / f.nx, y = t % f.ny, z = t / f.ny;
-        const int64_t zm = clampi(z - 1, f.nz), zp = clampi(z + 1, f.nz);
-        const int64_t ym = clampi(y - 1, f.ny), yp = clampi(y + 1, f.ny);
-        const int64_t xm = clampi(x - 1, f.nx), xp = clampi(x + 1, f.nx);
-        const float c = f.at(z, y, x);
-        const float hzz = d2v(f.at(zm, y, x), c, f.at(zp, y, x));
-        const float hyy = d2v(f.at(z, ym, x), c, f.at(z, yp, x));
-        const float hxx = d2v(f.at(z, y, xm), c, f.at(z, y, xp));
-        // d1_cen(d1_cen(f, z), y): Dz at y+-1, then (Dz[y+1] - Dz[y-1]) / 2
-        const float dz_yp = (f.at(zp, yp, x) - f.at(zm, yp, x)) / 2.f;
-        const float dz_ym = (f.at(zp, ym, x) - f.at(zm, ym, x)) / 2.f;
-        const float hyz = (dz_yp - dz_ym) / 2.f;
-        const float dz_xp = (f.at(zp, y, xp) - f.at(zm, y, xp)) / 2.f;
-        const float dz_xm = (f.at(zp, y, xm) - f.at(zm, y, xm)) / 2.f;
-        const float hxz = (dz_xp - dz_xm) / 2.f;
-        const float dy_xp = (f.at(z, yp, xp) - f.at(z, ym, xp)) / 2.f;
-        const float dy_xm = (f.at(z, yp, xm) - f.at(z, ym, xm)) / 2.f;
-        const float hxy = (dy_xp - dy_xm) / 2.f;
-        h[i] = hzz * w0;
-        h[n + i] = hyy * w1;
-        h[2 * n + i] = hxx * w2;
-        h[3 * n + i] = hyz * w3;
-        h[4 * n + i] = hxz * w4;
-        h[5 * n + i] = hxy * w5;
+        float hv[6];
+        hess6(f, z, y, x, d, w.w, hv);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) h[c * n + i] = hv[c];
     }
 }
 
-// d1_cen_adj (linops_core_mlx.py:53-58): out[i] = (G(i-1) - G(i+1)) / 2 with
-// G(-1) = -g[0], G(n) = -g[n-1].
-// Each element is first multiplied by its component weight (H_w = H * w,
-// linops_mlx.py:250), exactly the float32 product the reference forms.
-__device__ __forceinline__ float gext(const float* g, int64_t j, int64_t n, int64_t s, float w) {
-    return j < 0 ? -(__ldg(g) * w) : (j >= n ? -(__ldg(g + (n - 1) * s) * w) : __ldg(g + j * s) * w);
-}
-
-// d1_cen_adj along axis b of (d1_cen_adj along axis a of H) at index (ib, ia)
-// of a 2-D slice g (strides sb, sa).  The inner (axis a) adjoint is evaluated
-// at ib-1 and ib+1 first, then the outer one combines them.
-__device__ __forceinline__ float inner_adj(const float* g, int64_t ia, int64_t na, int64_t sa,
-                                           float w) {
-    return (gext(g, ia - 1, na, sa, w) - gext(g, ia + 1, na, sa, w)) / 2.f;
-}
-
-__device__ __forceinline__ float mixed_adj(const float* g, int64_t ib, int64_t nb, int64_t sb,
-                                           int64_t ia, int64_t na, int64_t sa, float w) {
-    // value of the inner adjoint on row jb of axis b
-    auto row = [&](int64_t jb) -> float {
-        if (jb < 0) return -inner_adj(g, ia, na, sa, w);
-        if (jb >= nb) return -inner_adj(g + (nb - 1) * sb, ia, na, sa, w);
-        return inner_adj(g + jb * sb, ia, na, sa, w);
-    };
-    return (row(ib - 1) - row(ib + 1)) / 2.f;
-}
-
-// d2 of a weighted component h * w along one axis with edge replication.
-__device__ __forceinline__ float d2w(const float* g, int64_t i, int64_t n, int64_t s, float w) {
-    const float fm = __ldg(g + clampi(i - 1, n) * s) * w;
-    const float f0 = __ldg(g + i * s) * w;
-    const float fp = __ldg(g + clampi(i + 1, n) * s) * w;
-    return d2v(fm, f0, fp);
-}
-
-// Hessian3D.adjoint (linops_mlx.py:244-259): weights applied per element,
-// then the six adjoint stencils summed in the reference's order.
-__global__ void k_hessian_adj(const float* __restrict__ hw, float* __restrict__ out, int64_t nz,
-                              int64_t ny, int64_t nx, float w0, float w1, float w2, float w3,
-                              float w4, float w5) {
-    const int64_t n = nz * ny * nx;
-    const int64_t sz = ny * nx, sy = nx, sx = 1;
+// Hessian3D.adjoint (linops_mlx.py:244-259).
+__global__ void k_hessian_adj(const float* __restrict__ hw, float* __restrict__ out, Dims d, W6 w) {
+    const int64_t n = d.nz * d.ny * d.nx;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t x = i % nx, t = i / nx, y = t % ny, z = t / ny;
-        const float azz = d2w(hw + y * sy + x, z, nz, sz, w0);
-        const float ayy = d2w(hw + n + z * sz + x, y, ny, sy, w1);
-        const float axx = d2w(hw + 2 * n + z * sz + y * sy, x, nx, sx, w2);
-        // adj_yz = d1_cen_adj(d1_cen_adj(H3, axis=y), axis=z)
-        const float ayz = mixed_adj(hw + 3 * n + x, z, nz, sz, y, ny, sy, w3);
-        // adj_xz = d1_cen_adj(d1_cen_adj(H4, axis=x), axis=z)
-        const float axz = mixed_adj(hw + 4 * n + y * sy, z, nz, sz, x, nx, sx, w4);
-        // adj_xy = d1_cen_adj(d1_cen_adj(H5, axis=x), axis=y)
-        const float axy = mixed_adj(hw + 5 * n + z * sz, y, ny, sy, x, nx, sx, w5);
-        out[i] = ((((azz + ayy) + axx) + ayz) + axz) + axy;
+        const int64_t x = i % d.nx, t = i / d.nx, y = t % d.ny, z = t / d.ny;
+        out[i] = hess_adj_at(hw, z, y, x, d, w.w);
     }
 }
 
-// Gradient3D: forward differences with f[n] = f[n-1] (linops_core_mlx.py:25-32).
 __global__ void k_gradient_fwd(Vol f, float* __restrict__ g, float r) {
     const int64_t n = f.nz * f.ny * f.nx;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -202,17 +134,6 @@ __global__ void k_gradient_adj(const float* __restrict__ g, float* __restrict__ 
         const float ax = d1f_adj(g + 2 * n + z * sz + y * sy, x, nx, 1, 1.f);
         out[i] = (az + ay) + ax;
     }
-}
-
-static void hessian_weights(float r, float w[6]) {
-    // linops_mlx.py:237-239 (SQRT2 is a float32 device scalar there)
-    const float s2 = sqrtf(2.f);
-    w[0] = (float)((double)r * (double)r);
-    w[1] = 1.f;
-    w[2] = 1.f;
-    w[3] = r * s2;
-    w[4] = r * s2;
-    w[5] = s2;
 }
 
 }  // namespace dk
@@ -307,22 +228,21 @@ int decon_banded_axis(const float* in, float* out, int64_t outer, int64_t n_in, 
 
 int decon_hessian3d_forward(const float* x, float* h, const int64_t shape[3], float r, void* stream) {
     if (!x || !h || !shape) return fail(DECON_ERR_NULL, "null pointer");
-    float w[6];
-    hessian_weights(r, w);
+    W6 w;
+    hessian_weights(r, w.w);
     Vol f{x, shape[0], shape[1], shape[2]};
     const int64_t n = shape[0] * shape[1] * shape[2];
-    k_hessian_fwd<<<grid1d(n, 256), 256, 0, as_stream(stream)>>>(f, h, w[0], w[1], w[2], w[3], w[4], w[5]);
+    k_hessian_fwd<<<grid1d(n, 256), 256, 0, as_stream(stream)>>>(f, h, w);
     DK_LAUNCHED();
     return DECON_OK;
 }
 
 int decon_hessian3d_adjoint(const float* h, float* x, const int64_t shape[3], float r, void* stream) {
     if (!h || !x || !shape) return fail(DECON_ERR_NULL, "null pointer");
-    float w[6];
-    hessian_weights(r, w);
+    W6 w;
+    hessian_weights(r, w.w);
     const int64_t n = shape[0] * shape[1] * shape[2];
-    k_hessian_adj<<<grid1d(n, 256), 256, 0, as_stream(stream)>>>(h, x, shape[0], shape[1], shape[2],
-                                                                 w[0], w[1], w[2], w[3], w[4], w[5]);
+    k_hessian_adj<<<grid1d(n, 256), 256, 0, as_stream(stream)>>>(h, x, Dims{shape[0], shape[1], shape[2]}, w);
     DK_LAUNCHED();
     return DECON_OK;
 }

@@ -11,6 +11,7 @@
 
 #include "conv_impl.cuh"
 #include "solvers.cuh"
+#include "stencil.cuh"
 
 namespace dk {
 
@@ -269,6 +270,155 @@ __global__ void k_record_loss(PdhgDev* s, double alpha, int kk) {
     if (threadIdx.x == 0) s->loss_hist[kk] = dl + alpha * rl;
 }
 
+// ---- fused Hessian3D PDHG kernels --------------------------------------------
+// The regulariser half of the iteration without materialising L x_bar, L^T y2
+// or L (x_new - x): the Hessian is evaluated on the fly from the fields below
+// (values identical to the stand-alone operator, the same float32 ops).
+
+struct XbarField {  // x_bar = x + theta (x - x_prev)
+    const float* xc;
+    const float* xp;
+    float th;
+    int64_t ny, nx;
+    __device__ __forceinline__ float operator()(int64_t z, int64_t y, int64_t x) const {
+        const int64_t i = (z * ny + y) * nx + x;
+        const float a = __ldg(xc + i);
+        return a + th * (a - __ldg(xp + i));
+    }
+};
+
+struct DiffField {  // x_new - x
+    const float* a;
+    const float* b;
+    int64_t ny, nx;
+    __device__ __forceinline__ float operator()(int64_t z, int64_t y, int64_t x) const {
+        const int64_t i = (z * ny + y) * nx + x;
+        return __ldg(a + i) - __ldg(b + i);
+    }
+};
+
+struct PlainField {
+    const float* p;
+    int64_t ny, nx;
+    __device__ __forceinline__ float operator()(int64_t z, int64_t y, int64_t x) const {
+        return __ldg(p + (z * ny + y) * nx + x);
+    }
+};
+
+// y2 = proj(y2 + sigma H x_bar) (pdhg_mlx.py:732-734 with x_bar of :841).
+template <int NORM>
+__global__ void __launch_bounds__(256) k_hess_dual(PdhgDev* s, float* __restrict__ y2,
+                                                   const float* __restrict__ xc,
+                                                   const float* __restrict__ xp, Dims d, W6 w,
+                                                   float alpha) {
+    if (s->stop) return;
+    const float sg = (float)s->sigma;
+    const XbarField f{xc, xp, (float)s->theta, d.ny, d.nx};
+    const int64_t n = d.nz * d.ny * d.nx;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t x = i % d.nx, t = i / d.nx, y = t % d.ny, z = t / d.ny;
+        float h[6];
+        hess6(f, z, y, x, d, w.w, h);
+        if constexpr (NORM == 0) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                const int64_t j = c * n + i;
+                y2[j] = fminf(fmaxf(y2[j] + sg * h[c], -alpha), alpha);
+            }
+        } else {
+            float v[6];
+            float ss = 0.f;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                v[c] = y2[c * n + i] + sg * h[c];
+                ss += v[c] * v[c];
+            }
+            const float sc = fmaxf(sqrtf(ss + 1e-12f) / alpha, 1.f);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) y2[c * n + i] = v[c] / sc;
+        }
+    }
+}
+
+// x_new = max(0, x - tau (A^T y1 + H^T y2)) with the FP64 sums of k_primal.
+__global__ void __launch_bounds__(256) k_hess_primal(PdhgDev* s, const float* __restrict__ xc,
+                                                     const float* __restrict__ aty,
+                                                     const float* __restrict__ y2,
+                                                     float* __restrict__ xn, Dims d, W6 w) {
+    if (s->stop) return;
+    const float tau = (float)s->tau;
+    const int64_t n = d.nz * d.ny * d.nx;
+    double dx2 = 0.0, xc2 = 0.0, xn2 = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t x = i % d.nx, t = i / d.nx, y = t % d.ny, z = t / d.ny;
+        const float a = xc[i];
+        const float g = aty[i] + hess_adj_at(y2, z, y, x, d, w.w);
+        const float v = fmaxf(a - tau * g, 0.f);
+        xn[i] = v;
+        const float dd = v - a;
+        dx2 += (double)dd * dd;
+        xc2 += (double)a * a;
+        xn2 += (double)v * v;
+    }
+    put_partial(s, kSlotDx2, dx2);
+    put_partial(s, kSlotXc2, xc2);
+    put_partial(s, kSlotXn2, xn2);
+}
+
+// ||A x_new - A x||^2 (slot DA2) and ||H (x_new - x)||^2 (slot DL2).
+__global__ void __launch_bounds__(256) k_hess_dk(PdhgDev* s, const float* __restrict__ axn,
+                                                 const float* __restrict__ axc, int64_t m,
+                                                 const float* __restrict__ xn,
+                                                 const float* __restrict__ xc, Dims d, W6 w) {
+    if (s->stop) return;
+    double a2 = 0.0, l2 = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double dd = (double)axn[i] - (double)axc[i];
+        a2 += dd * dd;
+    }
+    const DiffField f{xn, xc, d.ny, d.nx};
+    const int64_t n = d.nz * d.ny * d.nx;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t x = i % d.nx, t = i / d.nx, y = t % d.ny, z = t / d.ny;
+        float h[6];
+        hess6(f, z, y, x, d, w.w, h);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) l2 += (double)h[c] * (double)h[c];
+    }
+    put_partial(s, kSlotDA2, a2);
+    put_partial(s, kSlotDL2, l2);
+}
+
+// Regulariser part of the objective on H x (pdhg_mlx.py:873-879).
+template <int NORM>
+__global__ void __launch_bounds__(256) k_hess_regloss(PdhgDev* s, const float* __restrict__ x,
+                                                      Dims d, W6 w, int kk) {
+    if (!loss_active(s, kk)) return;
+    const PlainField f{x, d.ny, d.nx};
+    const int64_t n = d.nz * d.ny * d.nx;
+    double acc = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t xx = i % d.nx, t = i / d.nx, y = t % d.ny, z = t / d.ny;
+        float h[6];
+        hess6(f, z, y, xx, d, w.w, h);
+        if constexpr (NORM == 0) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) acc += fabs((double)h[c]);
+        } else {
+            float ss = 0.f;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) ss += h[c] * h[c];
+            acc += (double)sqrtf(ss + 1e-12f);
+        }
+    }
+    put_partial(s, kSlotReg, acc);
+}
+
 // ---- RL element-wise steps for composed operators (rl_mlx.py:146-150) -------
 
 __global__ void k_rl_ratio(const float* __restrict__ model, const float* __restrict__ y, float bg,
@@ -480,6 +630,64 @@ int decon_pdhg_loss(decon_pdhg* h, const float* ax, const float* data, float bac
     DK_LAUNCHED();
     if (norm == 0) k_loss_reg<0><<<kPdhgGrid, 256, 0, s>>>(h->dev, lx, ncomp, n, k);
     else k_loss_reg<1><<<kPdhgGrid, 256, 0, s>>>(h->dev, lx, ncomp, n, k);
+    DK_LAUNCHED();
+    k_record_loss<<<1, 256, 0, s>>>(h->dev, alpha, k);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_pdhg_hess_dual(decon_pdhg* h, float* y2, const float* xc, const float* xp,
+                         const int64_t shape[3], float r, float alpha, int norm, void* stream) {
+    if (!h || !y2 || !xc || !xp || !shape) return fail(DECON_ERR_NULL, "null pointer");
+    W6 w;
+    hessian_weights(r, w.w);
+    const Dims d{shape[0], shape[1], shape[2]};
+    const int64_t n = d.nz * d.ny * d.nx;
+    if (norm == 0)
+        k_hess_dual<0><<<g1(n), 256, 0, as_stream(stream)>>>(h->dev, y2, xc, xp, d, w, alpha);
+    else
+        k_hess_dual<1><<<g1(n), 256, 0, as_stream(stream)>>>(h->dev, y2, xc, xp, d, w, alpha);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_pdhg_hess_primal(decon_pdhg* h, const float* xc, const float* aty, const float* y2,
+                           float* xn, const int64_t shape[3], float r, void* stream) {
+    if (!h || !xc || !aty || !y2 || !xn || !shape) return fail(DECON_ERR_NULL, "null pointer");
+    W6 w;
+    hessian_weights(r, w.w);
+    k_hess_primal<<<kPdhgGrid, 256, 0, as_stream(stream)>>>(h->dev, xc, aty, y2, xn,
+                                                            Dims{shape[0], shape[1], shape[2]}, w);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_pdhg_hess_dk(decon_pdhg* h, const float* ax_new, const float* ax_cur, int64_t m,
+                       const float* xn, const float* xc, const int64_t shape[3], float r,
+                       void* stream) {
+    if (!h || !ax_new || !ax_cur || !xn || !xc || !shape) return fail(DECON_ERR_NULL, "null pointer");
+    W6 w;
+    hessian_weights(r, w.w);
+    k_hess_dk<<<kPdhgGrid, 256, 0, as_stream(stream)>>>(h->dev, ax_new, ax_cur, m, xn, xc,
+                                                        Dims{shape[0], shape[1], shape[2]}, w);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_pdhg_hess_loss(decon_pdhg* h, const float* ax, const float* data, float background,
+                         int loss_type, int64_t m, const float* x, const int64_t shape[3], float r,
+                         int norm, double alpha, int k, void* stream) {
+    if (!h || !ax || !data || !x || !shape) return fail(DECON_ERR_NULL, "null pointer");
+    if (k < 0 || k >= std::max(h->num_iter, 1)) return fail(DECON_ERR_VALUE, "loss index out of range");
+    W6 w;
+    hessian_weights(r, w.w);
+    const Dims d{shape[0], shape[1], shape[2]};
+    const cudaStream_t s = as_stream(stream);
+    if (loss_type == 0) k_loss_data<0><<<kPdhgGrid, 256, 0, s>>>(h->dev, ax, data, background, m, k);
+    else k_loss_data<1><<<kPdhgGrid, 256, 0, s>>>(h->dev, ax, data, background, m, k);
+    DK_LAUNCHED();
+    if (norm == 0) k_hess_regloss<0><<<kPdhgGrid, 256, 0, s>>>(h->dev, x, d, w, k);
+    else k_hess_regloss<1><<<kPdhgGrid, 256, 0, s>>>(h->dev, x, d, w, k);
     DK_LAUNCHED();
     k_record_loss<<<1, 256, 0, s>>>(h->dev, alpha, k);
     DK_LAUNCHED();

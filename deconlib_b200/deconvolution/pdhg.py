@@ -310,7 +310,7 @@ class PDHGRunner:
 
     def __init__(self, data, A, reg, x0, alpha, loss_type, num_iter, background, delta, eta,
                  eval_interval, tol, min_iter, patience, verbose=False, callback=None,
-                 generic=False):
+                 generic=False, fused=True):
         self.s = stream()
         self.data, self.A, self.reg = data, A, reg
         self.alpha = float(alpha)
@@ -341,6 +341,13 @@ class PDHGRunner:
         self.want_loss_each = generic and (verbose or callback is not None)
         self.stopped_at = None
         self.k = 0
+        # fused Hessian3D kernels (fused=False keeps the operator-by-operator path)
+        self.fused = (fused and isinstance(reg, HessianRegularizer) and reg.ndim == 3
+                      and x0.dim() == 3)
+        if self.fused:
+            self.shp = _lib.i64arr(tuple(x0.shape))
+            self.r = float(reg.r)
+            self.xbar = self.dxb = None
 
     def iterate(self) -> bool:
         """Queue iteration k; returns False once the solve has stopped."""
@@ -353,26 +360,44 @@ class PDHGRunner:
         _lib.call("decon_pdhg_dual_data", h, _lib.ptr(self.y1), _lib.ptr(axc), _lib.ptr(axp),
                   _lib.ptr(self.data), C.c_float(self.bg), self.lcode, m, s)
         aty = to_device(A.adjoint(self.y1))
-        _lib.call("decon_pdhg_xbar", h, _lib.ptr(xc), _lib.ptr(xp), _lib.ptr(self.xbar), n, s)
-        lxb = to_device(reg.forward(self.xbar))
-        _lib.call("decon_pdhg_dual_reg", h, _lib.ptr(self.y2), _lib.ptr(lxb), C.c_float(self.alpha),
-                  self.ncode, self.ncomp, n, s)
-        lty = to_device(reg.adjoint(self.y2))
-        _lib.call("decon_pdhg_primal", h, _lib.ptr(xc), _lib.ptr(aty), _lib.ptr(lty), _lib.ptr(xp),
-                  n, s)
-        xn = xp
-        axn = to_device(A.forward(xn))
-        _lib.call("decon_pdhg_sub", h, _lib.ptr(xn), _lib.ptr(xc), _lib.ptr(self.dxb), n, s)
-        ldx = to_device(reg.forward(self.dxb))
-        _lib.call("decon_pdhg_dk", h, _lib.ptr(axn), _lib.ptr(axc), m, _lib.ptr(ldx), ldx.numel(), s)
-        _lib.call("decon_pdhg_step", h, s)
-        self.AX[(k + 1) % 2] = axn
         do_loss = self.want_loss_each or ((not self.generic) and (k + 1) % self.eval_interval == 0)
-        if do_loss:
-            lx = to_device(reg.forward(xn))
-            _lib.call("decon_pdhg_loss", h, _lib.ptr(axn), _lib.ptr(self.data), C.c_float(self.bg),
-                      self.lcode, m, _lib.ptr(lx), self.ncode, self.ncomp, n,
-                      C.c_double(self.alpha), k, s)
+        if self.fused:
+            # Hessian3D: L x_bar, L^T y2 and L (x_new - x) evaluated on the fly
+            shp, r = self.shp, C.c_float(self.r)
+            _lib.call("decon_pdhg_hess_dual", h, _lib.ptr(self.y2), _lib.ptr(xc), _lib.ptr(xp), shp,
+                      r, C.c_float(self.alpha), self.ncode, s)
+            _lib.call("decon_pdhg_hess_primal", h, _lib.ptr(xc), _lib.ptr(aty), _lib.ptr(self.y2),
+                      _lib.ptr(xp), shp, r, s)
+            xn = xp
+            axn = to_device(A.forward(xn))
+            _lib.call("decon_pdhg_hess_dk", h, _lib.ptr(axn), _lib.ptr(axc), m, _lib.ptr(xn),
+                      _lib.ptr(xc), shp, r, s)
+            _lib.call("decon_pdhg_step", h, s)
+            if do_loss:
+                _lib.call("decon_pdhg_hess_loss", h, _lib.ptr(axn), _lib.ptr(self.data),
+                          C.c_float(self.bg), self.lcode, m, _lib.ptr(xn), shp, r, self.ncode,
+                          C.c_double(self.alpha), k, s)
+        else:
+            _lib.call("decon_pdhg_xbar", h, _lib.ptr(xc), _lib.ptr(xp), _lib.ptr(self.xbar), n, s)
+            lxb = to_device(reg.forward(self.xbar))
+            _lib.call("decon_pdhg_dual_reg", h, _lib.ptr(self.y2), _lib.ptr(lxb),
+                      C.c_float(self.alpha), self.ncode, self.ncomp, n, s)
+            lty = to_device(reg.adjoint(self.y2))
+            _lib.call("decon_pdhg_primal", h, _lib.ptr(xc), _lib.ptr(aty), _lib.ptr(lty),
+                      _lib.ptr(xp), n, s)
+            xn = xp
+            axn = to_device(A.forward(xn))
+            _lib.call("decon_pdhg_sub", h, _lib.ptr(xn), _lib.ptr(xc), _lib.ptr(self.dxb), n, s)
+            ldx = to_device(reg.forward(self.dxb))
+            _lib.call("decon_pdhg_dk", h, _lib.ptr(axn), _lib.ptr(axc), m, _lib.ptr(ldx), ldx.numel(),
+                      s)
+            _lib.call("decon_pdhg_step", h, s)
+            if do_loss:
+                lx = to_device(reg.forward(xn))
+                _lib.call("decon_pdhg_loss", h, _lib.ptr(axn), _lib.ptr(self.data),
+                          C.c_float(self.bg), self.lcode, m, _lib.ptr(lx), self.ncode, self.ncomp,
+                          n, C.c_double(self.alpha), k, s)
+        self.AX[(k + 1) % 2] = axn
         self.k = k + 1
         cb, verbose = self.callback, self.verbose
         if cb is not None or (verbose and do_loss) or self.k % _CHUNK == 0:

@@ -171,6 +171,23 @@ int decon_pdhg_step(decon_pdhg* h, void* stream);
 int decon_pdhg_loss(decon_pdhg* h, const float* ax, const float* data, float background,
                     int loss_type, int64_t m, const float* lx, int norm, int ncomp, int64_t n,
                     double alpha, int k, void* stream);
+/* Fused Hessian3D forms of the regulariser half (L = Hessian3D(r), shape
+ * (z, y, x)); the Hessian is evaluated on the fly, never stored:
+ *   hess_dual:   y2 = proj(y2 + sigma H x_bar), x_bar = x + theta (x - x_prev)
+ *   hess_primal: x_new = max(0, x - tau (aty + H^T y2)) + the FP64 sums of
+ *                decon_pdhg_primal
+ *   hess_dk:     ||A x_new - A x||^2 and ||H (x_new - x)||^2
+ *   hess_loss:   objective at iteration k with the H x_new norm fused. */
+int decon_pdhg_hess_dual(decon_pdhg* h, float* y2, const float* xc, const float* xp,
+                         const int64_t shape[3], float r, float alpha, int norm, void* stream);
+int decon_pdhg_hess_primal(decon_pdhg* h, const float* xc, const float* aty, const float* y2,
+                           float* xn, const int64_t shape[3], float r, void* stream);
+int decon_pdhg_hess_dk(decon_pdhg* h, const float* ax_new, const float* ax_cur, int64_t m,
+                       const float* xn, const float* xc, const int64_t shape[3], float r,
+                       void* stream);
+int decon_pdhg_hess_loss(decon_pdhg* h, const float* ax, const float* data, float background,
+                         int loss_type, int64_t m, const float* x, const int64_t shape[3], float r,
+                         int norm, double alpha, int k, void* stream);
 /* Reads the state (synchronises): iteration counter, final iteration,
  * converged and stop flags, (tau, sigma, theta) and the histories (host
  * arrays of num_iter doubles; any may be NULL). */

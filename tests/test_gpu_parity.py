@@ -275,3 +275,28 @@ def test_column_pass_variants_agree(D, monkeypatch, shape, fft):
         assert rel(a, outs[0][1]) < 1e-6
     from deconlib_b200 import _lib
     _lib.call("decon_device_status", _lib.stream_ptr())
+
+
+@pytest.mark.parametrize("norm", ["L1", "L1_2"])
+def test_pdhg_fused_hessian_matches_operator_path(D, g32, norm):
+    # The fused Hessian kernels evaluate the same float32 stencils as
+    # Hessian3D.forward / adjoint; only the FP64 summation order of
+    # ||L dx||^2 differs, so the trajectories agree to rounding.
+    from deconlib_b200.deconvolution.pdhg import (HessianRegularizer, PDHGRunner,
+                                                   _compute_spacing_ratio)
+    from deconlib_b200.deconvolution._device import to_device
+
+    data = to_device(g32["pd_obs"])
+    conv = D.LinearFFTConvolver(g32["psf_hr"], (16, 32, 32))
+    A = D.compose(D.FractionalAreaDownsample(2.0), conv)
+    reg = HessianRegularizer(3, _compute_spacing_ratio((0.05, 0.0425, 0.0425), 3), norm)
+    out = []
+    for fused in (True, False):
+        x0 = D.prox_nonneg(A.adjoint(data))
+        run = PDHGRunner(data, A, reg, x0, 1e-3, "poisson", 30, 5.0, 0.99, 0.5, 10, 1e-5, 20, 5,
+                         fused=fused)
+        assert run.fused == fused
+        out.append(run.run().result())
+    assert rel(out[0][0], cpu(out[1][0])) < 1e-6
+    np.testing.assert_allclose(out[0][3], out[1][3], rtol=1e-6)
+    np.testing.assert_allclose(out[0][5], out[1][5], rtol=1e-6)
