@@ -46,23 +46,41 @@ __global__ void k_window_copy(const float* __restrict__ src, float* __restrict__
     }
 }
 
-__global__ void k_banded(const float* __restrict__ in, float* __restrict__ out, int64_t outer,
-                         int64_t n_in, int64_t inner, int64_t n_out, const int32_t* __restrict__ idx,
-                         const float* __restrict__ w, int width) {
-    const int64_t n = outer * n_out * inner;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t q = i % inner;
-        const int64_t t = i / inner;
-        const int64_t o = t / n_out, j = t - o * n_out;
+// out[o, j, q] = sum_k w[j, k] in[o, idx[j, k], q], products rounded before
+// the in-order sum as mx.sum(gathered * weight, -1) does (no FMA contraction).
+// Resampled axis not innermost: one CTA row per (j, o), threads along q.
+__global__ void k_banded_inner(const float* __restrict__ in, float* __restrict__ out, int64_t outer,
+                               int64_t n_in, int64_t inner, int64_t n_out,
+                               const int32_t* __restrict__ idx, const float* __restrict__ w,
+                               int width) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= inner) return;
+    const int64_t j = blockIdx.y;
+    const int32_t* ij = idx + j * width;
+    const float* wj = w + j * width;
+    for (int64_t o = blockIdx.z; o < outer; o += gridDim.z) {
         const float* base = in + o * n_in * inner + q;
         float acc = 0.f;
-        // sum over the window in index order, as mx.sum(gathered * weight, -1)
-        for (int k = 0; k < width; ++k) {
-            const int64_t s = __ldg(idx + j * width + k);
-            acc += __ldg(w + j * width + k) * __ldg(base + s * inner);
-        }
-        out[i] = acc;
+        for (int k = 0; k < width; ++k)
+            acc = __fadd_rn(acc, __fmul_rn(__ldg(wj + k), __ldg(base + (int64_t)__ldg(ij + k) * inner)));
+        out[(o * n_out + j) * inner + q] = acc;
+    }
+}
+
+// Resampled axis innermost (inner == 1): threads along the output axis.
+__global__ void k_banded_last(const float* __restrict__ in, float* __restrict__ out, int64_t outer,
+                              int64_t n_in, int64_t n_out, const int32_t* __restrict__ idx,
+                              const float* __restrict__ w, int width) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n_out) return;
+    const int32_t* ij = idx + j * width;
+    const float* wj = w + j * width;
+    for (int64_t o = blockIdx.y; o < outer; o += gridDim.y) {
+        const float* base = in + o * n_in;
+        float acc = 0.f;
+        for (int k = 0; k < width; ++k)
+            acc = __fadd_rn(acc, __fmul_rn(__ldg(wj + k), __ldg(base + __ldg(ij + k))));
+        out[o * n_out + j] = acc;
     }
 }
 
@@ -220,8 +238,16 @@ int decon_banded_axis(const float* in, float* out, int64_t outer, int64_t n_in, 
         return fail(DECON_ERR_VALUE, "bad banded shape");
     const int64_t n = outer * n_out * inner;
     if (n == 0) return DECON_OK;
-    k_banded<<<grid1d(n, 256), 256, 0, as_stream(stream)>>>(in, out, outer, n_in, inner, n_out, idx,
-                                                            w, width);
+    const cudaStream_t st = as_stream(stream);
+    if (inner == 1) {
+        dim3 g((unsigned)cdiv(n_out, 256), (unsigned)std::min<int64_t>(outer, 65535));
+        k_banded_last<<<g, 256, 0, st>>>(in, out, outer, n_in, n_out, idx, w, width);
+    } else {
+        const int thr = inner >= 256 ? 256 : (int)round_up(inner, 32);
+        if (n_out > 65535) return fail(DECON_ERR_UNSUPPORTED, "resampled axis longer than 65535");
+        dim3 g((unsigned)cdiv(inner, thr), (unsigned)n_out, (unsigned)std::min<int64_t>(outer, 65535));
+        k_banded_inner<<<g, thr, 0, st>>>(in, out, outer, n_in, inner, n_out, idx, w, width);
+    }
     DK_LAUNCHED();
     return DECON_OK;
 }

@@ -1,0 +1,344 @@
+// Shared-memory tiled forms of the fused Hessian-PDHG kernels.
+//
+// A CTA of 32 x 8 threads owns an (x, y) tile and marches along z through a
+// chunk of kZChunk planes.  The field the stencil reads is staged plane by
+// plane, with a one-voxel halo, into shared memory (a ring of three planes
+// for the axes that need z -+ 1), so every neighbour value comes from global
+// memory about once instead of once per stencil tap.  The arithmetic is the
+// shared stencil code (hess6 / hess_adj_gen) with shared-memory accessors, so
+// the results equal the untiled kernels bit for bit.  CTAs walk a fixed list
+// of tiles (tile b, b + grid, ...) so the FP64 partial sums are per-CTA and
+// deterministic.
+#pragma once
+
+#include "solvers.cuh"
+#include "stencil.cuh"
+
+namespace dk {
+
+constexpr int kTX = 32, kTY = 8, kHX = kTX + 2, kHY = kTY + 2, kPL = kHX * kHY;
+constexpr int kZChunk = 16;
+
+struct TileGeo {
+    int64_t ntx, nty, ntz, ntiles;
+    __host__ __device__ TileGeo(const Dims& d)
+        : ntx((d.nx + kTX - 1) / kTX), nty((d.ny + kTY - 1) / kTY),
+          ntz((d.nz + kZChunk - 1) / kZChunk), ntiles(0) {
+        ntiles = ntx * nty * ntz;
+    }
+};
+
+__device__ __forceinline__ int sidx(int64_t yy, int64_t xx, int64_t y0, int64_t x0) {
+    return (int)((yy - y0 + 1) * kHX + (xx - x0 + 1));
+}
+
+// This thread's (up to two) halo-plane elements: fixed (row, column) of the
+// staged tile, loaded into registers one plane ahead of use.
+struct StageSlots {
+    int q[2];
+    int64_t off[2];  // in-plane offset (clamped y, x)
+    bool ok[2];
+    __device__ __forceinline__ StageSlots(int64_t x0, int64_t y0, const Dims& d) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            q[u] = threadIdx.x + u * blockDim.x;
+            ok[u] = q[u] < kPL;
+            const int ly = q[u] / kHX, lx = q[u] - ly * kHX;
+            off[u] = clampi(y0 - 1 + ly, d.ny) * d.nx + clampi(x0 - 1 + lx, d.nx);
+        }
+    }
+    // f(plane_offset + in_plane_offset) for plane zz
+    template <class F>
+    __device__ __forceinline__ void load(float r[2], const F& f, int64_t zz, int64_t plane) const {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) r[u] = ok[u] ? f(zz * plane + off[u]) : 0.f;
+    }
+    __device__ __forceinline__ void store(float* p, const float r[2]) const {
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+            if (ok[u]) p[q[u]] = r[u];
+    }
+};
+
+// Hessian components at tile-local (ly, lx) (1-based, halo at 0 and kT+1)
+// from staged planes: clamping is already in the staged values, so the taps
+// are plain neighbours; the float ops are those of hess6.
+__device__ __forceinline__ void hess6_smem(const float* pm, const float* p0, const float* pp, int ly,
+                                           int lx, const float w[6], float h[6]) {
+    const int c = ly * kHX + lx;
+    const int n = c - kHX, s = c + kHX, wv = c - 1, e = c + 1;
+    const float cv = p0[c];
+    const float hzz = d2v(pm[c], cv, pp[c]);
+    const float hyy = d2v(p0[n], cv, p0[s]);
+    const float hxx = d2v(p0[wv], cv, p0[e]);
+    const float dz_yp = (pp[s] - pm[s]) / 2.f;
+    const float dz_ym = (pp[n] - pm[n]) / 2.f;
+    const float hyz = (dz_yp - dz_ym) / 2.f;
+    const float dz_xp = (pp[e] - pm[e]) / 2.f;
+    const float dz_xm = (pp[wv] - pm[wv]) / 2.f;
+    const float hxz = (dz_xp - dz_xm) / 2.f;
+    const float dy_xp = (p0[s + 1] - p0[n + 1]) / 2.f;
+    const float dy_xm = (p0[s - 1] - p0[n - 1]) / 2.f;
+    const float hxy = (dy_xp - dy_xm) / 2.f;
+    h[0] = hzz * w[0];
+    h[1] = hyy * w[1];
+    h[2] = hxx * w[2];
+    h[3] = hyz * w[3];
+    h[4] = hxz * w[4];
+    h[5] = hxy * w[5];
+}
+
+// Boundary flags of a voxel: d1_cen_adj negates the edge-replicated value one
+// step outside the volume (G(-1) = -g[0], G(n) = -g[n-1]).
+struct Edge {
+    float zlo, zhi, ylo, yhi, xlo, xhi;  // -1 at the matching volume edge, else +1
+};
+
+// d1_cen_adj along a of (inner) then b of a staged component; a/b steps are
+// in-tile offsets (da, db are the index steps of axes a and b; planes for b = z).
+__device__ __forceinline__ float inner_s(const float* p, int c, int da, float slo, float shi, float w) {
+    return (slo * (p[c - da] * w) - shi * (p[c + da] * w)) / 2.f;
+}
+
+// Hessian3D.adjoint at tile-local (ly, lx) from staged components:
+// g0/g3/g4 as (prev, cur, next) plane triples, g1/g2/g5 in plane z.
+__device__ __forceinline__ float hess_adj_smem(const float* g0m, const float* g0c, const float* g0p,
+                                               const float* g1, const float* g2,
+                                               const float* g3m, const float* g3p,
+                                               const float* g4m, const float* g4p, const float* g5,
+                                               int ly, int lx, const Edge& e, const float w[6]) {
+    const int c = ly * kHX + lx;
+    const float azz = d2v(g0m[c] * w[0], g0c[c] * w[0], g0p[c] * w[0]);
+    const float ayy = d2v(g1[c - kHX] * w[1], g1[c] * w[1], g1[c + kHX] * w[1]);
+    const float axx = d2v(g2[c - 1] * w[2], g2[c] * w[2], g2[c + 1] * w[2]);
+    // yz: outer z (planes; at a z edge the staged neighbour plane is plane z
+    // itself and the row is negated), inner y
+    const float ayz = (e.zlo * inner_s(g3m, c, kHX, e.ylo, e.yhi, w[3]) -
+                       e.zhi * inner_s(g3p, c, kHX, e.ylo, e.yhi, w[3])) / 2.f;
+    // xz: outer z, inner x
+    const float axz = (e.zlo * inner_s(g4m, c, 1, e.xlo, e.xhi, w[4]) -
+                       e.zhi * inner_s(g4p, c, 1, e.xlo, e.xhi, w[4])) / 2.f;
+    // xy: outer y (rows c -+ kHX in plane z), inner x
+    const float axy = (e.ylo * inner_s(g5, c - kHX, 1, e.xlo, e.xhi, w[5]) -
+                       e.yhi * inner_s(g5, c + kHX, 1, e.xlo, e.xhi, w[5])) / 2.f;
+    return ((((azz + ayy) + axx) + ayz) + axz) + axy;
+}
+
+// Forward Hessian over every tile of the CTA: op(i, h[6]) per in-range voxel.
+// Plane z + 2 is loaded into registers while plane z is computed.
+template <class F, class OP>
+__device__ __forceinline__ void tiled_hess_forward(const F& f, const Dims& d, const float w[6],
+                                                   OP op) {
+    __shared__ float ring[3][kPL];
+    const TileGeo g(d);
+    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+    const int64_t plane = d.ny * d.nx;
+    for (int64_t tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
+        const int64_t bx = tile % g.ntx, r = tile / g.ntx, by = r % g.nty, bz = r / g.nty;
+        const int64_t x0 = bx * kTX, y0 = by * kTY, z0 = bz * kZChunk;
+        const int64_t z1 = min(z0 + kZChunk, d.nz);
+        const int64_t x = x0 + tx, y = y0 + ty;
+        const bool in = x < d.nx && y < d.ny;
+        const int64_t ipl = y * d.nx + x;
+        const StageSlots st(x0, y0, d);
+        float pre[2];
+        st.load(pre, f, clampi(z0 - 1, d.nz), plane);
+        st.store(ring[0], pre);
+        st.load(pre, f, z0, plane);
+        st.store(ring[1], pre);
+        st.load(pre, f, clampi(z0 + 1, d.nz), plane);
+        for (int64_t z = z0; z < z1; ++z) {
+            const int sp = (int)((z - z0) % 3), sc = (int)((z - z0 + 1) % 3),
+                      sn = (int)((z - z0 + 2) % 3);
+            st.store(ring[sn], pre);
+            __syncthreads();
+            if (z + 1 < z1) st.load(pre, f, clampi(z + 2, d.nz), plane);
+            if (in) {
+                float h[6];
+                hess6_smem(ring[sp], ring[sc], ring[sn], ty + 1, tx + 1, w, h);
+                op(z * plane + ipl, h);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <int NORM>
+__global__ void __launch_bounds__(256) k_hess_dual_t(PdhgDev* s, float* __restrict__ y2,
+                                                     const float* __restrict__ xc,
+                                                     const float* __restrict__ xp, Dims d, W6 w,
+                                                     float alpha) {
+    if (s->stop) return;
+    const float sg = (float)s->sigma, th = (float)s->theta;
+    const int64_t n = d.nz * d.ny * d.nx;
+    auto xbar = [&](int64_t i) -> float {
+        const float a = __ldg(xc + i);
+        return a + th * (a - __ldg(xp + i));
+    };
+    tiled_hess_forward(xbar, d, w.w, [&](int64_t i, const float* h) {
+        if constexpr (NORM == 0) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                const int64_t j = c * n + i;
+                y2[j] = fminf(fmaxf(y2[j] + sg * h[c], -alpha), alpha);
+            }
+        } else {
+            float v[6];
+            float ss = 0.f;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                v[c] = y2[c * n + i] + sg * h[c];
+                ss += v[c] * v[c];
+            }
+            const float sc = fmaxf(sqrtf(ss + 1e-12f) / alpha, 1.f);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) y2[c * n + i] = v[c] / sc;
+        }
+    });
+}
+
+__device__ __forceinline__ void put_slot(PdhgDev* s, int slot, double v) {
+    const double b = block_sum(v);
+    if (threadIdx.x == 0) s->partials[slot * kPdhgGrid + blockIdx.x] = b;
+}
+
+// ||A x_new - A x||^2 and ||H (x_new - x)||^2.
+__global__ void __launch_bounds__(256) k_hess_dk_t(PdhgDev* s, const float* __restrict__ axn,
+                                                   const float* __restrict__ axc, int64_t m,
+                                                   const float* __restrict__ xn,
+                                                   const float* __restrict__ xc, Dims d, W6 w,
+                                                   int slot_a, int slot_l) {
+    if (s->stop) return;
+    double a2 = 0.0, l2 = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double dd = (double)axn[i] - (double)axc[i];
+        a2 += dd * dd;
+    }
+    auto diff = [&](int64_t i) -> float { return __ldg(xn + i) - __ldg(xc + i); };
+    tiled_hess_forward(diff, d, w.w, [&](int64_t, const float* h) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) l2 += (double)h[c] * (double)h[c];
+    });
+    put_slot(s, slot_a, a2);
+    put_slot(s, slot_l, l2);
+}
+
+template <int NORM>
+__global__ void __launch_bounds__(256) k_hess_regloss_t(PdhgDev* s, const float* __restrict__ x,
+                                                        Dims d, W6 w, int kk, int slot) {
+    if (!(kk < s->final_iter && !(s->converged && kk == s->final_iter - 1))) return;
+    double acc = 0.0;
+    auto plain = [&](int64_t i) -> float { return __ldg(x + i); };
+    tiled_hess_forward(plain, d, w.w, [&](int64_t, const float* h) {
+        if constexpr (NORM == 0) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) acc += fabs((double)h[c]);
+        } else {
+            float ss = 0.f;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) ss += h[c] * h[c];
+            acc += (double)sqrtf(ss + 1e-12f);
+        }
+    });
+    put_slot(s, slot, acc);
+}
+
+// x_new = max(0, x - tau (A^T y1 + H^T y2)) with H^T y2 from staged planes:
+// components 0, 3, 4 (read at z -+ 1) in rings of three planes, components
+// 1, 2, 5 (read in plane z only) one plane each.
+__global__ void __launch_bounds__(256) k_hess_primal_t(PdhgDev* s, const float* __restrict__ xc,
+                                                       const float* __restrict__ aty,
+                                                       const float* __restrict__ y2,
+                                                       float* __restrict__ xn, Dims d, W6 w,
+                                                       int s_dx2, int s_xc2, int s_xn2) {
+    if (s->stop) return;
+    __shared__ float rz[3][3][kPL];  // components 0, 3, 4
+    __shared__ float pz[3][kPL];     // components 1, 2, 5
+    const float tau = (float)s->tau;
+    const int64_t n = d.nz * d.ny * d.nx, plane = d.ny * d.nx;
+    const TileGeo g(d);
+    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+    double dx2 = 0.0, xc2 = 0.0, xn2 = 0.0;
+    auto comp = [&](int c) { return [=](int64_t i) -> float { return __ldg(y2 + c * n + i); }; };
+    const auto c0 = comp(0), c1 = comp(1), c2 = comp(2), c3 = comp(3), c4 = comp(4), c5 = comp(5);
+    for (int64_t tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
+        const int64_t bx = tile % g.ntx, r = tile / g.ntx, by = r % g.nty, bz = r / g.nty;
+        const int64_t x0 = bx * kTX, y0 = by * kTY, z0 = bz * kZChunk;
+        const int64_t z1 = min(z0 + kZChunk, d.nz);
+        const int64_t x = x0 + tx, y = y0 + ty;
+        const bool in = x < d.nx && y < d.ny;
+        const int64_t ipl = y * d.nx + x;
+        Edge e;
+        e.ylo = y == 0 ? -1.f : 1.f;
+        e.yhi = y == d.ny - 1 ? -1.f : 1.f;
+        e.xlo = x == 0 ? -1.f : 1.f;
+        e.xhi = x == d.nx - 1 ? -1.f : 1.f;
+        const StageSlots st(x0, y0, d);
+        float p0[2], p3[2], p4[2], p1[2], p2[2], p5[2];
+        const int64_t zb = clampi(z0 - 1, d.nz);
+        st.load(p0, c0, zb, plane);
+        st.load(p3, c3, zb, plane);
+        st.load(p4, c4, zb, plane);
+        st.store(rz[0][0], p0);
+        st.store(rz[1][0], p3);
+        st.store(rz[2][0], p4);
+        st.load(p0, c0, z0, plane);
+        st.load(p3, c3, z0, plane);
+        st.load(p4, c4, z0, plane);
+        st.store(rz[0][1], p0);
+        st.store(rz[1][1], p3);
+        st.store(rz[2][1], p4);
+        {
+            const int64_t zn = clampi(z0 + 1, d.nz);
+            st.load(p0, c0, zn, plane);
+            st.load(p3, c3, zn, plane);
+            st.load(p4, c4, zn, plane);
+            st.load(p1, c1, z0, plane);
+            st.load(p2, c2, z0, plane);
+            st.load(p5, c5, z0, plane);
+        }
+        for (int64_t z = z0; z < z1; ++z) {
+            const int sp = (int)((z - z0) % 3), sc = (int)((z - z0 + 1) % 3),
+                      sn = (int)((z - z0 + 2) % 3);
+            st.store(rz[0][sn], p0);
+            st.store(rz[1][sn], p3);
+            st.store(rz[2][sn], p4);
+            st.store(pz[0], p1);
+            st.store(pz[1], p2);
+            st.store(pz[2], p5);
+            __syncthreads();
+            if (z + 1 < z1) {
+                const int64_t zn = clampi(z + 2, d.nz);
+                st.load(p0, c0, zn, plane);
+                st.load(p3, c3, zn, plane);
+                st.load(p4, c4, zn, plane);
+                st.load(p1, c1, z + 1, plane);
+                st.load(p2, c2, z + 1, plane);
+                st.load(p5, c5, z + 1, plane);
+            }
+            if (in) {
+                e.zlo = z == 0 ? -1.f : 1.f;
+                e.zhi = z == d.nz - 1 ? -1.f : 1.f;
+                const int64_t i = z * plane + ipl;
+                const float a = xc[i];
+                const float lt = hess_adj_smem(rz[0][sp], rz[0][sc], rz[0][sn], pz[0], pz[1],
+                                               rz[1][sp], rz[1][sn], rz[2][sp], rz[2][sn], pz[2],
+                                               ty + 1, tx + 1, e, w.w);
+                const float gr = aty[i] + lt;
+                const float v = fmaxf(a - tau * gr, 0.f);
+                xn[i] = v;
+                const float dd = v - a;
+                dx2 += (double)dd * dd;
+                xc2 += (double)a * a;
+                xn2 += (double)v * v;
+            }
+            __syncthreads();
+        }
+    }
+    put_slot(s, s_dx2, dx2);
+    put_slot(s, s_xc2, xc2);
+    put_slot(s, s_xn2, xn2);
+}
+
+}  // namespace dk

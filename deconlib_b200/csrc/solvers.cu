@@ -12,6 +12,7 @@
 #include "conv_impl.cuh"
 #include "solvers.cuh"
 #include "stencil.cuh"
+#include "pdhg_tiled.cuh"
 
 namespace dk {
 
@@ -643,10 +644,13 @@ int decon_pdhg_hess_dual(decon_pdhg* h, float* y2, const float* xc, const float*
     hessian_weights(r, w.w);
     const Dims d{shape[0], shape[1], shape[2]};
     const int64_t n = d.nz * d.ny * d.nx;
+    (void)n;
+    const TileGeo tg(d);
+    const int grid = (int)std::min<int64_t>(tg.ntiles, (int64_t)sm_count() * 8);
     if (norm == 0)
-        k_hess_dual<0><<<g1(n), 256, 0, as_stream(stream)>>>(h->dev, y2, xc, xp, d, w, alpha);
+        k_hess_dual_t<0><<<grid, 256, 0, as_stream(stream)>>>(h->dev, y2, xc, xp, d, w, alpha);
     else
-        k_hess_dual<1><<<g1(n), 256, 0, as_stream(stream)>>>(h->dev, y2, xc, xp, d, w, alpha);
+        k_hess_dual_t<1><<<grid, 256, 0, as_stream(stream)>>>(h->dev, y2, xc, xp, d, w, alpha);
     DK_LAUNCHED();
     return DECON_OK;
 }
@@ -656,8 +660,8 @@ int decon_pdhg_hess_primal(decon_pdhg* h, const float* xc, const float* aty, con
     if (!h || !xc || !aty || !y2 || !xn || !shape) return fail(DECON_ERR_NULL, "null pointer");
     W6 w;
     hessian_weights(r, w.w);
-    k_hess_primal<<<kPdhgGrid, 256, 0, as_stream(stream)>>>(h->dev, xc, aty, y2, xn,
-                                                            Dims{shape[0], shape[1], shape[2]}, w);
+    k_hess_primal_t<<<kPdhgGrid, 256, 0, as_stream(stream)>>>(
+        h->dev, xc, aty, y2, xn, Dims{shape[0], shape[1], shape[2]}, w, kSlotDx2, kSlotXc2, kSlotXn2);
     DK_LAUNCHED();
     return DECON_OK;
 }
@@ -668,8 +672,8 @@ int decon_pdhg_hess_dk(decon_pdhg* h, const float* ax_new, const float* ax_cur, 
     if (!h || !ax_new || !ax_cur || !xn || !xc || !shape) return fail(DECON_ERR_NULL, "null pointer");
     W6 w;
     hessian_weights(r, w.w);
-    k_hess_dk<<<kPdhgGrid, 256, 0, as_stream(stream)>>>(h->dev, ax_new, ax_cur, m, xn, xc,
-                                                        Dims{shape[0], shape[1], shape[2]}, w);
+    k_hess_dk_t<<<kPdhgGrid, 256, 0, as_stream(stream)>>>(
+        h->dev, ax_new, ax_cur, m, xn, xc, Dims{shape[0], shape[1], shape[2]}, w, kSlotDA2, kSlotDL2);
     DK_LAUNCHED();
     return DECON_OK;
 }
@@ -686,8 +690,8 @@ int decon_pdhg_hess_loss(decon_pdhg* h, const float* ax, const float* data, floa
     if (loss_type == 0) k_loss_data<0><<<kPdhgGrid, 256, 0, s>>>(h->dev, ax, data, background, m, k);
     else k_loss_data<1><<<kPdhgGrid, 256, 0, s>>>(h->dev, ax, data, background, m, k);
     DK_LAUNCHED();
-    if (norm == 0) k_hess_regloss<0><<<kPdhgGrid, 256, 0, s>>>(h->dev, x, d, w, k);
-    else k_hess_regloss<1><<<kPdhgGrid, 256, 0, s>>>(h->dev, x, d, w, k);
+    if (norm == 0) k_hess_regloss_t<0><<<kPdhgGrid, 256, 0, s>>>(h->dev, x, d, w, k, kSlotReg);
+    else k_hess_regloss_t<1><<<kPdhgGrid, 256, 0, s>>>(h->dev, x, d, w, k, kSlotReg);
     DK_LAUNCHED();
     k_record_loss<<<1, 256, 0, s>>>(h->dev, alpha, k);
     DK_LAUNCHED();

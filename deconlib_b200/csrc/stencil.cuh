@@ -79,19 +79,75 @@ __device__ __forceinline__ float d2w(const float* g, int64_t i, int64_t n, int64
     return d2v(fm, f0, fp);
 }
 
-// Hessian3D.adjoint at voxel (z, y, x) of the six components hw[c * n + i]
-// (linops_mlx.py:244-259): the six adjoint stencils summed in the reference's order.
+// Hessian3D.adjoint at voxel (z, y, x) (linops_mlx.py:244-259) for any
+// accessor G(c, z, y, x) -> component c at in-range coordinates: the six
+// adjoint stencils (weights applied per element, boundary sign flips of
+// d1_cen_adj) summed in the reference's order.  The global-memory and the
+// shared-memory tiled kernels both use this one definition.
+template <class G>
+__device__ __forceinline__ float hess_adj_gen(const G& g, int64_t z, int64_t y, int64_t x,
+                                              const Dims& d, const float w[6]) {
+    // d2 of the weighted component c along one axis, edge-replicated
+    const float azz = d2v(g(0, clampi(z - 1, d.nz), y, x) * w[0], g(0, z, y, x) * w[0],
+                          g(0, clampi(z + 1, d.nz), y, x) * w[0]);
+    const float ayy = d2v(g(1, z, clampi(y - 1, d.ny), x) * w[1], g(1, z, y, x) * w[1],
+                          g(1, z, clampi(y + 1, d.ny), x) * w[1]);
+    const float axx = d2v(g(2, z, y, clampi(x - 1, d.nx)) * w[2], g(2, z, y, x) * w[2],
+                          g(2, z, y, clampi(x + 1, d.nx)) * w[2]);
+    // d1_cen_adj(d1_cen_adj(., inner axis), outer axis); G(-1) = -g[0], G(n) = -g[n-1]
+    auto ext = [&](int c, int64_t zz, int64_t yy, int64_t xx, int axis, float wc) -> float {
+        int64_t n = axis == 0 ? d.nz : (axis == 1 ? d.ny : d.nx);
+        int64_t v = axis == 0 ? zz : (axis == 1 ? yy : xx);
+        const bool neg = v < 0 || v >= n;
+        const int64_t cl = v < 0 ? 0 : (v >= n ? n - 1 : v);
+        if (axis == 0) zz = cl;
+        else if (axis == 1) yy = cl;
+        else xx = cl;
+        const float val = g(c, zz, yy, xx) * wc;
+        return neg ? -val : val;
+    };
+    // inner adjoint along axis a at outer index ob (axis b), evaluated at point p
+    auto inner = [&](int c, int b, int64_t ob, int a, int64_t z0, int64_t y0, int64_t x0,
+                     float wc) -> float {
+        int64_t zz = z0, yy = y0, xx = x0;
+        if (b == 0) zz = ob;
+        else if (b == 1) yy = ob;
+        else xx = ob;
+        int64_t zm = zz, ym = yy, xm = xx, zp = zz, yp = yy, xp = xx;
+        if (a == 0) { zm -= 1; zp += 1; }
+        else if (a == 1) { ym -= 1; yp += 1; }
+        else { xm -= 1; xp += 1; }
+        return (ext(c, zm, ym, xm, a, wc) - ext(c, zp, yp, xp, a, wc)) / 2.f;
+    };
+    auto mixed = [&](int c, int b, int a, float wc) -> float {
+        const int64_t nb = b == 0 ? d.nz : (b == 1 ? d.ny : d.nx);
+        const int64_t ib = b == 0 ? z : (b == 1 ? y : x);
+        auto row = [&](int64_t jb) -> float {
+            if (jb < 0) return -inner(c, b, 0, a, z, y, x, wc);
+            if (jb >= nb) return -inner(c, b, nb - 1, a, z, y, x, wc);
+            return inner(c, b, jb, a, z, y, x, wc);
+        };
+        return (row(ib - 1) - row(ib + 1)) / 2.f;
+    };
+    const float ayz = mixed(3, 0, 1, w[3]);
+    const float axz = mixed(4, 0, 2, w[4]);
+    const float axy = mixed(5, 1, 2, w[5]);
+    return ((((azz + ayy) + axx) + ayz) + axz) + axy;
+}
+
+// Accessor of the six components stored as hw[c * n + i].
+struct Hess6Global {
+    const float* hw;
+    int64_t n, ny, nx;
+    __device__ __forceinline__ float operator()(int c, int64_t z, int64_t y, int64_t x) const {
+        return __ldg(hw + c * n + (z * ny + y) * nx + x);
+    }
+};
+
 __device__ __forceinline__ float hess_adj_at(const float* hw, int64_t z, int64_t y, int64_t x,
                                              const Dims& d, const float w[6]) {
-    const int64_t n = d.nz * d.ny * d.nx;
-    const int64_t sz = d.ny * d.nx, sy = d.nx, sx = 1;
-    const float azz = d2w(hw + y * sy + x, z, d.nz, sz, w[0]);
-    const float ayy = d2w(hw + n + z * sz + x, y, d.ny, sy, w[1]);
-    const float axx = d2w(hw + 2 * n + z * sz + y * sy, x, d.nx, sx, w[2]);
-    const float ayz = mixed_adj(hw + 3 * n + x, z, d.nz, sz, y, d.ny, sy, w[3]);
-    const float axz = mixed_adj(hw + 4 * n + y * sy, z, d.nz, sz, x, d.nx, sx, w[4]);
-    const float axy = mixed_adj(hw + 5 * n + z * sz, y, d.ny, sy, x, d.nx, sx, w[5]);
-    return ((((azz + ayy) + axx) + ayz) + axz) + axy;
+    const Hess6Global g{hw, d.nz * d.ny * d.nx, d.ny, d.nx};
+    return hess_adj_gen(g, z, y, x, d, w);
 }
 
 // Component weights [r^2, 1, 1, sqrt2 r, sqrt2 r, sqrt2] (linops_mlx.py:237-239;
