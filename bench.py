@@ -218,16 +218,16 @@ def run_ours(args, ws, rank, local):
     lib.decon_profile_stop(C.byref(ms_z), C.byref(nz_launch))
     launches = lib.decon_launch_count() - n0
     ms = e0.elapsed_time(e1)
+    from deconlib_b200.replicas import aggregate
+
+    ms, units = aggregate(ms, n_obj * K)  # max device time, total voxel-iterations
     if ws > 1:
         import torch.distributed as dist
 
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     clk = clocks.stop()
     info = runner.result()
-    value = n_obj * K * ws / (ms / 1e3)
+    value = units / (ms / 1e3)
 
     # roofline of the axial pass
     z_bytes = zpass_bytes(OBJ, conv.fft_shape)
@@ -260,8 +260,8 @@ def run_ours(args, ws, rank, local):
     torch.cuda.synchronize()
     ms_rz, n_rz = C.c_double(), C.c_int64()
     lib.decon_profile_stop(C.byref(ms_rz), C.byref(n_rz))
-    ms_rl = r0.elapsed_time(r1)
-    rl_value = n_obj * K * ws / (ms_rl / 1e3)
+    ms_rl, rl_units = aggregate(r0.elapsed_time(r1), n_obj * K)
+    rl_value = rl_units / (ms_rl / 1e3)
     fz, fy, fx = c_rl.fft_shape
     hx = fx // 2 + 1
     rl_model_bytes = 28 * n_obj + 8 * 8 * OBJ[0] * fy * hx + 2 * 8 * fz * fy * hx
@@ -273,8 +273,8 @@ def run_ours(args, ws, rank, local):
                            spacing=SPACING_PD, background=5.0, num_iter=K, tol=0.0)
     out = res.restored.cpu().numpy()
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    e2e_value = n_obj * res.iterations * ws / e2e_s
+    e2e_s, e2e_units = aggregate(time.perf_counter() - t0, n_obj * res.iterations)
+    e2e_value = e2e_units / e2e_s
 
     line = {
         "metric": METRIC,
