@@ -61,6 +61,7 @@ _SIGS = {
     "decon_gradient3d_adjoint": (C.c_int, [_p, _p, _i64p, C.c_float, _p]),
     "decon_reduce_workspace_bytes": (_i64, []),
     "decon_reduce": (C.c_int, [_p, _p, _i64, C.c_int, _p, _p, _p]),
+    "decon_reduce_noalloc": (C.c_int, [_p, _p, _i64, C.c_int, _p, _p]),
     "decon_pdhg_create": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_int, C.c_int, C.POINTER(_p)]),
     "decon_pdhg_destroy": (C.c_int, [_p]),

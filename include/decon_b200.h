@@ -253,6 +253,19 @@ int64_t decon_reduce_workspace_bytes(void);
 int decon_reduce(const float* a, const float* b, int64_t n, int op, double* out, void* workspace,
                  void* stream);
 
+/* The reduction above for callers that cannot allocate device memory (no
+ * counterpart in the reference): plug-ins inside a host application that owns
+ * every device allocation, or pipelines that reserve memory up front because
+ * cudaMalloc can synchronise the device and fail at run time.  It allocates
+ * nothing: its scratch is a fixed 128 KB device array inside the library
+ * (held by every GPU that loads it until exit), so n is limited to
+ * 67,108,864 elements (DECON_ERR_VALUE beyond).  The first call on a device
+ * looks up that array's address with the device current; make that first
+ * call before any stream capture.  All calls share the array: calls whose
+ * kernels overlap on the GPU race, so order them on one stream. */
+int decon_reduce_noalloc(const float* a, const float* b, int64_t n, int op, double* out,
+                         void* stream);
+
 /* ---- kernel timing (no reference counterpart: measurement support) ------ */
 
 #define DECON_PROF_XR2C 1 /* X R2C pass              */
