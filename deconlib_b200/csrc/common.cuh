@@ -46,6 +46,20 @@ void count_launch();
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Division by a run-time divisor 1 <= d < 2^16 of dividends 0 <= q < 2^16 as
+// one multiply: with m = floor(2^32 / d) + 1, floor(q / d) = (q m) >> 32.
+// (q m / 2^32 exceeds q / d by less than q / 2^32 < 2^-16, while a
+// non-integer q / d lies at least 1 / d > 2^-16 below the next integer.)
+// Index loops of the FFT kernels divide a flat thread index by a row length
+// this way instead of with the integer-division sequence.
+struct FastDiv {
+    uint64_t m;
+};
+inline FastDiv make_fastdiv(int64_t d) { return FastDiv{(1ull << 32) / (uint64_t)d + 1}; }
+__device__ __forceinline__ int fdiv(int q, FastDiv f) {
+    return (int)(((uint64_t)(uint32_t)q * f.m) >> 32);
+}
+
 inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 inline int64_t round_up(int64_t a, int64_t b) { return cdiv(a, b) * b; }
 

@@ -41,8 +41,9 @@ __global__ void __launch_bounds__(kFftThreads) k_colfft(ColArgs a) {
     const int64_t o = blockIdx.x / a.ntiles;
     const int64_t kx0 = (int64_t)(blockIdx.x - o * a.ntiles) * T;
     const float2* src = a.src + o * a.src_os + kx0;
+    const int lgT = 31 - __clz(T);  // T is a power of two
     for (int q = tid; q < L * T; q += blockDim.x) {
-        const int j = q / T, t = q - j * T;
+        const int j = q >> lgT, t = q & (T - 1);
         float2 v = make_float2(0.f, 0.f);
         if (j < a.nin && kx0 + t < a.ncols) v = src[(int64_t)j * a.src_js + t];
         sm[phys(j, t, T)] = v;
@@ -57,7 +58,7 @@ __global__ void __launch_bounds__(kFftThreads) k_colfft(ColArgs a) {
     if (a.mode == COL_OTF || a.mode == COL_OTF_CONJ) {
         const float2* otf = a.otf + o * a.otf_os + kx0;
         for (int q = tid; q < L * T; q += blockDim.x) {
-            const int j = q / T, tt = q - j * T;
+            const int j = q >> lgT, tt = q & (T - 1);
             if (kx0 + tt < a.ncols) {
                 const float2 w = __ldg(&otf[(int64_t)j * a.otf_js + tt]);
                 const int p = phys(j, tt, T);
@@ -69,7 +70,7 @@ __global__ void __launch_bounds__(kFftThreads) k_colfft(ColArgs a) {
     }
     float2* dst = a.dst + o * a.dst_os + kx0;
     for (int q = tid; q < a.nout * T; q += blockDim.x) {
-        const int j = q / T, tt = q - j * T;
+        const int j = q >> lgT, tt = q & (T - 1);
         if (kx0 + tt < a.ncols) dst[(int64_t)j * a.dst_js + tt] = sm[phys(j, tt, T)];
     }
 }
@@ -309,6 +310,13 @@ int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cva
              win.wx == p.N[2] && (reinterpret_cast<uintptr_t>(in) & 15) == 0;
     a.T = p.T_x;
     a.nrows = nz_rows * a.Ny;
+    {
+        const int L = a.ax.L;
+        const int64_t nin = p.odd ? std::min<int64_t>(a.Nx, L) : std::min<int64_t>((a.Nx + 1) / 2, L);
+        a.fd_q4 = make_fastdiv(std::max<int64_t>(1, a.Nx / 4));
+        a.fd_H = make_fastdiv(a.Hx);
+        a.fd_nin = make_fastdiv(std::max<int64_t>(1, nin));
+    }
     const int nthr = threads_for(a.T, a.ax);
     const int64_t nblk = cdiv(a.nrows, a.T);
     const size_t smem = (size_t)a.T * a.ax.L * sizeof(float2);
@@ -377,6 +385,14 @@ int launch_xc2r(const ConvPlan& p, int epi, const float2* in, Win3 win, float* o
     a.aux1 = aux1;
     a.bg = bg;
     a.partials = partials;
+    {
+        const int L = a.ax.L;
+        a.fd_L = make_fastdiv(L);
+        a.fd_h2 = make_fastdiv(std::max(1, L / 2));
+        a.fd_npair = make_fastdiv(L / 2 + 1);
+        a.fd_q4 = make_fastdiv(std::max<int64_t>(1, a.Nx / 4));
+        a.fd_Nx = make_fastdiv(a.Nx);
+    }
     const int nthr = threads_for(a.T, a.ax);
     const int64_t nblk = cdiv(a.nrows, a.T);
     if (nblk_out) *nblk_out = (int)nblk;

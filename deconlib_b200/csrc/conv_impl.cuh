@@ -40,6 +40,7 @@ struct XR2CArgs {
     int Hx, odd, T, vec4;
     Axis ax;            // length Fx/2 (even Fx) or Fx (odd)
     const float2* twx;  // W_Fx table
+    FastDiv fd_q4, fd_H, fd_nin;  // Nx / 4, Hx, packed non-zero points
 };
 
 struct ColArgs {
@@ -84,6 +85,7 @@ struct XC2RArgs {
     const float* aux1;
     float bg;
     double* partials;
+    FastDiv fd_L, fd_h2, fd_npair, fd_q4, fd_Nx;  // L, L / 2, L / 2 + 1, Nx / 4, Nx
 };
 
 // Device-resident state of one LinearFFTConvolver.

@@ -85,6 +85,7 @@ __device__ __forceinline__ float fetch_x(const XR2CArgs& a, const RowSrc& r, int
 template <int PRO, int LS>
 __global__ void __launch_bounds__(kFftThreads) k_xr2c(XR2CArgs a) {
     extern __shared__ float2 sm[];
+    __shared__ RowSrc rsrc[32];  // per-row source (general path)
     const int T = a.T, L = a.ax.L, tid = threadIdx.x;
     const int64_t row0 = (int64_t)blockIdx.x * T;
     // packed points that can be non-zero
@@ -98,7 +99,7 @@ __global__ void __launch_bounds__(kFftThreads) k_xr2c(XR2CArgs a) {
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int c = c0 + u * blockDim.x;
-                const int t = c / q4;
+                const int t = fdiv(c, a.fd_q4);
                 const int64_t row = row0 + t;
                 v[u] = (c < nq && row < a.nrows)
                            ? __ldg(reinterpret_cast<const float4*>(a.in + row * a.Nx) + (c - t * q4))
@@ -108,26 +109,33 @@ __global__ void __launch_bounds__(kFftThreads) k_xr2c(XR2CArgs a) {
             for (int u = 0; u < U; ++u) {
                 const int c = c0 + u * blockDim.x;
                 if (c < nq) {
-                    const int t = c / q4, x4 = c - t * q4;
+                    const int t = fdiv(c, a.fd_q4), x4 = c - t * q4;
                     sm[phys(2 * x4, t, T)] = make_float2(v[u].x, v[u].y);
                     sm[phys(2 * x4 + 1, t, T)] = make_float2(v[u].z, v[u].w);
                 }
             }
         }
     } else {
-        for (int q = tid; q < T * nin; q += blockDim.x) {
-            const int t = q / nin, n = q - t * nin;
-            const int64_t row = row0 + t;
-            float2 v = make_float2(0.f, 0.f);
+        // (z, y) of each row once, not per element
+        if (tid < T) {
+            const int64_t row = row0 + tid;
+            RowSrc rs{nullptr, false};
             if (row < a.nrows) {
                 const int64_t z = row / a.Ny, y = row - z * a.Ny;
-                const RowSrc rs = row_source<PRO>(a, z, y);
-                if (a.odd) {
-                    v.x = fetch_x<PRO>(a, rs, n);
-                } else {
-                    v.x = fetch_x<PRO>(a, rs, 2 * (int64_t)n);
-                    v.y = fetch_x<PRO>(a, rs, 2 * (int64_t)n + 1);
-                }
+                rs = row_source<PRO>(a, z, y);
+            }
+            rsrc[tid] = rs;
+        }
+        __syncthreads();
+        for (int q = tid; q < T * nin; q += blockDim.x) {
+            const int t = fdiv(q, a.fd_nin), n = q - t * nin;
+            const RowSrc rs = rsrc[t];
+            float2 v = make_float2(0.f, 0.f);
+            if (a.odd) {
+                v.x = fetch_x<PRO>(a, rs, n);
+            } else {
+                v.x = fetch_x<PRO>(a, rs, 2 * (int64_t)n);
+                v.y = fetch_x<PRO>(a, rs, 2 * (int64_t)n + 1);
             }
             sm[phys(n, t, T)] = v;
         }
@@ -144,7 +152,7 @@ __global__ void __launch_bounds__(kFftThreads) k_xr2c(XR2CArgs a) {
     fft_lines<-1, LS>(sm, T, tid % T, tid / T, a.ax, nin);
     const int H = a.Hx;
     for (int q = tid; q < T * H; q += blockDim.x) {
-        const int t = q / H, k = q - t * H;
+        const int t = fdiv(q, a.fd_H), k = q - t * H;
         const int64_t row = row0 + t;
         if (row >= a.nrows) continue;
         float2 X;
@@ -196,12 +204,14 @@ __device__ __forceinline__ void epilogue(const XC2RArgs& a, int64_t i, float v, 
 template <int EPI, int LS>
 __global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
     extern __shared__ float2 sm[];
-    __shared__ float2 nyq[32];  // X[M] of each row (even Fx)
+    __shared__ float2 nyq[32];    // X[M] of each row (even Fx)
+    __shared__ int64_t obase[32];  // output index of x = 0 of each row (general path)
+    constexpr int64_t kOutside = INT64_MIN;
     const int T = a.T, L = a.ax.L, tid = threadIdx.x;
     const int64_t row0 = (int64_t)blockIdx.x * T;
     if (a.odd) {
         for (int q = tid; q < T * L; q += blockDim.x) {
-            const int t = q / L, k = q - t * L;
+            const int t = fdiv(q, a.fd_L), k = q - t * L;
             const int64_t row = row0 + t;
             float2 Z = make_float2(0.f, 0.f);
             if (row < a.nrows) {
@@ -224,7 +234,7 @@ __global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int c = c0 + u * blockDim.x;
-                const int t = c / h2;
+                const int t = fdiv(c, a.fd_h2);
                 const int64_t row = row0 + t;
                 v[u] = (c < nq && row < a.nrows)
                            ? __ldg(reinterpret_cast<const float4*>(a.in + row * a.P) + (c - t * h2))
@@ -234,7 +244,7 @@ __global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
             for (int u = 0; u < U; ++u) {
                 const int c = c0 + u * blockDim.x;
                 if (c < nq) {
-                    const int t = c / h2, q2 = c - t * h2;
+                    const int t = fdiv(c, a.fd_h2), q2 = c - t * h2;
                     sm[phys(2 * q2, t, T)] = make_float2(v[u].x, v[u].y);
                     sm[phys(2 * q2 + 1, t, T)] = make_float2(v[u].z, v[u].w);
                 }
@@ -252,7 +262,7 @@ __global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
         // thread per pair (k, M - k); irfft ignores Im of DC and Nyquist.
         const int npair = (M >> 1) + 1;
         for (int q = tid; q < T * npair; q += blockDim.x) {
-            const int t = q / npair, k = q - t * npair;
+            const int t = fdiv(q, a.fd_npair), k = q - t * npair;
             if (k == 0) {
                 float2 x0 = sm[phys(0, t, T)], xm = nyq[t];
                 x0.y = 0.f;
@@ -291,7 +301,7 @@ __global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
         // plain rows, full window: 4 voxels per thread step
         const int q4 = (int)(Nx >> 2), nq = T * q4;
         for (int c = tid; c < nq; c += blockDim.x) {
-            const int t = c / q4, x4 = c - t * q4;
+            const int t = fdiv(c, a.fd_q4), x4 = c - t * q4;
             const int64_t row = row0 + t;
             if (row >= a.nrows) continue;
             const float2 p0 = sm[phys(2 * x4, t, T)], p1 = sm[phys(2 * x4 + 1, t, T)];
@@ -330,23 +340,34 @@ __global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
             }
         }
     } else {
-        for (int64_t q = tid; q < (int64_t)T * Nx; q += blockDim.x) {
-            const int t = (int)(q / Nx);
-            const int64_t x = q - (int64_t)t * Nx;
-            const int64_t row = row0 + t;
-            if (row >= a.nrows) continue;
-            const int64_t z = row / a.Ny, y = row - z * a.Ny;
-            const int64_t iz = z - a.win.oz, iy = y - a.win.oy, ix = x - a.win.ox;
-            if (iz < 0 || iz >= a.win.wz || iy < 0 || iy >= a.win.wy || ix < 0 || ix >= a.win.wx)
-                continue;
+        // window rows: output index of x = 0 per row, once
+        if (tid < T) {
+            const int64_t row = row0 + tid;
+            int64_t b = kOutside;
+            if (row < a.nrows) {
+                const int64_t z = row / a.Ny, y = row - z * a.Ny;
+                const int64_t iz = z - a.win.oz, iy = y - a.win.oy;
+                if (iz >= 0 && iz < a.win.wz && iy >= 0 && iy < a.win.wy)
+                    b = (iz * a.win.wy + iy) * a.win.wx - a.win.ox;
+            }
+            obase[tid] = b;
+        }
+        __syncthreads();
+        const int nx = (int)Nx;
+        for (int q = tid; q < T * nx; q += blockDim.x) {
+            const int t = fdiv(q, a.fd_Nx);
+            const int x = q - t * nx;
+            const int64_t b = obase[t];
+            const int64_t ix = x - a.win.ox;
+            if (b == kOutside || ix < 0 || ix >= a.win.wx) continue;
             float v;
             if (a.odd) {
-                v = sm[phys((int)x, t, T)].x;
+                v = sm[phys(x, t, T)].x;
             } else {
-                const float2 c = sm[phys((int)(x >> 1), t, T)];
+                const float2 c = sm[phys(x >> 1, t, T)];
                 v = (x & 1) ? c.y : c.x;
             }
-            epilogue<EPI>(a, (iz * a.win.wy + iy) * a.win.wx + ix, v * a.scale, acc);
+            epilogue<EPI>(a, b + x, v * a.scale, acc);
         }
     }
     if constexpr (EPI == EPI_RL_RATIO || EPI == EPI_PRED) {
