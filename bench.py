@@ -139,6 +139,91 @@ def rl_inputs(D):
     return psf, obs
 
 
+def serve_jobs(D, n_jobs, seed=4):
+    """Seeded request stream of the served workload: Poisson arrivals at a
+    rate drawn from [5, 50] jobs/s; each job is RL (50 iterations, beads +
+    shells, 1000 photons, background 10) or Hessian-PDHG (100 iterations,
+    2x sampling, 500 photons, background 5, default tol / min_iter /
+    patience) on an object of even shape drawn from 32-128 x 128-512 x
+    128-512, with its own widefield PSF (NA 1.0-1.45 capped below ni,
+    wavelength 0.45-0.65 um, ni 1.33-1.52, ns = min(ni, 1.334), index-mismatch
+    depth 0-20 um)."""
+    from deconlib_b200 import synth
+    from deconlib_b200.serving import Job, poisson_arrivals
+
+    rng = np.random.default_rng(seed)
+    rate = float(rng.uniform(5.0, 50.0))
+    arrivals = poisson_arrivals(n_jobs, rate, rng)
+    jobs = []
+    for i in range(n_jobs):
+        kind = "rl" if rng.random() < 0.5 else "pdhg"
+        shp = (2 * int(rng.integers(16, 65)), 2 * int(rng.integers(64, 257)),
+               2 * int(rng.integers(64, 257)))
+        ni = float(rng.uniform(1.33, 1.52))
+        na = min(float(rng.uniform(1.0, 1.45)), 0.98 * ni)
+        wl = float(rng.uniform(0.45, 0.65))
+        depth = float(rng.uniform(0.0, 20.0))
+        sp = SPACING_RL if kind == "rl" else SPACING_PD
+        psf = synth.widefield_psf(shp, sp[0], sp[1], wavelength=wl, na=na, ni=ni,
+                                  ns=min(ni, 1.334), depth=depth)
+        truth = synth.beads(shp, 200, rng)
+        synth.shells(shp, sp, 5, rng, out=truth)
+        if kind == "rl":
+            blur = D.LinearFFTConvolver(psf, shp).forward(truth).cpu().numpy()
+            obs = synth.poisson_observation(blur, 1000.0, 10.0, rng)
+            jobs.append(Job(i, "rl", obs, psf, 50, float(arrivals[i]), 10.0))
+        else:
+            fwd = D.compose(D.FractionalAreaDownsample(2.0, in_shape=shp), D.LinearFFTConvolver(psf, shp))
+            obs = synth.poisson_observation(fwd.forward(truth).cpu().numpy(), 500.0, 5.0, rng)
+            opts = dict(alpha=1e-3, regularization="hessian", sampling_factors=2.0, spacing=SPACING_PD)
+            jobs.append(Job(i, "pdhg", obs, psf, 100, float(arrivals[i]), 5.0, opts))
+    return jobs, rate
+
+
+def solve_alone(D, job):
+    """One job through the public API (the plain FP32 GPU form)."""
+    if job.kind == "rl":
+        r = D.richardson_lucy_with_operator(job.observed, D.LinearFFTConvolver(job.psf, job.observed.shape),
+                                            num_iter=job.num_iter, background=job.background)
+    else:
+        r = D.solve_pdhg_mlx(job.observed, job.psf, num_iter=job.num_iter, background=job.background,
+                             **job.options)
+    return r.restored.cpu().numpy(), r.iterations
+
+
+def run_serving(D, n_jobs):
+    """Served stream vs the same jobs solved one at a time through the API."""
+    import torch
+
+    from deconlib_b200.serving import DeconServer, job_signal_shape
+
+    jobs, rate = serve_jobs(D, n_jobs)
+    server = DeconServer(budget_bytes=150 * 10**9, max_active=8, chunk=8)
+    server.run(jobs[:2], realtime=False)  # warm-up (first-use set-up of every kernel family)
+    live = server.run(jobs, realtime=True)
+    burst = server.run(jobs, realtime=False)
+    flat = DeconServer(budget_bytes=150 * 10**9, max_active=8, chunk=8, prioritise=False).run(
+        jobs, realtime=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    alone = [solve_alone(D, j) for j in jobs]
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    vi = sum(int(np.prod(job_signal_shape(j))) * it for j, (_, it) in zip(jobs, alone))
+    worst = 0.0
+    for res, (ref, _) in zip(live.results, alone):
+        worst = max(worst, float(np.linalg.norm(res.restored - ref) / max(np.linalg.norm(ref), 1e-30)))
+    out = {"workload": "poisson_stream_rl50_pdhg100_mixed_shapes", "jobs": len(jobs),
+           "rate_jobs_per_s": rate, "budget_bytes": server.budget, "max_active": server.max_active,
+           "realtime": live.summary(), "all_at_once": burst.summary(),
+           "realtime_equal_priority": flat.summary(),
+           "plain_sequential_voxel_iter_per_s": vi / t_seq, "plain_sequential_s": t_seq,
+           "max_rel_l2_served_vs_alone": worst,
+           "note": "latency = arrival to restored volume on the host; plain = the same jobs "
+                   "one at a time through richardson_lucy_with_operator / solve_pdhg_mlx"}
+    return out
+
+
 # ---------------------------------------------------------------------------
 # algorithmic bytes of the axial pass (per launch)
 # ---------------------------------------------------------------------------
@@ -317,6 +402,8 @@ def run_ours(args, ws, rank, local):
                "workload": "rl_object128x256x256_beads_shells"},
         "pdhg_iterations_run": info[1],
     }
+    if args.serve_jobs > 0:
+        line["serve"] = run_serving(D, args.serve_jobs)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_pdhg(psf, obs, iters=1)
     if rank == 0:
@@ -463,7 +550,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", choices=["full", "conv", "pdhg"], default="full",
+    ap.add_argument("--serve-jobs", type=int, default=16,
+                    help="jobs in the served request stream (0: skip the serving measurement)")
+    ap.add_argument("--mode", choices=["full", "conv", "pdhg", "serve"], default="full",
                     help="conv: only warm-up + steps forward/adjoint convolutions of the PDHG "
                          "operator; pdhg: only the timed PDHG iterations (small, fixed launch "
                          "sequences for ncu captures)")
@@ -476,6 +565,14 @@ def main():
         return
     if args.mode == "pdhg":
         run_pdhg_only(args)
+        return
+    if args.mode == "serve":
+        import torch
+
+        import deconlib_b200.deconvolution as D
+
+        torch.cuda.set_device(local)
+        print(json.dumps({"mode": "serve", **run_serving(D, max(args.serve_jobs, 1))}), flush=True)
         return
     if args.impl == "reference":
         run_reference(args, ws, rank, local)

@@ -35,6 +35,7 @@ _SIGS = {
     "decon_fast_padded_shape": (C.c_int, [C.c_int, _i64p, _i64p, _i64p, _i64p]),
     "decon_conv_create": (C.c_int, [_p, _i64p, _i64p, _i64p, C.c_int, _p, C.POINTER(_p)]),
     "decon_conv_destroy": (C.c_int, [_p]),
+    "decon_conv_set_kernel": (C.c_int, [_p, _p, C.c_int, _p]),
     "decon_conv_norm_sq": (C.c_int, [_p, _dp]),
     "decon_conv_shape": (C.c_int, [_p, _i64p, _i64p]),
     "decon_conv_get_otf": (C.c_int, [_p, _p, _p]),
@@ -65,6 +66,8 @@ _SIGS = {
     "decon_pdhg_create": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_int, C.c_int, C.POINTER(_p)]),
     "decon_pdhg_destroy": (C.c_int, [_p]),
+    "decon_pdhg_reset": (C.c_int, [_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                   C.c_int, C.c_int, _p]),
     "decon_pdhg_dual_data": (C.c_int, [_p, _p, _p, _p, _p, C.c_float, C.c_int, _i64, _p]),
     "decon_pdhg_dual_reg": (C.c_int, [_p, _p, _p, C.c_float, C.c_int, C.c_int, _i64, _p]),
     "decon_pdhg_xbar": (C.c_int, [_p, _p, _p, _p, _i64, _p]),

@@ -138,6 +138,39 @@ int decon_fast_padded_shape(int ndim, const int64_t* signal, const int64_t* kern
     return DECON_OK;
 }
 
+// Kernel sum (FP64, linops_mlx.py:408-409) and OTF = rfftn(kernel canvas):
+// X pass over all Fz*Fy rows straight into the OTF buffer, then in-place Y
+// and Z forward passes (unpruned); operator_norm_sq = max |OTF|^2.  Reads
+// the two FP64 scalars back (synchronises the stream).
+static int build_otf(decon_conv* p, const float* kernel, int normalize, cudaStream_t s) {
+    int st;
+    const int64_t Fz = p->F[0], Fy = p->F[1];
+    p->kdiv = 1.f;
+    const int64_t nk = p->K[0] * p->K[1] * p->K[2];
+    if (normalize) {
+        DK_TRY(reduce_f32(kernel, nullptr, nk, DECON_RED_SUM, p->dscal, p->partials, p->npartials, s));
+        double ksum = 0;
+        cudaError_t e = cudaMemcpyAsync(&ksum, p->dscal, sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return fail(DECON_ERR_CUDA, "kernel sum failed: %s", cudaGetErrorString(e));
+        p->kdiv = (float)ksum;
+    }
+    Win3 none{0, 0, 0, 0, 0, 0};
+    if ((st = launch_xr2c(*p, PRO_KERNEL, kernel, none, 0.f, 0.f, Fz, p->otf, s)) ||
+        (st = launch_col(*p, p->ax_y, p->T_y, COL_FWD, p->otf, Fy * p->P, p->P, (int)Fy, p->otf,
+                         Fy * p->P, p->P, (int)Fy, Fz, s)) ||
+        (st = launch_col(*p, p->ax_z, p->T_z, COL_FWD, p->otf, p->P, Fy * p->P, (int)Fz, p->otf,
+                         p->P, Fy * p->P, (int)Fz, Fy, s)) ||
+        (st = max_abs2(p->otf, Fz * Fy, p->Hx, p->P, p->dscal + 1, p->partials, s)))
+        return st;
+    double nrm = 0;
+    cudaError_t e = cudaMemcpyAsync(&nrm, p->dscal + 1, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(DECON_ERR_CUDA, "OTF build failed: %s", cudaGetErrorString(e));
+    p->norm_sq = nrm;
+    return DECON_OK;
+}
+
 static int conv_create_impl(const float* kernel, const int64_t kshape[3],
                             const int64_t signal_shape[3], const int64_t fft_shape[3], int normalize,
                             bool circular, void* stream, decon_conv** out) {
@@ -235,47 +268,11 @@ static int conv_create_impl(const float* kernel, const int64_t kshape[3],
                    encode_spectrum_map(&p->tm_s2_j2, p->s2, P, Fy, nz, 1, p->s2z_box) &&
                    encode_spectrum_map(&p->tm_otf_z, p->otf, P, Fy, Fz, 1, p->otf_box);
     }
-    // Kernel sum (FP64) for normalisation (linops_mlx.py:408-409).
-    p->kdiv = 1.f;
-    const int64_t nk = p->K[0] * p->K[1] * p->K[2];
-    if (normalize) {
-        if ((st = reduce_f32(kernel, nullptr, nk, DECON_RED_SUM, p->dscal, p->partials, p->npartials, s))) {
-            free_plan(p);
-            delete p;
-            return st;
-        }
-        double ksum = 0;
-        cudaError_t e = cudaMemcpyAsync(&ksum, p->dscal, sizeof(double), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) {
-            free_plan(p);
-            delete p;
-            return fail(DECON_ERR_CUDA, "kernel sum failed: %s", cudaGetErrorString(e));
-        }
-        p->kdiv = (float)ksum;
-    }
-    // OTF = rfftn(kernel canvas): X pass over all Fz*Fy rows straight into the
-    // OTF buffer, then in-place Y and Z forward passes (unpruned).
-    Win3 none{0, 0, 0, 0, 0, 0};
-    if ((st = launch_xr2c(*p, PRO_KERNEL, kernel, none, 0.f, 0.f, Fz, p->otf, s)) ||
-        (st = launch_col(*p, p->ax_y, p->T_y, COL_FWD, p->otf, Fy * p->P, p->P, (int)Fy, p->otf,
-                         Fy * p->P, p->P, (int)Fy, Fz, s)) ||
-        (st = launch_col(*p, p->ax_z, p->T_z, COL_FWD, p->otf, p->P, Fy * p->P, (int)Fz, p->otf,
-                         p->P, Fy * p->P, (int)Fz, Fy, s)) ||
-        (st = max_abs2(p->otf, Fz * Fy, p->Hx, p->P, p->dscal + 1, p->partials, s))) {
+    if ((st = build_otf(p, kernel, normalize, s))) {
         free_plan(p);
         delete p;
         return st;
     }
-    double nrm = 0;
-    cudaError_t e = cudaMemcpyAsync(&nrm, p->dscal + 1, sizeof(double), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-        free_plan(p);
-        delete p;
-        return fail(DECON_ERR_CUDA, "OTF build failed: %s", cudaGetErrorString(e));
-    }
-    p->norm_sq = nrm;
     *out = p;
     return DECON_OK;
 }
@@ -288,6 +285,16 @@ int decon_conv_create(const float* kernel, const int64_t kshape[3], const int64_
 int decon_conv_create_circular(const float* kernel, const int64_t shape[3], int normalize,
                                void* stream, decon_conv** out) {
     return conv_create_impl(kernel, shape, shape, shape, normalize, true, stream, out);
+}
+
+int decon_conv_set_kernel(decon_conv* p, const float* kernel, int normalize, void* stream) {
+    if (!p || !kernel) return fail(DECON_ERR_NULL, "decon_conv_set_kernel: null pointer");
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != p->device)
+        return fail(DECON_ERR_VALUE, "decon_conv_set_kernel: plan lives on device %d, current is %d",
+                    p->device, cur);
+    return build_otf(p, kernel, normalize, as_stream(stream));
 }
 
 int decon_conv_destroy(decon_conv* p) {

@@ -498,24 +498,11 @@ static int g1(int64_t n) {
 
 extern "C" {
 
-int decon_pdhg_create(int num_iter, double step_scale, double delta, double eta, double tol,
-                      int min_iter, int patience, decon_pdhg** out) {
-    if (!out) return fail(DECON_ERR_NULL, "null pointer");
-    if (num_iter < 0) return fail(DECON_ERR_VALUE, "num_iter must be >= 0");
-    *out = nullptr;
-    decon_pdhg* h = new (std::nothrow) decon_pdhg();
-    if (!h) return fail(DECON_ERR_OOM, "host allocation failed");
-    h->num_iter = num_iter;
-    const int nh = std::max(num_iter, 1);
-    const size_t bytes = sizeof(PdhgDev) + (size_t)(4 * nh + kPdhgSlots * kPdhgGrid) * sizeof(double);
-    cudaError_t e = cudaMalloc(&h->mem, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        delete h;
-        return fail(DECON_ERR_OOM, "cudaMalloc of PDHG state failed: %s", cudaGetErrorString(e));
-    }
+// Scalar state of a fresh solve over the history arrays at `base` (nh
+// entries each, then the partial-sum slots).
+static PdhgDev pdhg_initial(int num_iter, double step_scale, double delta, double eta, double tol,
+                            int min_iter, int patience, double* base, int nh) {
     PdhgDev d{};
-    double* base = reinterpret_cast<double*>(reinterpret_cast<char*>(h->mem) + sizeof(PdhgDev));
     d.tau = d.sigma = step_scale;
     d.theta = 1.0;
     d.step_scale = step_scale;
@@ -532,6 +519,28 @@ int decon_pdhg_create(int num_iter, double step_scale, double delta, double eta,
     d.loss_hist = base + 2 * nh;
     d.rel_hist = base + 3 * nh;
     d.partials = base + 4 * nh;
+    return d;
+}
+
+int decon_pdhg_create(int num_iter, double step_scale, double delta, double eta, double tol,
+                      int min_iter, int patience, decon_pdhg** out) {
+    if (!out) return fail(DECON_ERR_NULL, "null pointer");
+    if (num_iter < 0) return fail(DECON_ERR_VALUE, "num_iter must be >= 0");
+    *out = nullptr;
+    decon_pdhg* h = new (std::nothrow) decon_pdhg();
+    if (!h) return fail(DECON_ERR_OOM, "host allocation failed");
+    h->num_iter = num_iter;
+    const int nh = std::max(num_iter, 1);
+    h->capacity = nh;
+    const size_t bytes = sizeof(PdhgDev) + (size_t)(4 * nh + kPdhgSlots * kPdhgGrid) * sizeof(double);
+    cudaError_t e = cudaMalloc(&h->mem, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        delete h;
+        return fail(DECON_ERR_OOM, "cudaMalloc of PDHG state failed: %s", cudaGetErrorString(e));
+    }
+    double* base = reinterpret_cast<double*>(reinterpret_cast<char*>(h->mem) + sizeof(PdhgDev));
+    const PdhgDev d = pdhg_initial(num_iter, step_scale, delta, eta, tol, min_iter, patience, base, nh);
     h->dev = reinterpret_cast<PdhgDev*>(h->mem);
     e = cudaMemcpy(h->dev, &d, sizeof(d), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(base, 0, (size_t)(4 * nh + kPdhgSlots * kPdhgGrid) * sizeof(double));
@@ -541,6 +550,24 @@ int decon_pdhg_create(int num_iter, double step_scale, double delta, double eta,
         return fail(DECON_ERR_CUDA, "PDHG state init failed: %s", cudaGetErrorString(e));
     }
     *out = h;
+    return DECON_OK;
+}
+
+int decon_pdhg_reset(decon_pdhg* h, int num_iter, double step_scale, double delta, double eta,
+                     double tol, int min_iter, int patience, void* stream) {
+    if (!h) return fail(DECON_ERR_NULL, "null pointer");
+    if (num_iter < 0) return fail(DECON_ERR_VALUE, "num_iter must be >= 0");
+    const int nh = h->capacity;
+    if (std::max(num_iter, 1) > nh)
+        return fail(DECON_ERR_VALUE, "decon_pdhg_reset: num_iter %d exceeds the state's capacity %d",
+                    num_iter, nh);
+    const cudaStream_t s = as_stream(stream);
+    double* base = reinterpret_cast<double*>(reinterpret_cast<char*>(h->mem) + sizeof(PdhgDev));
+    const PdhgDev d = pdhg_initial(num_iter, step_scale, delta, eta, tol, min_iter, patience, base, nh);
+    // pageable source: the call returns once the struct is staged
+    DK_CUDA(cudaMemcpyAsync(h->dev, &d, sizeof(d), cudaMemcpyHostToDevice, s));
+    DK_CUDA(cudaMemsetAsync(base, 0, (size_t)(4 * nh + kPdhgSlots * kPdhgGrid) * sizeof(double), s));
+    h->num_iter = num_iter;
     return DECON_OK;
 }
 

@@ -26,4 +26,5 @@ struct decon_pdhg {
     void* mem = nullptr;
     dk::PdhgDev* dev = nullptr;
     int num_iter = 0;
+    int capacity = 0;  // history length allocated (decon_pdhg_reset accepts num_iter <= capacity)
 };

@@ -13,10 +13,11 @@ from .composition import Compose, LinearOperator, as_numpy_op, compose
 from .core_operators import Crop, FractionalAreaDownsample, FractionalAreaUpsample, Pad
 from .linops import (FFTConvolver, Gradient1D, Gradient2D, Gradient3D, Hessian1D, Hessian2D,
                      Hessian3D, LinearFFTConvolver, fast_padded_shape, pad_corner_origin_kernel)
-from .pdhg import (GradientRegularizer, HessianRegularizer, IdentityRegularizer,
-                   prox_gaussian_dual, prox_l1_2_dual, prox_l1_dual, prox_nonneg,
-                   prox_poisson_dual, solve_pdhg_mlx, solve_pdhg_with_operator)
-from .rl import RLResult, poisson_i_divergence, richardson_lucy_solver, richardson_lucy_with_operator
+from .pdhg import (GradientRegularizer, HessianRegularizer, IdentityRegularizer, PDHGRunner,
+                   pdhg_mlx_runner, pdhg_result, prox_gaussian_dual, prox_l1_2_dual, prox_l1_dual,
+                   prox_nonneg, prox_poisson_dual, solve_pdhg_mlx, solve_pdhg_with_operator)
+from .rl import (RLResult, RLRunner, poisson_i_divergence, richardson_lucy_solver,
+                 richardson_lucy_with_operator)
 
 __all__ = [
     "MLXDeconvolutionResult", "Compose", "LinearOperator", "as_numpy_op", "compose", "Crop",
@@ -26,4 +27,5 @@ __all__ = [
     "IdentityRegularizer", "prox_gaussian_dual", "prox_l1_2_dual", "prox_l1_dual", "prox_nonneg",
     "prox_poisson_dual", "solve_pdhg_mlx", "solve_pdhg_with_operator", "RLResult",
     "poisson_i_divergence", "richardson_lucy_solver", "richardson_lucy_with_operator",
+    "RLRunner", "PDHGRunner", "pdhg_mlx_runner", "pdhg_result",
 ]

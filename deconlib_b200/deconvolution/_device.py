@@ -55,13 +55,15 @@ _WS = {}
 
 
 def workspace() -> torch.Tensor:
-    """Per-device reduction workspace (used in stream order only)."""
-    dev = torch.cuda.current_device()
-    ws = _WS.get(dev)
+    """Reduction workspace of the current stream: reductions queued on one
+    stream run in order, so one workspace per (device, stream) is race-free
+    even when several solves run on different streams."""
+    key = (torch.cuda.current_device(), torch.cuda.current_stream().cuda_stream)
+    ws = _WS.get(key)
     if ws is None:
         n = int(_lib.load().decon_reduce_workspace_bytes()) // 8
         ws = torch.empty(n + 8, dtype=torch.float64, device="cuda")
-        _WS[dev] = ws
+        _WS[key] = ws
     return ws
 
 

@@ -203,6 +203,23 @@ class LinearFFTConvolver:
                                circular=False)
         self.operator_norm_sq = self._plan.norm_sq
 
+    def set_kernel(self, kernel) -> "LinearFFTConvolver":
+        """Replace the kernel by another of the same shape, rebuilding the OTF
+        in this plan's device buffers (no allocation, no cudaFree).  Not in
+        the reference; a serving loop uses it to hand a pooled plan to the next
+        job of the same shape.  Synchronises the current stream."""
+        k = to_device(kernel)
+        if tuple(k.shape) != self.kernel_shape:
+            raise ValueError(f"set_kernel expects a kernel of shape {self.kernel_shape}, "
+                             f"got {tuple(k.shape)}")
+        _lib.call("decon_conv_set_kernel", self._plan.handle, _lib.ptr(k), int(self.normalize),
+                  stream())
+        nrm = C.c_double()
+        _lib.check(_lib.load().decon_conv_norm_sq(self._plan.handle, C.byref(nrm)))
+        self._plan.norm_sq = float(nrm.value)
+        self.operator_norm_sq = self._plan.norm_sq
+        return self
+
     @property
     def otf(self) -> torch.Tensor:
         """rfftn of the (normalised) kernel canvas, complex64 on the device."""

@@ -36,7 +36,7 @@ from .linops import (Gradient1D, Gradient2D, Gradient3D, Hessian1D, Hessian2D, H
 __all__ = [
     "solve_pdhg_mlx", "solve_pdhg_with_operator", "IdentityRegularizer", "GradientRegularizer",
     "HessianRegularizer", "prox_poisson_dual", "prox_gaussian_dual", "prox_nonneg",
-    "prox_l1_dual", "prox_l1_2_dual",
+    "prox_l1_dual", "prox_l1_2_dual", "PDHGRunner", "pdhg_mlx_runner", "pdhg_result",
 ]
 
 _CHUNK = 16
@@ -272,6 +272,15 @@ class _State:
                                          float(tol), int(min_iter), int(patience), C.byref(h)))
         self.h = h
         self.num_iter = num_iter
+        self.capacity = max(int(num_iter), 1)
+
+    def reset(self, num_iter, step_scale, delta, eta, tol, min_iter, patience):
+        """Start a new solve in this state (num_iter <= capacity), queued on
+        the current stream."""
+        _lib.call("decon_pdhg_reset", self.h, int(num_iter), float(step_scale), float(delta),
+                  float(eta), float(tol), int(min_iter), int(patience), stream())
+        self.num_iter = num_iter
+        return self
 
     def read(self, hist=False):
         k, fi, cv, st = C.c_int(), C.c_int(), C.c_int(), C.c_int()
@@ -310,7 +319,7 @@ class PDHGRunner:
 
     def __init__(self, data, A, reg, x0, alpha, loss_type, num_iter, background, delta, eta,
                  eval_interval, tol, min_iter, patience, verbose=False, callback=None,
-                 generic=False, fused=True):
+                 generic=False, fused=True, state=None):
         self.s = stream()
         self.data, self.A, self.reg = data, A, reg
         self.alpha = float(alpha)
@@ -321,7 +330,11 @@ class PDHGRunner:
         self.tol, self.patience = tol, patience
         self.verbose, self.callback, self.generic = verbose, callback, generic
         step_scale = 0.99 / (A.operator_norm_sq + reg.operator_norm_sq) ** 0.5
-        self.state = _State(num_iter, step_scale, delta, eta, tol, min_iter, patience)
+        if state is not None and state.capacity >= max(int(num_iter), 1):
+            # pooled state (serving loop): no allocation
+            self.state = state.reset(num_iter, step_scale, delta, eta, tol, min_iter, patience)
+        else:
+            self.state = _State(num_iter, step_scale, delta, eta, tol, min_iter, patience)
         self.h = self.state.h
         self.ncomp = reg.output_components
         self.X = [x0.contiguous(), x0.clone()]
@@ -450,6 +463,16 @@ class PDHGRunner:
         return x, final_iter, converged, taus, sigmas, losses
 
 
+def _conv_for(conv, psf, signal_shape):
+    """A normalised LinearFFTConvolver of ``psf`` on ``signal_shape``: the
+    given pooled one with its OTF rebuilt, or a new one."""
+    if conv is None:
+        return LinearFFTConvolver(psf, signal_shape=signal_shape, normalize=True)
+    if tuple(conv.signal_shape) != tuple(signal_shape) or not conv.normalize:
+        raise ValueError(f"pooled convolver is for {conv.signal_shape}, the solve needs {signal_shape}")
+    return conv.set_kernel(psf)
+
+
 def solve_pdhg_mlx(observed, psf, alpha: float = 0.01,
                    regularization: Literal["identity", "gradient", "hessian"] = "hessian",
                    norm: Literal["L1", "L1_2"] = "L1",
@@ -461,6 +484,39 @@ def solve_pdhg_mlx(observed, psf, alpha: float = 0.01,
                    tol: float = 1e-5, min_iter: int = 20, patience: int = 5
                    ) -> MLXDeconvolutionResult:
     """PSF entry point of adaptive PDHG (pdhg_mlx.py:507-920)."""
+    runner, meta = pdhg_mlx_runner(
+        observed, psf, alpha=alpha, regularization=regularization, norm=norm, loss_type=loss_type,
+        num_iter=num_iter, background=background, spacing=spacing, bin_factors=bin_factors,
+        sampling_factors=sampling_factors, icf_sigmas=icf_sigmas, icf_spacings=icf_spacings,
+        init=init, verbose=verbose, callback=callback, delta=delta, eta=eta,
+        eval_interval=eval_interval, tol=tol, min_iter=min_iter, patience=patience)
+    return pdhg_result(runner.run(), meta)
+
+
+def pdhg_result(runner: "PDHGRunner", metadata: dict) -> MLXDeconvolutionResult:
+    """The result record of a finished runner (synchronises its stream)."""
+    x, fi, cv, taus, sigmas, losses = runner.result()
+    return MLXDeconvolutionResult(restored=x, iterations=fi, loss_history=losses, converged=cv,
+                                  tau_history=taus, sigma_history=sigmas, metadata=metadata)
+
+
+def pdhg_mlx_runner(observed, psf, alpha: float = 0.01,
+                    regularization: Literal["identity", "gradient", "hessian"] = "hessian",
+                    norm: Literal["L1", "L1_2"] = "L1",
+                    loss_type: Literal["poisson", "gaussian"] = "poisson", num_iter: int = 200,
+                    background: float = 0.0, spacing: Optional[Tuple[float, ...]] = None,
+                    bin_factors=None, sampling_factors=None, icf_sigmas=None, icf_spacings=None,
+                    init=None, verbose: bool = False, callback: Optional[Callable] = None,
+                    delta: float = 0.99, eta: float = 0.5, eval_interval: int = 10,
+                    tol: float = 1e-5, min_iter: int = 20, patience: int = 5,
+                    conv: Optional[LinearFFTConvolver] = None, state=None):
+    """Set-up of ``solve_pdhg_mlx`` without the iterations: returns the
+    ``PDHGRunner`` (iterations queued on the current stream by ``iterate``)
+    and the result metadata, for callers that interleave solves.
+
+    ``conv`` / ``state`` (serving loop): a pooled LinearFFTConvolver of the
+    right kernel and signal shapes, whose OTF is rebuilt for ``psf`` in place,
+    and a pooled PDHG state; both avoid device allocation and cudaFree."""
     data = to_device(observed)
     psf_shape = tuple(int(s) for s in (psf.shape if hasattr(psf, "shape") else np.shape(psf)))
     ndim = data.dim()
@@ -479,7 +535,7 @@ def solve_pdhg_mlx(observed, psf, alpha: float = 0.01,
                 "For sampling_factors, psf.shape must match the reconstructed "
                 f"high-resolution shape {highres}; got {psf_shape}"
             )
-        conv = LinearFFTConvolver(psf, signal_shape=highres, normalize=True)
+        conv = _conv_for(conv, psf, highres)
         blur_op = compose(FractionalAreaDownsample(scale=factors), conv)
     elif bin_factors is not None:
         factors = _normalize_bin_factors(bin_factors, ndim)
@@ -493,10 +549,10 @@ def solve_pdhg_mlx(observed, psf, alpha: float = 0.01,
                 "For bin_factors, observed.shape must match psf.shape divided "
                 f"by bin_factors; expected {lowres}, got {tuple(data.shape)}"
             )
-        conv = LinearFFTConvolver(psf, signal_shape=highres, normalize=True)
+        conv = _conv_for(conv, psf, highres)
         blur_op = compose(FractionalAreaDownsample(scale=factors), conv)
     else:
-        blur_op = LinearFFTConvolver(psf, signal_shape=tuple(data.shape), normalize=True)
+        blur_op = _conv_for(conv, psf, tuple(data.shape))
         highres = tuple(data.shape)
     r = _compute_spacing_ratio(spacing, ndim)
     reg = _create_regularizer(regularization, ndim, r, norm)
@@ -505,15 +561,13 @@ def solve_pdhg_mlx(observed, psf, alpha: float = 0.01,
     else:
         x0 = to_device(blur_op.adjoint(data)) if (sampling_factors is not None or bin_factors is not None) else data.clone()
         x0 = prox_nonneg(x0)
-    x, fi, cv, taus, sigmas, losses = PDHGRunner(
-        data, blur_op, reg, x0, alpha, loss_type, num_iter, background, delta, eta, eval_interval,
-        tol, min_iter, patience, verbose, callback, generic=False).run().result()
-    return MLXDeconvolutionResult(
-        restored=x, iterations=fi, loss_history=losses, converged=cv, tau_history=taus,
-        sigma_history=sigmas,
-        metadata={"algorithm": "malitsky_pock_pdhg", "regularization": regularization, "norm": norm,
-                  "loss_type": loss_type, "alpha": alpha, "background": background, "tol": tol,
-                  "min_iter": min_iter, "patience": patience})
+    runner = PDHGRunner(data, blur_op, reg, x0, alpha, loss_type, num_iter, background, delta, eta,
+                        eval_interval, tol, min_iter, patience, verbose, callback, generic=False,
+                        state=state)
+    meta = {"algorithm": "malitsky_pock_pdhg", "regularization": regularization, "norm": norm,
+            "loss_type": loss_type, "alpha": alpha, "background": background, "tol": tol,
+            "min_iter": min_iter, "patience": patience}
+    return runner, meta
 
 
 def solve_pdhg_with_operator(observed, blur_op: LinearOperator, alpha: float = 0.01,

@@ -27,7 +27,7 @@ from .. import _lib
 from ._device import empty, fill, stream, to_device, workspace
 from .linops import LinearFFTConvolver
 
-__all__ = ["RLResult", "poisson_i_divergence", "richardson_lucy_with_operator",
+__all__ = ["RLResult", "RLRunner", "poisson_i_divergence", "richardson_lucy_with_operator",
            "richardson_lucy_solver"]
 
 
@@ -70,7 +70,71 @@ def richardson_lucy_with_operator(observed, blur_op, num_iter: int = 50, backgro
     return _rl_generic(y, blur_op, num_iter, bg, init, callback, eval_interval, verbose)
 
 
+class RLRunner:
+    """Fused RL iterations of one job on a LinearFFTConvolver, split into
+    set-up / ``iterate`` / ``finish`` so that a caller (the serving loop) can
+    queue iterations of several jobs on their own streams and interleave them.
+
+    Everything is queued on the stream that is current at construction; no
+    call synchronises before ``finish``.  The I-divergence of iteration k is
+    summed inside the forward pass of iteration k + 1 (and of the final
+    prediction), so loss logging costs no extra convolution."""
+
+    def __init__(self, observed, op: LinearFFTConvolver, num_iter: int = 50,
+                 background: float = 0.0, init=None, eval_interval: int = 10):
+        self.s = stream()
+        self.y = to_device(observed)
+        self.op, self.plan = op, op.plan
+        self.bg = float(background)
+        self.num_iter, self.eval_interval = int(num_iter), int(eval_interval)
+        self.n = self.y.numel()
+        self.x = empty(self.y.shape)
+        self.sens = empty(self.y.shape)
+        self.ratio = empty(self.y.shape)
+        self.pred = empty(self.y.shape)
+        x_init = to_device(init) if init is not None else None
+        _lib.call("decon_rl_setup", self.plan, _lib.ptr(self.y), C.c_float(self.bg),
+                  _lib.ptr(x_init), _lib.ptr(self.x), _lib.ptr(self.sens), self.s)
+        self.losses_dev = torch.zeros(max(self.num_iter, 1), dtype=torch.float64, device="cuda")
+        self.loss_idx = []
+        self.k = 0
+
+    def iterate(self) -> bool:
+        """Queue iteration k; returns False once all iterations are queued."""
+        if self.k >= self.num_iter:
+            return False
+        prev = self.k - 1
+        lp = None
+        if prev >= 0 and _want_loss(prev, self.num_iter, self.eval_interval):
+            lp = _lib.ptr(self.losses_dev[prev:])
+            self.loss_idx.append(prev)
+        _lib.call("decon_rl_iteration", self.plan, _lib.ptr(self.y), C.c_float(self.bg),
+                  _lib.ptr(self.sens), _lib.ptr(self.x), _lib.ptr(self.ratio), lp, self.s)
+        self.k += 1
+        return self.k < self.num_iter
+
+    def finish(self) -> RLResult:
+        """Queue the final prediction (with the last iteration's loss) and
+        read the loss history (synchronises this runner's stream)."""
+        last = self.k - 1
+        lp = None
+        if last >= 0:
+            lp = _lib.ptr(self.losses_dev[last:])
+            self.loss_idx.append(last)
+        _lib.call("decon_rl_predict", self.plan, _lib.ptr(self.y), C.c_float(self.bg),
+                  _lib.ptr(self.x), _lib.ptr(self.pred), lp, self.s)
+        vals = self.losses_dev.cpu().numpy()
+        losses = [float(vals[i]) / self.n for i in self.loss_idx]
+        return RLResult(restored=self.x, pred=self.pred, iterations=self.k, loss_history=losses,
+                        background=self.bg, full_shape=tuple(self.x.shape), valid_slices=None)
+
+
 def _rl_fused(y, op, num_iter, bg, init, callback, eval_interval, verbose):
+    if callback is None and not verbose:
+        r = RLRunner(y, op, num_iter, bg, init, eval_interval)
+        while r.iterate():
+            pass
+        return r.finish()
     plan = op.plan
     n = y.numel()
     x = empty(y.shape)
@@ -82,44 +146,22 @@ def _rl_fused(y, op, num_iter, bg, init, callback, eval_interval, verbose):
     losses_dev = torch.zeros(max(num_iter, 1), dtype=torch.float64, device="cuda")
     pred = empty(y.shape)
     k = -1
-    loss_idx = []
-    if callback is None and not verbose:
-        for k in range(num_iter):
-            prev = k - 1
-            lp = None
-            if prev >= 0 and _want_loss(prev, num_iter, eval_interval):
-                lp = _lib.ptr(losses_dev[prev:])
-                loss_idx.append(prev)
-            _lib.call("decon_rl_iteration", plan, _lib.ptr(y), C.c_float(bg), _lib.ptr(sens),
-                      _lib.ptr(x), _lib.ptr(ratio), lp, stream())
-        last = num_iter - 1
-        lp = None
-        if last >= 0:
-            lp = _lib.ptr(losses_dev[last:])
-            loss_idx.append(last)
-        _lib.call("decon_rl_predict", plan, _lib.ptr(y), C.c_float(bg), _lib.ptr(x), _lib.ptr(pred),
-                  lp, stream())
-        vals = losses_dev.cpu().numpy()
-        losses = [float(vals[i]) / n for i in loss_idx]
-        iters = k + 1
-    else:
-        losses = []
-        for k in range(num_iter):
-            _lib.call("decon_rl_iteration", plan, _lib.ptr(y), C.c_float(bg), _lib.ptr(sens),
-                      _lib.ptr(x), _lib.ptr(ratio), None, stream())
-            if _want_loss(k, num_iter, eval_interval):
-                _lib.call("decon_rl_predict", plan, _lib.ptr(y), C.c_float(bg), _lib.ptr(x),
-                          _lib.ptr(ratio), _lib.ptr(losses_dev[k:]), stream())
-                loss = float(losses_dev[k].item()) / n
-                losses.append(loss)
-                if verbose:
-                    print(f"  Iter {k:4d}: mean I-div = {loss:.6g}")
-            if callback is not None and callback(k, x):
-                break
-        _lib.call("decon_rl_predict", plan, _lib.ptr(y), C.c_float(bg), _lib.ptr(x), _lib.ptr(pred),
-                  None, stream())
-        iters = k + 1
-    return RLResult(restored=x, pred=pred, iterations=iters, loss_history=losses,
+    losses = []
+    for k in range(num_iter):
+        _lib.call("decon_rl_iteration", plan, _lib.ptr(y), C.c_float(bg), _lib.ptr(sens),
+                  _lib.ptr(x), _lib.ptr(ratio), None, stream())
+        if _want_loss(k, num_iter, eval_interval):
+            _lib.call("decon_rl_predict", plan, _lib.ptr(y), C.c_float(bg), _lib.ptr(x),
+                      _lib.ptr(ratio), _lib.ptr(losses_dev[k:]), stream())
+            loss = float(losses_dev[k].item()) / n
+            losses.append(loss)
+            if verbose:
+                print(f"  Iter {k:4d}: mean I-div = {loss:.6g}")
+        if callback is not None and callback(k, x):
+            break
+    _lib.call("decon_rl_predict", plan, _lib.ptr(y), C.c_float(bg), _lib.ptr(x), _lib.ptr(pred),
+              None, stream())
+    return RLResult(restored=x, pred=pred, iterations=k + 1, loss_history=losses,
                     background=bg, full_shape=tuple(x.shape), valid_slices=None)
 
 

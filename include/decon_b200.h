@@ -75,6 +75,14 @@ int decon_conv_create(const float* kernel, const int64_t kshape[3], const int64_
  * Synchronises. */
 int decon_conv_create_circular(const float* kernel, const int64_t shape[3], int normalize,
                                void* stream, decon_conv** out);
+/* Rebuild the OTF of an existing plan for a new kernel of the same kernel
+ * shape (same normalisation rule, operator_norm_sq recomputed), reusing its
+ * device buffers: no cudaMalloc / cudaFree, so a serving loop can hand a
+ * pooled plan to the next job of the same shape without the device-wide
+ * synchronisation of cudaFree.  Queued on `stream`, which it synchronises
+ * (the two FP64 scalars are read back).  Replaces constructing a new
+ * FFTConvolver (linops_mlx.py:395-415) for a same-shape kernel. */
+int decon_conv_set_kernel(decon_conv* plan, const float* kernel, int normalize, void* stream);
 int decon_conv_destroy(decon_conv* plan);
 /* operator_norm_sq = max |OTF|^2 (linops_mlx.py:415). */
 int decon_conv_norm_sq(const decon_conv* plan, double* out);
@@ -143,6 +151,12 @@ typedef struct decon_pdhg decon_pdhg; /* device-resident tau/sigma/theta + histo
  * host can queue iterations without synchronising. */
 int decon_pdhg_create(int num_iter, double step_scale, double delta, double eta, double tol,
                       int min_iter, int patience, decon_pdhg** out);
+/* Start a new solve in an existing state (same meaning as decon_pdhg_create;
+ * num_iter must not exceed the num_iter the state was created with).  Queued
+ * on `stream`; no allocation, so pooled states cost no cudaFree.  The
+ * reference creates fresh scalars per call (pdhg_mlx.py:693-701). */
+int decon_pdhg_reset(decon_pdhg* h, int num_iter, double step_scale, double delta, double eta,
+                     double tol, int min_iter, int patience, void* stream);
 int decon_pdhg_destroy(decon_pdhg* h);
 /* y1 = prox_{sigma F*}(y1 + sigma ((1+theta) Ax_cur - theta Ax_prev)),
  * loss_type 0 Poisson (pdhg_mlx.py:115-166), 1 Gaussian (:169-189). */
