@@ -44,6 +44,13 @@ _SIGS = {
     "decon_rl_setup": (C.c_int, [_p, _p, C.c_float, _p, _p, _p, _p]),
     "decon_rl_iteration": (C.c_int, [_p, _p, C.c_float, _p, _p, _p, _p, _p]),
     "decon_rl_predict": (C.c_int, [_p, _p, C.c_float, _p, _p, _p, _p]),
+    "decon_rl_run": (C.c_int, [_p, _p, C.c_float, _p, _p, _p, C.c_int, _p]),
+    "decon_batch_rl_create": (C.c_int, [C.c_int, _p, _p, _p, _p, _p, _p, C.c_int, C.POINTER(_p)]),
+    "decon_batch_rl_setup": (C.c_int, [_p, _p, _p]),
+    "decon_batch_rl_run": (C.c_int, [_p, C.c_int, C.c_int, _p]),
+    "decon_batch_rl_predict": (C.c_int, [_p, _p, _p]),
+    "decon_batch_graph_nodes": (C.c_int, [_p, C.c_int, _i64p]),
+    "decon_batch_destroy": (C.c_int, [_p]),
     "decon_rl_ratio": (C.c_int, [_p, _p, C.c_float, _p, _i64, _p, _p, _p]),
     "decon_rl_update": (C.c_int, [_p, _p, _p, _i64, _p]),
     "decon_rl_data_floor": (C.c_int, [_p, C.c_float, _p, _i64, _p]),

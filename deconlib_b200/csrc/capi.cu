@@ -17,6 +17,7 @@ static thread_local std::string g_err;
 static std::atomic<long long> g_launches{0};
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(int64_t n) { g_launches.fetch_add((long long)n, std::memory_order_relaxed); }
 
 void set_error(const char* fmt, ...) {
     char buf[1024];

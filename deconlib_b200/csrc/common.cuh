@@ -28,6 +28,8 @@ int fail(int code, const char* fmt, ...);
 // Count of kernels launched by the library (decon_launch_count), for the
 // benchmark's launch accounting.
 void count_launch();
+// n kernels launched at once (a CUDA graph replay counts its kernel nodes)
+void count_launches(int64_t n);
 
 #define DK_LAUNCHED()                                                                     \
     do {                                                                                  \

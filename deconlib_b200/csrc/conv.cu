@@ -18,7 +18,9 @@
 // 16 complex values, so every 16-wide column tile of the strided passes
 // reads whole 128-byte lines.
 #include <cmath>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include <algorithm>
@@ -219,12 +221,41 @@ struct ProfState {
 };
 static ProfState g_prof;
 
+// Per (device, kernel, dynamic shared memory, block size): the shared-memory
+// opt-in is set and the occupancy queried once; later launches, including
+// launches recorded into a CUDA graph, only look the entry up.
+static int kernel_prepare(void* fn, size_t smem, int nthr, int* per_sm) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, void*, size_t, int>, int> done;
+    int dev = 0;
+    DK_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(dev, fn, smem, nthr);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = done.find(key);
+        if (it != done.end()) {
+            if (per_sm) *per_sm = it->second;
+            return DECON_OK;
+        }
+    }
+    if (smem > 48 * 1024)
+        DK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, nthr, smem) != cudaSuccess) {
+        cudaGetLastError();
+        occ = 0;
+    }
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        done[key] = occ;
+    }
+    if (per_sm) *per_sm = occ;
+    return DECON_OK;
+}
+
 static int launch(void* fn, int64_t nblk, int nthr, size_t smem, cudaStream_t st, void* args,
                   int cls) {
-    if (smem > 48 * 1024) {
-        // idempotent; cheap compared with the launch
-        DK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    }
+    DK_TRY(kernel_prepare(fn, smem, nthr, nullptr));
     if (nblk <= 0) return DECON_OK;
     if (nblk > 0x7fffffffLL) return fail(DECON_ERR_UNSUPPORTED, "grid too large");
     void* params[] = {args};
@@ -506,13 +537,9 @@ static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const C
     const size_t smem = 1024 + (size_t)ns * L * 16 * sizeof(float2);
     const int nthr = 16 * R;
     *status = DECON_OK;
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
-        *status = fail(DECON_ERR_CUDA, "smem attribute failed");
-        return true;
-    }
     int per_sm = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nthr, smem) != cudaSuccess || per_sm < 1)
-        per_sm = 1;
+    if ((*status = kernel_prepare(fn, smem, nthr, &per_sm)) != DECON_OK) return true;
+    if (per_sm < 1) per_sm = 1;
     const int64_t total = nouter * a.ntiles;
     const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count() * per_sm);
     *status = launch(fn, grid, nthr, smem, st, &a,

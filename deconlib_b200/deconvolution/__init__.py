@@ -18,6 +18,9 @@ from .pdhg import (GradientRegularizer, HessianRegularizer, IdentityRegularizer,
                    prox_nonneg, prox_poisson_dual, solve_pdhg_mlx, solve_pdhg_with_operator)
 from .rl import (RLResult, RLRunner, poisson_i_divergence, richardson_lucy_solver,
                  richardson_lucy_with_operator)
+from .shapes import compute_padded_shape, compute_visible_shape, get_valid_slices
+from .forward_model import ForwardModel, make_forward_model
+from .tile_processing import TilePlan, TileSpec, optimal_tile_size, plan_tiles, process_tiles
 
 __all__ = [
     "MLXDeconvolutionResult", "Compose", "LinearOperator", "as_numpy_op", "compose", "Crop",
@@ -27,5 +30,7 @@ __all__ = [
     "IdentityRegularizer", "prox_gaussian_dual", "prox_l1_2_dual", "prox_l1_dual", "prox_nonneg",
     "prox_poisson_dual", "solve_pdhg_mlx", "solve_pdhg_with_operator", "RLResult",
     "poisson_i_divergence", "richardson_lucy_solver", "richardson_lucy_with_operator",
-    "RLRunner", "PDHGRunner", "pdhg_mlx_runner", "pdhg_result",
+    "RLRunner", "PDHGRunner", "pdhg_mlx_runner", "pdhg_result", "compute_padded_shape",
+    "compute_visible_shape", "get_valid_slices", "ForwardModel", "make_forward_model", "TilePlan",
+    "TileSpec", "optimal_tile_size", "plan_tiles", "process_tiles",
 ]

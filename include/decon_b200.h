@@ -120,6 +120,36 @@ int decon_rl_iteration(decon_conv* plan, const float* observed, float background
  * (observed, pred) (rl_mlx.py:159-160,174). */
 int decon_rl_predict(decon_conv* plan, const float* observed, float background, const float* x,
                      float* pred, double* loss_sum, void* stream);
+/* `iterations` RL iterations queued back to back with no host
+ * synchronisation and no loss (graph-capturable): the loop body of
+ * rl_mlx.py:140-152 `iterations` times. */
+int decon_rl_run(decon_conv* plan, const float* observed, float background, const float* sens,
+                 float* x, float* ratio, int iterations, void* stream);
+
+/* ---- batched RL: many independent problems in one CUDA graph ------------
+ * Problem i has its own plan (distinct plans; a plan's scratch spectra serve
+ * one problem), observation, background and x / sens / ratio buffers of its
+ * plan's signal shape.  The reference solves tiles one at a time
+ * (tile_processing.py:226-288); here K iterations of all problems are
+ * recorded once into a CUDA graph, forked over `nstreams` internal streams
+ * balanced by FFT canvas volume, and replayed.  Pointers are kept, not
+ * copied: the buffers must outlive the batch. */
+typedef struct decon_batch decon_batch;
+int decon_batch_rl_create(int n, decon_conv* const* plans, const float* const* observed,
+                          const float* background, float* const* x, float* const* sens,
+                          float* const* ratio, int nstreams, decon_batch** out);
+/* decon_rl_setup for every problem (x_init may be NULL, or hold NULL entries). */
+int decon_batch_rl_setup(decon_batch* b, const float* const* x_init, void* stream);
+/* `iterations` iterations of every problem: replays of the cached graph of
+ * `iters_per_graph` iterations (captured on first use) plus one remainder
+ * graph; ordered after prior work on `stream`, and later work on `stream`
+ * waits for it. */
+int decon_batch_rl_run(decon_batch* b, int iterations, int iters_per_graph, void* stream);
+/* pred_i = A_i x_i + b_i for every problem. */
+int decon_batch_rl_predict(decon_batch* b, float* const* pred, void* stream);
+/* Kernel nodes in the cached graph of `iters_per_graph` iterations (0 if none). */
+int decon_batch_graph_nodes(const decon_batch* b, int iters_per_graph, int64_t* kernels);
+int decon_batch_destroy(decon_batch* b);
 
 /* Element-wise RL steps for an arbitrary composed blur operator (the
  * caller runs forward/adjoint through the operator entry points):

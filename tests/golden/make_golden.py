@@ -252,6 +252,52 @@ def _run(out_path):
     g["pdo_sigma"] = np.array(res.sigma_history)
     g["pdo_loss"] = np.array(res.loss_history)
 
+    # --- tiling geometry, shapes, canonical forward model -----------------
+    from deconlib.deconvolution.forward_model import make_forward_model
+    from deconlib.deconvolution.shapes import compute_padded_shape, get_valid_slices
+    from deconlib.deconvolution.tile_processing import optimal_tile_size, plan_tiles
+
+    def enc(sl):
+        return [[x.start, x.stop] for x in sl]
+
+    tile_cases = [((64, 300, 300), 2.0, 16, 128, 48), ((40, 257, 190), 1.0, 8, 64, 48),
+                  ((100, 512, 512), (1.0, 1.5, 1.5), 20, 200, 48), ((30, 90), 2.0, 4, 40, 48),
+                  ((96, 700, 333), 1.0, 31, 256, 32)]
+    for i, (shape, zoom, guard, ts, mz) in enumerate(tile_cases):
+        plan = plan_tiles(shape, zoom, guard, ts, mz)
+        g[f"tile{i}_tile_shape"] = np.array(plan.tile_shape)
+        g[f"tile{i}_visible"] = np.array(plan.visible_shape)
+        g[f"tile{i}_specs"] = np.array([[enc(t.read), enc(t.write), enc(t.crop)] for t in plan.tiles])
+        g[f"tile{i}_index"] = np.array([t.index for t in plan.tiles])
+    ots = []
+    for N in (50, 64, 100, 257, 512, 1000, 1024, 2048):
+        for guard in (0, 8, 31):
+            for ts in (64, 128, 300, 512):
+                try:
+                    ots.append((N, guard, ts, optimal_tile_size(N, guard, ts)))
+                except ValueError:
+                    ots.append((N, guard, ts, -1))
+    g["optimal_tile_size"] = np.array(ots)
+    for i, (sig, ker) in enumerate([((100, 100), (31, 31)), ((64, 128, 128), (64, 128, 128)),
+                                    ((17, 40, 33), (8, 9, 12))]):
+        shp, pad = compute_padded_shape(sig, ker)
+        g[f"pad{i}_shape"] = np.array(shp)
+        g[f"pad{i}_pad"] = np.array(pad)
+        g[f"pad{i}_valid"] = np.array(enc(get_valid_slices(shp, sig, pad)))
+        g[f"pad{i}_valid_default"] = np.array(enc(get_valid_slices(shp, sig)))
+    # forward model with zoom 2 on an even PSF (the registration fix)
+    psf_fm = _psf((8, 16, 16), 0.2, 0.17)
+    fm = make_forward_model(psf_fm, (6, 12, 10), 2.0)
+    g["fm_psf"] = np.asarray(psf_fm, np.float32)
+    g["fm_padded"] = np.array(fm.padded_shape)
+    g["fm_valid"] = np.array(enc(fm.valid_slices))
+    xin = rng.random(fm.padded_shape, dtype=np.float32)
+    g["fm_x"] = xin
+    g["fm_fwd"] = np.array(fm.op.forward(mx.array(xin)))
+    yin = rng.random((6, 12, 10), dtype=np.float32)
+    g["fm_y"] = yin
+    g["fm_adj"] = np.array(fm.op.adjoint(mx.array(yin)))
+
     np.savez_compressed(out_path, **{k: np.asarray(v) for k, v in g.items()})
     print(f"wrote {out_path}: {len(g)} arrays")
 
