@@ -226,11 +226,14 @@ class BatchedRL:
     def run(self, num_iter: int) -> "BatchedRL":
         _lib.call("decon_batch_rl_run", self.h, int(num_iter), self.iters_per_graph, stream())
         self.iterations += int(num_iter)
+        if num_iter > 0:
+            self.last_graph_iters = min(self.iters_per_graph, int(num_iter))
         return self
 
     def graph_kernels(self) -> int:
+        """Kernel nodes of the graph the last run replayed (K = min(iters_per_graph, n))."""
         k = C.c_int64()
-        _lib.call("decon_batch_graph_nodes", self.h, self.iters_per_graph, C.byref(k))
+        _lib.call("decon_batch_graph_nodes", self.h, getattr(self, "last_graph_iters", 0), C.byref(k))
         return int(k.value)
 
     @property
