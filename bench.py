@@ -224,6 +224,124 @@ def run_serving(D, n_jobs):
     return out
 
 
+BATCH_VOLUME = (256, 1024, 1024)
+
+
+def batch_inputs(D, seed=20):
+    """Batched tiled workload: a 256x1024x1024 volume of the plain-RL object
+    type scaled up (51,200 beads, 320 hollow shells; spacing 0.1 / 0.085 um;
+    the 64x128x128 widefield PSF of the plain-RL case; 1000 peak photons,
+    background 10, Poisson), split into overlapping tiles with seeded cores
+    z 48-96, y / x 160-320 and a 32-voxel halo, plus 16 independent volumes
+    of shape U(32-128 x 128-384 x 128-384), each with its own PSF (NA
+    1.0-1.45 capped below ni, wavelength 0.45-0.65 um, ni 1.33-1.52)."""
+    import torch
+
+    from deconlib_b200 import synth
+    from deconlib_b200.batch import plan_uneven_tiles
+
+    rng = np.random.default_rng(seed)
+    psf = synth.widefield_psf((64, 128, 128), SPACING_RL[0], SPACING_RL[1])
+    truth = synth.beads(BATCH_VOLUME, 51200, rng)
+    synth.shells(BATCH_VOLUME, SPACING_RL, 320, rng, out=truth)
+    blur = D.LinearFFTConvolver(psf, BATCH_VOLUME).forward(truth)
+    del truth
+    blur = blur.cpu().numpy()
+    data = synth.poisson_observation(blur, 1000.0, 10.0, rng)
+    del blur
+    torch.cuda.empty_cache()
+    tiles = plan_uneven_tiles(BATCH_VOLUME, [(48, 96), (160, 320), (160, 320)], 32, rng)
+    vols = []
+    for _ in range(16):
+        shp = (int(rng.integers(32, 129)), int(rng.integers(128, 385)), int(rng.integers(128, 385)))
+        ni = float(rng.uniform(1.33, 1.52))
+        p = synth.widefield_psf(shp, SPACING_RL[0], SPACING_RL[1], wavelength=float(rng.uniform(0.45, 0.65)),
+                                na=min(float(rng.uniform(1.0, 1.45)), 0.98 * ni), ni=ni,
+                                ns=min(ni, 1.334))
+        t = synth.beads(shp, max(20, int(np.prod(shp)) // 5000), rng)
+        synth.shells(shp, SPACING_RL, 5, rng, out=t)
+        b = D.LinearFFTConvolver(p, shp).forward(t).cpu().numpy()
+        vols.append((synth.poisson_observation(b, 1000.0, 10.0, rng), p, 10.0))
+    return data, psf, tiles, vols
+
+
+def run_batched(D, iters=100):
+    """All tiles + volumes in one batch (autotuned canvases, one CUDA graph of
+    all iterations) vs the same problems solved one at a time through
+    richardson_lucy_with_operator with the default canvas."""
+    import torch
+
+    from deconlib_b200 import _lib
+    from deconlib_b200.batch import BatchedRL
+    from deconlib_b200.deconvolution._device import to_device
+
+    t0 = time.perf_counter()
+    data, psf, tiles, vols = batch_inputs(D)
+    vol = to_device(data)
+    probs = [(vol[t.read].contiguous(), psf) for t in tiles] + [(o, p) for o, p, _ in vols]
+    del vol
+    t_inputs = time.perf_counter() - t0
+    lib = _lib.load()
+    # set-up: autotuning, plans and OTFs, RL initialisation
+    t0 = time.perf_counter()
+    b = BatchedRL(probs, 10.0, fft_shapes="auto", nstreams=8, iters_per_graph=iters)
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t0
+    # first run records the graph (all problems x all iterations) and replays it
+    t0 = time.perf_counter()
+    b.run(iters)
+    torch.cuda.synchronize()
+    t_first = time.perf_counter() - t0
+    # timed: the same solve from a fresh start, one replay of the cached graph
+    _lib.call("decon_batch_rl_setup", b.h, None, _lib.stream_ptr())
+    torch.cuda.synchronize()
+    n0 = lib.decon_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.run(iters)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = lib.decon_launch_count() - n0
+    voxels_processed = sum(int(o.numel()) for o in b.obs)
+    voxels_useful = int(np.prod(BATCH_VOLUME)) + sum(int(np.prod(v[0].shape)) for v in vols)
+    stitched = torch.empty(BATCH_VOLUME, dtype=torch.float32, device="cuda")
+    for t, x in zip(tiles, b.restored[:len(tiles)]):
+        stitched[t.write] = x[t.crop]
+    # per-problem plain solves (default canvas) and the stitched / batched results against them
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    worst = 0.0
+    for i, (obs, p) in enumerate(probs):
+        ref = D.richardson_lucy_with_operator(obs, D.LinearFFTConvolver(p, tuple(obs.shape)),
+                                              num_iter=iters, background=10.0).restored
+        if i < len(tiles):
+            got, ref = stitched[tiles[i].write], ref[tiles[i].crop]
+        else:
+            got = b.restored[i]
+        worst = max(worst, float(torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref)))
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    out = {"workload": "batched_tiled_rl_256x1024x1024_uneven_tiles_plus_16_volumes",
+           "tiles": len(tiles), "volumes": len(vols), "iterations": iters,
+           "graph_replays": 1, "graph_kernels": b.graph_kernels(), "gpu_launches_counted": int(launches),
+           "ms": ms, "useful_voxel_iter_per_s": voxels_useful * iters / (ms / 1e3),
+           "processed_voxel_iter_per_s": voxels_processed * iters / (ms / 1e3),
+           "plain_per_problem_s": t_plain,
+           "plain_useful_voxel_iter_per_s": voxels_useful * iters / t_plain,
+           "max_rel_l2_vs_plain_per_problem": worst,
+           "setup_s": {"inputs": t_inputs, "autotune_plans_otf_init": t_setup,
+                       "first_run_with_capture": t_first},
+           "fft_shapes_distinct": len(set(b.fft_shapes)),
+           "note": "ms = device time of one replay of the captured graph (every problem, every "
+                   "iteration); useful voxels = the stitched volume + the 16 volumes; plain = each "
+                   "problem through richardson_lucy_with_operator one after another (wall clock, "
+                   "includes its loss logging)"}
+    del b, probs, stitched
+    torch.cuda.empty_cache()
+    return out
+
+
 # ---------------------------------------------------------------------------
 # algorithmic bytes of the axial pass (per launch)
 # ---------------------------------------------------------------------------
@@ -404,6 +522,8 @@ def run_ours(args, ws, rank, local):
     }
     if args.serve_jobs > 0:
         line["serve"] = run_serving(D, args.serve_jobs)
+    if args.batch_iters > 0:
+        line["batched"] = run_batched(D, args.batch_iters)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_pdhg(psf, obs, iters=1)
     if rank == 0:
@@ -550,9 +670,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-iters", type=int, default=100,
+                    help="RL iterations of the batched tiled workload (0: skip it)")
     ap.add_argument("--serve-jobs", type=int, default=16,
                     help="jobs in the served request stream (0: skip the serving measurement)")
-    ap.add_argument("--mode", choices=["full", "conv", "pdhg", "serve"], default="full",
+    ap.add_argument("--mode", choices=["full", "conv", "pdhg", "serve", "batch"], default="full",
                     help="conv: only warm-up + steps forward/adjoint convolutions of the PDHG "
                          "operator; pdhg: only the timed PDHG iterations (small, fixed launch "
                          "sequences for ncu captures)")
@@ -573,6 +695,14 @@ def main():
 
         torch.cuda.set_device(local)
         print(json.dumps({"mode": "serve", **run_serving(D, max(args.serve_jobs, 1))}), flush=True)
+        return
+    if args.mode == "batch":
+        import torch
+
+        import deconlib_b200.deconvolution as D
+
+        torch.cuda.set_device(local)
+        print(json.dumps({"mode": "batch", **run_batched(D, max(args.batch_iters, 1))}), flush=True)
         return
     if args.impl == "reference":
         run_reference(args, ws, rank, local)

@@ -151,12 +151,18 @@ def autotune_fft_shape(signal_shape, psf, candidates: Optional[List[tuple]] = No
                        max_candidates: int = 6, reps: int = 3) -> tuple:
     """Fastest canvas for a LinearFFTConvolver of ``psf`` on ``signal_shape``:
     each candidate's forward + adjoint pair is timed with CUDA events after a
-    warm-up; the winner is cached per (signal shape, kernel shape)."""
+    warm-up; the winner is cached per (signal shape, kernel shape) and per
+    candidate list, so shapes with the same candidate canvases are timed once."""
     kshape = tuple(int(s) for s in psf.shape)
     key = (tuple(int(s) for s in signal_shape), kshape)
     if key in _TUNED:
         return _TUNED[key]
     cands = (candidates or fft_shape_candidates(signal_shape, kshape))[:max_candidates]
+    # tiles of nearby shapes share their candidate canvases: one timing serves them all
+    ckey = ("canvases", tuple(cands))
+    if ckey in _TUNED:
+        _TUNED[key] = _TUNED[ckey]
+        return _TUNED[key]
     x = empty(key[0])
     x.fill_(1.0)
     best, best_ms = cands[0], float("inf")
@@ -173,7 +179,7 @@ def autotune_fft_shape(signal_shape, psf, candidates: Optional[List[tuple]] = No
         if ms < best_ms:
             best, best_ms = fs, ms
         del conv
-    _TUNED[key] = tuple(best)
+    _TUNED[key] = _TUNED[ckey] = tuple(best)
     return _TUNED[key]
 
 

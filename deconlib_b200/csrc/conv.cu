@@ -221,34 +221,37 @@ struct ProfState {
 };
 static ProfState g_prof;
 
-// Per (device, kernel, dynamic shared memory, block size): the shared-memory
-// opt-in is set and the occupancy queried once; later launches, including
-// launches recorded into a CUDA graph, only look the entry up.
+// Per (device, kernel, dynamic shared memory, block size): the occupancy is
+// queried once; per (device, kernel) the shared-memory opt-in only ever rises
+// to the largest size launched so far (a launch with less shared memory must
+// not lower it under another plan's larger launches).  Later launches,
+// including launches recorded into a CUDA graph, only look the entries up.
 static int kernel_prepare(void* fn, size_t smem, int nthr, int* per_sm) {
     static std::mutex mu;
     static std::map<std::tuple<int, void*, size_t, int>, int> done;
+    static std::map<std::pair<int, void*>, size_t> opt_in;
     int dev = 0;
     DK_CUDA(cudaGetDevice(&dev));
     const auto key = std::make_tuple(dev, fn, smem, nthr);
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        auto it = done.find(key);
-        if (it != done.end()) {
-            if (per_sm) *per_sm = it->second;
-            return DECON_OK;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = done.find(key);
+    if (it != done.end()) {
+        if (per_sm) *per_sm = it->second;
+        return DECON_OK;
+    }
+    if (smem > 48 * 1024) {
+        size_t& cur = opt_in[std::make_pair(dev, fn)];
+        if (smem > cur) {
+            DK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            cur = smem;
         }
     }
-    if (smem > 48 * 1024)
-        DK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, nthr, smem) != cudaSuccess) {
         cudaGetLastError();
         occ = 0;
     }
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        done[key] = occ;
-    }
+    done[key] = occ;
     if (per_sm) *per_sm = occ;
     return DECON_OK;
 }

@@ -300,3 +300,20 @@ def test_pdhg_fused_hessian_matches_operator_path(D, g32, norm):
     assert rel(out[0][0], cpu(out[1][0])) < 1e-6
     np.testing.assert_allclose(out[0][3], out[1][3], rtol=1e-6)
     np.testing.assert_allclose(out[0][5], out[1][5], rtol=1e-6)
+
+
+def test_kernel_shared_memory_opt_in_never_shrinks(D):
+    # The runtime-radix X-pass kernel serves every non-power-of-two length with
+    # a dynamic shared-memory size that depends on the length: a plan that
+    # needs less (Fx = 400, 51 KB) used after one that needs more (Fx = 480,
+    # 61 KB) must not lower the kernel's opt-in under the larger plan.
+    rng = np.random.default_rng(4)
+    k = rng.random((3, 5, 100)).astype(np.float32)
+    x = rng.random((4, 8, 200)).astype(np.float32)
+    big = D.LinearFFTConvolver(k, (4, 8, 200), fft_shape=(8, 16, 480))
+    small = D.LinearFFTConvolver(k, (4, 8, 200), fft_shape=(8, 16, 400))
+    a = cpu(big.forward(x))
+    b = cpu(small.forward(x))
+    c = cpu(big.forward(x))
+    assert rel(b, a) < 1e-5
+    np.testing.assert_array_equal(a, c)
