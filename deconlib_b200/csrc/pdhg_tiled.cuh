@@ -1,14 +1,25 @@
-// Shared-memory tiled forms of the fused Hessian-PDHG kernels.
+// Shared-memory tiled, software-pipelined forms of the fused Hessian-PDHG
+// kernels.
 //
 // A CTA of 32 x 8 threads owns an (x, y) tile and marches along z through a
-// chunk of kZChunk planes.  The field the stencil reads is staged plane by
-// plane, with a one-voxel halo, into shared memory (a ring of three planes
-// for the axes that need z -+ 1), so every neighbour value comes from global
-// memory about once instead of once per stencil tap.  The arithmetic is the
-// shared stencil code (hess6 / hess_adj_gen) with shared-memory accessors, so
-// the results equal the untiled kernels bit for bit.  CTAs walk a fixed list
-// of tiles (tile b, b + grid, ...) so the FP64 partial sums are per-CTA and
-// deterministic.
+// chunk of kZChunk planes; CTAs walk a fixed list of tiles (tile b, b + grid,
+// ...) so the FP64 partial sums are per-CTA and deterministic.  The planes
+// of every field the stencil reads (with a one-voxel halo) and the
+// centre-only operands stream into shared memory with 4-byte cp.async, D
+// planes ahead of use, as one continuous stream across the CTA's tiles: the
+// loads never wait on the arithmetic and the arithmetic waits on a load only
+// when the D-deep pipeline runs dry.  Each thread consumes exactly the
+// elements it copied (its own cp.async group), converts them into a 4-plane
+// working ring (e.g. x_bar = x + theta (x - x_prev)), and one barrier per
+// plane makes the ring visible to the CTA; the 4th ring plane lets a plane be
+// written while slower threads still read the previous three.  The
+// arithmetic is the shared stencil code with shared-memory accessors, so the
+// results equal the untiled kernels bit for bit.
+//
+// The primal update (k_hess_primal_t: six staged y2 components, x and
+// A^T y1) keeps a one-plane register prefetch and static three-plane rings:
+// eight CTAs fit an SM, and on the B200 this measured faster than the
+// pipelined form, whose six deep rings cost occupancy and issue slots.
 #pragma once
 
 #include "solvers.cuh"
@@ -124,86 +135,227 @@ __device__ __forceinline__ float hess_adj_smem(const float* g0m, const float* g0
     return ((((azz + ayy) + axx) + ayz) + axz) + axy;
 }
 
-// Forward Hessian over every tile of the CTA: op(i, h[6]) per in-range voxel.
-// Plane z + 2 is loaded into registers while plane z is computed.
-template <class F, class OP>
-__device__ __forceinline__ void tiled_hess_forward(const F& f, const Dims& d, const float w[6],
-                                                   OP op) {
-    __shared__ float ring[3][kPL];
-    const TileGeo g(d);
-    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-    const int64_t plane = d.ny * d.nx;
-    for (int64_t tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
-        const int64_t bx = tile % g.ntx, r = tile / g.ntx, by = r % g.nty, bz = r / g.nty;
-        const int64_t x0 = bx * kTX, y0 = by * kTY, z0 = bz * kZChunk;
-        const int64_t z1 = min(z0 + kZChunk, d.nz);
-        const int64_t x = x0 + tx, y = y0 + ty;
-        const bool in = x < d.nx && y < d.ny;
-        const int64_t ipl = y * d.nx + x;
-        const StageSlots st(x0, y0, d);
-        float pre[2];
-        st.load(pre, f, clampi(z0 - 1, d.nz), plane);
-        st.store(ring[0], pre);
-        st.load(pre, f, z0, plane);
-        st.store(ring[1], pre);
-        st.load(pre, f, clampi(z0 + 1, d.nz), plane);
-        for (int64_t z = z0; z < z1; ++z) {
-            const int sp = (int)((z - z0) % 3), sc = (int)((z - z0 + 1) % 3),
-                      sn = (int)((z - z0 + 2) % 3);
-            st.store(ring[sn], pre);
-            __syncthreads();
-            if (z + 1 < z1) st.load(pre, f, clampi(z + 2, d.nz), plane);
-            if (in) {
-                float h[6];
-                hess6_smem(ring[sp], ring[sc], ring[sn], ty + 1, tx + 1, w, h);
-                op(z * plane + ipl, h);
-            }
-            __syncthreads();
-        }
-    }
+// ---- software pipeline ------------------------------------------------------
+
+__device__ __forceinline__ void cpa4(float* dst, const float* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+template <int N>
+struct Ptrs {
+    const float* p[N > 0 ? N : 1];
+};
+
+// Position in this CTA's stream of (tile, stage).  Stage s of a tile with
+// planes [z0, z1) carries halo plane clamp(z0 - 1 + s) and, for s >= 2, the
+// centre operands of plane z0 + s - 2, which is computed when stage s is
+// consumed; a tile has (z1 - z0) + 2 stages.  The in-plane offsets of this
+// thread's halo slots and centre voxel are set once per tile.
+struct StageCursor {
+    int64_t tile, x0, y0, z0, z1;
+    int s, S;
+    int hoff[2];  // in-plane offsets of the thread's halo slots (clamped; a plane has < 2^31 voxels)
+    int coff;     // in-plane offset of the thread's voxel, -1 outside the volume
+    __device__ __forceinline__ void set(int64_t t, const TileGeo& g, const Dims& d, const int ly[2],
+                                        const int lx[2], int tx, int ty) {
+        tile = t;
+        s = 0;
+        if (t < g.ntiles) {
+            const int64_t bx = t % g.ntx, r = t / g.ntx, by = r % g.nty, bz = r / g.nty;
+            x0 = bx * kTX;
+            y0 = by * kTY;
+            z0 = bz * kZChunk;
+            z1 = min(z0 + kZChunk, d.nz);
+            S = (int)(z1 - z0) + 2;
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+                hoff[u] = (int)(clampi(y0 - 1 + ly[u], d.ny) * d.nx + clampi(x0 - 1 + lx[u], d.nx));
+            const int64_t x = x0 + tx, y = y0 + ty;
+            coff = (x < d.nx && y < d.ny) ? (int)(y * d.nx + x) : -1;
+        }
+    }
+};
+
+// Dynamic shared memory of one pipeline: NH halo fields x D planes, NC
+// centre operands x D planes, NW working fields x 4 planes (NW = 0: the
+// staged planes are used in place).
+template <int NH, int NW, int NC, int D>
+struct PipeLayout {
+    static constexpr int kH = NH * D * kPL;
+    static constexpr int kC = NC * D * kTX * kTY;
+    static constexpr int kW = NW * 4 * kPL;
+    static constexpr size_t bytes = (size_t)(kH + kC + kW) * sizeof(float);
+};
+
+// Runs the stream.  body(z, x, y, i, cv[NC], W) computes plane z at (x, y)
+// (linear index i) with W[3 f + k] = field f at plane z - 1 + k
+// (shared-memory planes of kHX x kHY).  All threads run every stage (one
+// barrier each).
+//
+// NW > 0: conv(raw[NH], out[NW]) turns the thread's own staged halo values
+// into NW working fields in a 4-plane ring; a staged slot is consumed by the
+// thread that copied it, so it is refilled at once: stages run D ahead.
+// NW == 0: the body reads the staged planes directly (NH fields).  A slot is
+// free only after every thread has finished the body that read it, i.e.
+// after the next barrier: stage g - 3 + D is issued at step g >= 3 into the
+// slot of stage g - 3, so stages run D - 3 ahead.
+template <int NH, int NW, int NC, int D, class CONV, class BODY>
+__device__ __forceinline__ void hess_pipeline(const Dims& d, const Ptrs<NH>& hs, const Ptrs<NC>& cs,
+                                              CONV conv, BODY body) {
+    constexpr bool kDirect = NW == 0;
+    constexpr int NF = kDirect ? NH : NW;  // fields the body sees
+    static_assert(kDirect ? D >= 4 : D >= 2, "pipeline depth");
+    extern __shared__ float smf[];
+    float* hraw = smf;
+    float* craw = hraw + PipeLayout<NH, NW, NC, D>::kH;
+    float* work = craw + PipeLayout<NH, NW, NC, D>::kC;
+    const TileGeo g(d);
+    const int tid = threadIdx.x, tx = tid % kTX, ty = tid / kTX;
+    const int64_t plane = d.ny * d.nx;
+    int q[2], ly[2], lx[2];
+    bool okq[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        q[u] = tid + u * kTX * kTY;
+        okq[u] = q[u] < kPL;
+        ly[u] = q[u] / kHX;
+        lx[u] = q[u] - ly[u] * kHX;
+    }
+    StageCursor is, cc;
+    is.set(blockIdx.x, g, d, ly, lx, tx, ty);
+    cc = is;
+    int gi = 0, gc = 0;
+    auto issue = [&]() {
+        if (is.tile < g.ntiles) {
+            const int slot = gi % D;
+            const int64_t zh = clampi(is.z0 - 1 + is.s, d.nz) * plane;
+#pragma unroll
+            for (int a = 0; a < NH; ++a) {
+                const float* base = hs.p[a] + zh;
+                float* dst = hraw + (a * D + slot) * kPL;
+#pragma unroll
+                for (int u = 0; u < 2; ++u)
+                    if (okq[u]) cpa4(dst + q[u], base + is.hoff[u]);
+            }
+            if (NC > 0 && is.s >= 2 && is.coff >= 0) {
+                const int64_t zc = (is.z0 + is.s - 2) * plane;
+#pragma unroll
+                for (int c = 0; c < NC; ++c) cpa4(&craw[(c * D + slot) * (kTX * kTY) + tid], cs.p[c] + zc + is.coff);
+            }
+            if (++is.s == is.S) is.set(is.tile + gridDim.x, g, d, ly, lx, tx, ty);
+            ++gi;
+        }
+        cpa_commit();
+    };
+#pragma unroll 1
+    for (int k = 0; k < D; ++k) issue();
+#pragma unroll 1
+    while (cc.tile < g.ntiles) {
+        const int slot = gc % D;
+        if constexpr (kDirect) {
+            cpa_wait<D - 4>();
+        } else {
+            cpa_wait<D - 1>();
+            const int ws = gc & 3;
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                if (!okq[u]) continue;
+                float raw[NH], out[NW > 0 ? NW : 1];
+#pragma unroll
+                for (int a = 0; a < NH; ++a) raw[a] = hraw[(a * D + slot) * kPL + q[u]];
+                conv(raw, out);
+#pragma unroll
+                for (int f = 0; f < NW; ++f) work[(f * 4 + ws) * kPL + q[u]] = out[f];
+            }
+        }
+        __syncthreads();
+        if constexpr (kDirect) {
+            if (gc >= 3) issue();  // into the slot of stage gc - 3, read last at step gc - 1
+            else cpa_commit();
+        }
+        if (cc.s >= 2 && cc.coff >= 0) {
+            const int64_t z = cc.z0 + cc.s - 2;
+            const int64_t x = cc.x0 + tx, y = cc.y0 + ty;
+            float cv[NC > 0 ? NC : 1];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) cv[c] = craw[(c * D + slot) * (kTX * kTY) + tid];
+            const float* W[3 * NF];
+#pragma unroll
+            for (int f = 0; f < NF; ++f)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    if constexpr (kDirect) W[3 * f + k] = hraw + (f * D + (gc - 2 + k) % D) * kPL;
+                    else W[3 * f + k] = work + (f * 4 + ((gc - 2 + k) & 3)) * kPL;
+                }
+            body(z, x, y, z * plane + cc.coff, cv, W);
+        }
+        if (++cc.s == cc.S) cc.set(cc.tile + gridDim.x, g, d, ly, lx, tx, ty);
+        ++gc;
+        if constexpr (!kDirect) issue();
+    }
+    cpa_wait<0>();
+}
+
+constexpr int kDualDepth = 4, kDkDepth = 8, kLossDepth = 8;
+using DualLayout = PipeLayout<2, 1, 6, kDualDepth>;
+using DkLayout = PipeLayout<2, 1, 0, kDkDepth>;
+using LossLayout = PipeLayout<1, 1, 0, kLossDepth>;
+
+// y2 = proj(y2 + sigma H x_bar), x_bar = x + theta (x - x_prev) formed at staging.
 template <int NORM>
-__global__ void __launch_bounds__(256) k_hess_dual_t(PdhgDev* s, float* __restrict__ y2,
+__global__ void __launch_bounds__(256) k_hess_dual_p(PdhgDev* s, float* y2,
                                                      const float* __restrict__ xc,
                                                      const float* __restrict__ xp, Dims d, W6 w,
                                                      float alpha) {
     if (s->stop) return;
     const float sg = (float)s->sigma, th = (float)s->theta;
     const int64_t n = d.nz * d.ny * d.nx;
-    auto xbar = [&](int64_t i) -> float {
-        const float a = __ldg(xc + i);
-        return a + th * (a - __ldg(xp + i));
-    };
-    tiled_hess_forward(xbar, d, w.w, [&](int64_t i, const float* h) {
-        if constexpr (NORM == 0) {
+    Ptrs<2> hs{{xc, xp}};
+    Ptrs<6> cs;
 #pragma unroll
-            for (int c = 0; c < 6; ++c) {
-                const int64_t j = c * n + i;
-                y2[j] = fminf(fmaxf(y2[j] + sg * h[c], -alpha), alpha);
+    for (int c = 0; c < 6; ++c) cs.p[c] = y2 + c * n;
+    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+    hess_pipeline<2, 1, 6, kDualDepth>(
+        d, hs, cs, [&](const float* r, float* o) { o[0] = r[0] + th * (r[0] - r[1]); },
+        [&](int64_t, int64_t, int64_t, int64_t i, const float* cv, const float* const* W) {
+            float h[6];
+            hess6_smem(W[0], W[1], W[2], ty + 1, tx + 1, w.w, h);
+            if constexpr (NORM == 0) {
+#pragma unroll
+                for (int c = 0; c < 6; ++c) y2[c * n + i] = fminf(fmaxf(cv[c] + sg * h[c], -alpha), alpha);
+            } else {
+                float v[6];
+                float ss = 0.f;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) {
+                    v[c] = cv[c] + sg * h[c];
+                    ss += v[c] * v[c];
+                }
+                const float sc = fmaxf(sqrtf(ss + 1e-12f) / alpha, 1.f);
+#pragma unroll
+                for (int c = 0; c < 6; ++c) y2[c * n + i] = v[c] / sc;
             }
-        } else {
-            float v[6];
-            float ss = 0.f;
-#pragma unroll
-            for (int c = 0; c < 6; ++c) {
-                v[c] = y2[c * n + i] + sg * h[c];
-                ss += v[c] * v[c];
-            }
-            const float sc = fmaxf(sqrtf(ss + 1e-12f) / alpha, 1.f);
-#pragma unroll
-            for (int c = 0; c < 6; ++c) y2[c * n + i] = v[c] / sc;
-        }
-    });
+        });
 }
 
+// Per-CTA FP64 partial sum into slot `slot`; with a grid smaller than
+// kPdhgGrid, CTA 0 zeroes the slots no CTA writes (the fold sums all).
 __device__ __forceinline__ void put_slot(PdhgDev* s, int slot, double v) {
     const double b = block_sum(v);
     if (threadIdx.x == 0) s->partials[slot * kPdhgGrid + blockIdx.x] = b;
+    if (blockIdx.x == 0)
+        for (int i = gridDim.x + threadIdx.x; i < kPdhgGrid; i += blockDim.x) s->partials[slot * kPdhgGrid + i] = 0.0;
 }
 
 // ||A x_new - A x||^2 and ||H (x_new - x)||^2.
-__global__ void __launch_bounds__(256) k_hess_dk_t(PdhgDev* s, const float* __restrict__ axn,
+__global__ void __launch_bounds__(256) k_hess_dk_p(PdhgDev* s, const float* __restrict__ axn,
                                                    const float* __restrict__ axc, int64_t m,
                                                    const float* __restrict__ xn,
                                                    const float* __restrict__ xc, Dims d, W6 w,
@@ -215,32 +367,49 @@ __global__ void __launch_bounds__(256) k_hess_dk_t(PdhgDev* s, const float* __re
         const double dd = (double)axn[i] - (double)axc[i];
         a2 += dd * dd;
     }
-    auto diff = [&](int64_t i) -> float { return __ldg(xn + i) - __ldg(xc + i); };
-    tiled_hess_forward(diff, d, w.w, [&](int64_t, const float* h) {
+    Ptrs<2> hs{{xn, xc}};
+    Ptrs<0> cs{{nullptr}};
+    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+    hess_pipeline<2, 1, 0, kDkDepth>(
+        d, hs, cs, [&](const float* r, float* o) { o[0] = r[0] - r[1]; },
+        [&](int64_t, int64_t, int64_t, int64_t, const float*, const float* const* W) {
+            float h[6];
+            hess6_smem(W[0], W[1], W[2], ty + 1, tx + 1, w.w, h);
+            // the six squares of one voxel in FP32, the sum over voxels in FP64
+            float v = 0.f;
 #pragma unroll
-        for (int c = 0; c < 6; ++c) l2 += (double)h[c] * (double)h[c];
-    });
+            for (int c = 0; c < 6; ++c) v = fmaf(h[c], h[c], v);
+            l2 += (double)v;
+        });
     put_slot(s, slot_a, a2);
     put_slot(s, slot_l, l2);
 }
 
 template <int NORM>
-__global__ void __launch_bounds__(256) k_hess_regloss_t(PdhgDev* s, const float* __restrict__ x,
+__global__ void __launch_bounds__(256) k_hess_regloss_p(PdhgDev* s, const float* __restrict__ x,
                                                         Dims d, W6 w, int kk, int slot) {
     if (!(kk < s->final_iter && !(s->converged && kk == s->final_iter - 1))) return;
     double acc = 0.0;
-    auto plain = [&](int64_t i) -> float { return __ldg(x + i); };
-    tiled_hess_forward(plain, d, w.w, [&](int64_t, const float* h) {
-        if constexpr (NORM == 0) {
+    Ptrs<1> hs{{x}};
+    Ptrs<0> cs{{nullptr}};
+    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+    hess_pipeline<1, 1, 0, kLossDepth>(
+        d, hs, cs, [&](const float* r, float* o) { o[0] = r[0]; },
+        [&](int64_t, int64_t, int64_t, int64_t, const float*, const float* const* W) {
+            float h[6];
+            hess6_smem(W[0], W[1], W[2], ty + 1, tx + 1, w.w, h);
+            if constexpr (NORM == 0) {
+                float v = 0.f;
 #pragma unroll
-            for (int c = 0; c < 6; ++c) acc += fabs((double)h[c]);
-        } else {
-            float ss = 0.f;
+                for (int c = 0; c < 6; ++c) v += fabsf(h[c]);
+                acc += (double)v;
+            } else {
+                float ss = 0.f;
 #pragma unroll
-            for (int c = 0; c < 6; ++c) ss += h[c] * h[c];
-            acc += (double)sqrtf(ss + 1e-12f);
-        }
-    });
+                for (int c = 0; c < 6; ++c) ss += h[c] * h[c];
+                acc += (double)sqrtf(ss + 1e-12f);
+            }
+        });
     put_slot(s, slot, acc);
 }
 

@@ -8,6 +8,8 @@
 // synchronising; the FP64 reductions (||dx||^2, ||x||^2, ||dKx||^2, losses)
 // are folded in fixed order by the one-CTA step kernel.
 #include <cfloat>
+#include <map>
+#include <mutex>
 
 #include "conv_impl.cuh"
 #include "solvers.cuh"
@@ -492,6 +494,32 @@ __global__ void k_clamp_min(const float* __restrict__ a, float lo, float* __rest
 
 using namespace dk;
 
+// Dynamic shared-memory opt-in of a stencil kernel (once per device and
+// kernel; each kernel always uses the same size) and its resident CTAs per SM.
+static int smem_prepare(const void* fn, size_t bytes, int* per_sm) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, int> done;
+    int dev = 0;
+    DK_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    const auto key = std::make_pair(dev, fn);
+    auto it = done.find(key);
+    if (it == done.end()) {
+        if (bytes > 48 * 1024)
+            DK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        DK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            occ = 1;
+        }
+        it = done.emplace(key, std::max(occ, 1)).first;
+    }
+    if (per_sm) *per_sm = it->second;
+    return DECON_OK;
+}
+
 static int g1(int64_t n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, 256), (int64_t)sm_count() * 16));
 }
@@ -673,11 +701,14 @@ int decon_pdhg_hess_dual(decon_pdhg* h, float* y2, const float* xc, const float*
     const int64_t n = d.nz * d.ny * d.nx;
     (void)n;
     const TileGeo tg(d);
-    const int grid = (int)std::min<int64_t>(tg.ntiles, (int64_t)sm_count() * 8);
+    const void* fn = norm == 0 ? (const void*)k_hess_dual_p<0> : (const void*)k_hess_dual_p<1>;
+    int per_sm = 1;
+    DK_TRY(smem_prepare(fn, DualLayout::bytes, &per_sm));
+    const int grid = (int)std::min<int64_t>(tg.ntiles, (int64_t)sm_count() * per_sm);
     if (norm == 0)
-        k_hess_dual_t<0><<<grid, 256, 0, as_stream(stream)>>>(h->dev, y2, xc, xp, d, w, alpha);
+        k_hess_dual_p<0><<<grid, 256, DualLayout::bytes, as_stream(stream)>>>(h->dev, y2, xc, xp, d, w, alpha);
     else
-        k_hess_dual_t<1><<<grid, 256, 0, as_stream(stream)>>>(h->dev, y2, xc, xp, d, w, alpha);
+        k_hess_dual_p<1><<<grid, 256, DualLayout::bytes, as_stream(stream)>>>(h->dev, y2, xc, xp, d, w, alpha);
     DK_LAUNCHED();
     return DECON_OK;
 }
@@ -699,7 +730,10 @@ int decon_pdhg_hess_dk(decon_pdhg* h, const float* ax_new, const float* ax_cur, 
     if (!h || !ax_new || !ax_cur || !xn || !xc || !shape) return fail(DECON_ERR_NULL, "null pointer");
     W6 w;
     hessian_weights(r, w.w);
-    k_hess_dk_t<<<kPdhgGrid, 256, 0, as_stream(stream)>>>(
+    int per_sm = 1;
+    DK_TRY(smem_prepare((const void*)k_hess_dk_p, DkLayout::bytes, &per_sm));
+    const int grid = std::min(kPdhgGrid, sm_count() * per_sm);
+    k_hess_dk_p<<<grid, 256, DkLayout::bytes, as_stream(stream)>>>(
         h->dev, ax_new, ax_cur, m, xn, xc, Dims{shape[0], shape[1], shape[2]}, w, kSlotDA2, kSlotDL2);
     DK_LAUNCHED();
     return DECON_OK;
@@ -717,8 +751,12 @@ int decon_pdhg_hess_loss(decon_pdhg* h, const float* ax, const float* data, floa
     if (loss_type == 0) k_loss_data<0><<<kPdhgGrid, 256, 0, s>>>(h->dev, ax, data, background, m, k);
     else k_loss_data<1><<<kPdhgGrid, 256, 0, s>>>(h->dev, ax, data, background, m, k);
     DK_LAUNCHED();
-    if (norm == 0) k_hess_regloss_t<0><<<kPdhgGrid, 256, 0, s>>>(h->dev, x, d, w, k, kSlotReg);
-    else k_hess_regloss_t<1><<<kPdhgGrid, 256, 0, s>>>(h->dev, x, d, w, k, kSlotReg);
+    int per_sm = 1;
+    DK_TRY(smem_prepare(norm == 0 ? (const void*)k_hess_regloss_p<0> : (const void*)k_hess_regloss_p<1>,
+                        LossLayout::bytes, &per_sm));
+    const int grid = std::min(kPdhgGrid, sm_count() * per_sm);
+    if (norm == 0) k_hess_regloss_p<0><<<grid, 256, LossLayout::bytes, s>>>(h->dev, x, d, w, k, kSlotReg);
+    else k_hess_regloss_p<1><<<grid, 256, LossLayout::bytes, s>>>(h->dev, x, d, w, k, kSlotReg);
     DK_LAUNCHED();
     k_record_loss<<<1, 256, 0, s>>>(h->dev, alpha, k);
     DK_LAUNCHED();
