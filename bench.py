@@ -342,6 +342,113 @@ def run_batched(D, iters=100):
     return out
 
 
+def _rl_fp64_reference(psf, obs, bg, checkpoints):
+    """FP64 accuracy reference at full size: Richardson-Lucy with the same
+    steps as rl_mlx.py:117-175 (A^T max(y - b, 1e-6) start, sensitivity
+    A^T 1 with the active-support mask, multiplicative update floored at
+    1e-10), the wrap-free convolution done with torch.fft in float64 on the
+    GPU.  A measurement reference only: it is not timed and not the product."""
+    import torch
+
+    from deconlib_b200.deconvolution.linops import fast_padded_shape, pad_corner_origin_kernel
+
+    N = tuple(obs.shape)
+    F = fast_padded_shape(N, psf.shape)
+    k = pad_corner_origin_kernel(psf.astype(np.float64) / psf.astype(np.float64).sum(), F)
+    otf = torch.fft.rfftn(torch.from_numpy(k).cuda())
+    crop = tuple(slice(0, n) for n in N)
+
+    def conv(x, adj=False):
+        X = torch.fft.rfftn(x, s=F)
+        return torch.fft.irfftn(X * (otf.conj() if adj else otf), s=F)[crop]
+
+    y = torch.from_numpy(obs.astype(np.float64)).cuda()
+    x = torch.clamp(conv(torch.clamp(y - bg, min=1e-6), True), min=1e-6)
+    sens_raw = conv(torch.ones_like(y), True)
+    floor = max(float(sens_raw.max()) * 1e-6, 1e-10)
+    active = sens_raw > floor
+    sens = torch.where(active, sens_raw, torch.ones_like(sens_raw))
+    x = torch.where(active, x, torch.zeros_like(x))
+    snaps = {}
+    for it in range(1, max(checkpoints) + 1):
+        ratio = y / torch.clamp(conv(x) + bg, min=1e-10)
+        x = torch.clamp(x * torch.where(active, conv(ratio, True) / sens, torch.zeros_like(x)), min=1e-10)
+        if it in checkpoints:
+            snaps[it] = x.float().clone()
+    return snaps
+
+
+def _errs(a, ref):
+    import torch
+
+    d = (a - ref).double()
+    return {"rel_l2": float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(ref.double())),
+            "max_abs": float(d.abs().max()), "ref_max": float(ref.abs().max())}
+
+
+def run_mixed(D, iters=200):
+    """Plain FP32 vs mixed precision (FP16 OTF with per-kz-plane power-of-two
+    scales) for RL and Hessian-PDHG at 128x256x256: device time per
+    iteration and the error at iterations 10 / 50 / 200 (PDHG: 10 / 50 /
+    100) against an FP64 reference (RL) or the FP32 GPU path (PDHG)."""
+    import torch
+
+    from deconlib_b200.deconvolution.pdhg import pdhg_mlx_runner
+    from deconlib_b200.deconvolution.rl import RLRunner
+
+    checks = tuple(c for c in (10, 50, 200) if c <= iters)
+    psf, obs = rl_inputs(D)
+    ref = _rl_fp64_reference(psf, obs, 10.0, checks)
+    n = int(np.prod(OBJ))
+    out = {"workload": "rl_object128x256x256 + hessian_pdhg_sampling2_object128x256x256",
+           "fp64_reference": "torch.fft float64 RL on the GPU (same steps as rl_mlx.py:117-175)",
+           "rl": {}, "pdhg": {}}
+    for prec in ("fp32", "mixed"):
+        op = D.LinearFFTConvolver(psf, OBJ, precision=prec)
+        r = RLRunner(obs, op, iters, 10.0, eval_interval=10**9)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        snaps, ms = {}, 0.0
+        done = 0
+        for c in checks:
+            e0.record()
+            while r.k < c:
+                r.iterate()
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            snaps[c] = r.x.clone()
+            done = c
+        out["rl"][prec] = {"voxel_iter_per_s": n * done / (ms / 1e3), "ms_per_iter": ms / done,
+                           "vs_fp64": {str(c): _errs(snaps[c], ref[c]) for c in checks}}
+        del r, op
+    pchecks = tuple(c for c in (10, 50, 100) if c <= iters)
+    ppsf, pobs = pdhg_inputs(D)
+    pres = {}
+    for prec in ("fp32", "mixed"):
+        runner, _ = pdhg_mlx_runner(pobs, ppsf, alpha=1e-3, regularization="hessian",
+                                    sampling_factors=2.0, spacing=SPACING_PD, background=5.0,
+                                    num_iter=max(pchecks), tol=0.0, precision=prec)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        snaps, ms = {}, 0.0
+        for c in pchecks:
+            e0.record()
+            while runner.k < c:
+                runner.iterate()
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            snaps[c] = runner.X[runner.k % 2].clone()
+        pres[prec] = snaps
+        out["pdhg"][prec] = {"voxel_iter_per_s": n * max(pchecks) / (ms / 1e3),
+                             "ms_per_iter": ms / max(pchecks)}
+        del runner
+    out["pdhg"]["mixed"]["vs_fp32"] = {str(c): _errs(pres["mixed"][c], pres["fp32"][c]) for c in pchecks}
+    torch.cuda.empty_cache()
+    return out
+
+
 # ---------------------------------------------------------------------------
 # algorithmic bytes of the axial pass (per launch)
 # ---------------------------------------------------------------------------
@@ -524,6 +631,8 @@ def run_ours(args, ws, rank, local):
         line["serve"] = run_serving(D, args.serve_jobs)
     if args.batch_iters > 0:
         line["batched"] = run_batched(D, args.batch_iters)
+    if args.mixed_iters > 0:
+        line["mixed"] = run_mixed(D, args.mixed_iters)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_pdhg(psf, obs, iters=1)
     if rank == 0:
@@ -670,11 +779,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mixed-iters", type=int, default=200,
+                    help="RL iterations of the FP32 vs mixed-precision comparison (0: skip it)")
     ap.add_argument("--batch-iters", type=int, default=100,
                     help="RL iterations of the batched tiled workload (0: skip it)")
     ap.add_argument("--serve-jobs", type=int, default=16,
                     help="jobs in the served request stream (0: skip the serving measurement)")
-    ap.add_argument("--mode", choices=["full", "conv", "pdhg", "serve", "batch"], default="full",
+    ap.add_argument("--mode", choices=["full", "conv", "pdhg", "serve", "batch", "mixed"],
+                    default="full",
                     help="conv: only warm-up + steps forward/adjoint convolutions of the PDHG "
                          "operator; pdhg: only the timed PDHG iterations (small, fixed launch "
                          "sequences for ncu captures)")
@@ -695,6 +807,14 @@ def main():
 
         torch.cuda.set_device(local)
         print(json.dumps({"mode": "serve", **run_serving(D, max(args.serve_jobs, 1))}), flush=True)
+        return
+    if args.mode == "mixed":
+        import torch
+
+        import deconlib_b200.deconvolution as D
+
+        torch.cuda.set_device(local)
+        print(json.dumps({"mode": "mixed", **run_mixed(D, max(args.mixed_iters, 10))}), flush=True)
         return
     if args.mode == "batch":
         import torch

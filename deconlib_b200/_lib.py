@@ -36,6 +36,7 @@ _SIGS = {
     "decon_conv_create": (C.c_int, [_p, _i64p, _i64p, _i64p, C.c_int, _p, C.POINTER(_p)]),
     "decon_conv_destroy": (C.c_int, [_p]),
     "decon_conv_set_kernel": (C.c_int, [_p, _p, C.c_int, _p]),
+    "decon_conv_set_precision": (C.c_int, [_p, C.c_int, _p]),
     "decon_conv_norm_sq": (C.c_int, [_p, _dp]),
     "decon_conv_shape": (C.c_int, [_p, _i64p, _i64p]),
     "decon_conv_get_otf": (C.c_int, [_p, _p, _p]),

@@ -68,6 +68,8 @@ static int make_twiddles(int L, float2** out) {
 
 static void free_plan(ConvPlan* p) {
     if (!p) return;
+    cudaFree(p->otf16);
+    cudaFree(p->otf_inv);
     cudaFree(p->otf);
     cudaFree(p->s1);
     cudaFree(p->s2);
@@ -105,6 +107,55 @@ __global__ void k_rl_mask(float* __restrict__ x, float* __restrict__ sens, const
 
 static int grid_for(int64_t n, int threads) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, threads), (int64_t)sm_count() * 16));
+}
+
+// ---- mixed precision: FP16 OTF with a power-of-two scale per kz plane -------
+
+// max |OTF|^2 over plane kz (one CTA per plane, FP32: only the exponent is used)
+__global__ void k_otf_plane_max(const float2* __restrict__ otf, int64_t Fy, int64_t Hx, int64_t P,
+                                float* __restrict__ inv) {
+    const int64_t kz = blockIdx.x;
+    const float2* pl = otf + kz * Fy * P;
+    float m = 0.f;
+    for (int64_t i = threadIdx.x; i < Fy * Hx; i += blockDim.x) {
+        const int64_t ky = i / Hx, kx = i - ky * Hx;
+        const float2 v = pl[ky * P + kx];
+        m = fmaxf(m, v.x * v.x + v.y * v.y);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+    __shared__ float red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, red[w]);
+        m = fmaxf(m, red[0]);
+        // |OTF| < 2^e with e = ceil(log2 sqrt(m)); scaled values stay below 2^14
+        int e = 0;
+        if (m > 0.f) {
+            frexpf(sqrtf(m), &e);
+        }
+        inv[kz] = ldexpf(1.f, e - 14);  // OTF = stored * inv
+    }
+}
+
+__global__ void k_otf_to_half(const float2* __restrict__ otf, int64_t n_plane, int64_t n,
+                              const float* __restrict__ inv, __half2* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float s = 1.f / inv[i / n_plane];  // power of two: exact
+        const float2 v = otf[i];
+        out[i] = __floats2half2_rn(v.x * s, v.y * s);
+    }
+}
+
+int quantize_otf(const ConvPlan& p, cudaStream_t s) {
+    const int64_t Fz = p.F[0], Fy = p.F[1];
+    k_otf_plane_max<<<(unsigned)Fz, 256, 0, s>>>(p.otf, Fy, p.Hx, p.P, p.otf_inv);
+    DK_LAUNCHED();
+    const int64_t n = Fz * Fy * p.P;
+    k_otf_to_half<<<grid_for(n, 256), 256, 0, s>>>(p.otf, Fy * p.P, n, p.otf_inv, p.otf16);
+    DK_LAUNCHED();
+    return DECON_OK;
 }
 
 }  // namespace dk
@@ -169,6 +220,7 @@ static int build_otf(decon_conv* p, const float* kernel, int normalize, cudaStre
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(DECON_ERR_CUDA, "OTF build failed: %s", cudaGetErrorString(e));
     p->norm_sq = nrm;
+    if (p->precision == 1) DK_TRY(quantize_otf(*p, s));
     return DECON_OK;
 }
 
@@ -296,6 +348,29 @@ int decon_conv_set_kernel(decon_conv* p, const float* kernel, int normalize, voi
         return fail(DECON_ERR_VALUE, "decon_conv_set_kernel: plan lives on device %d, current is %d",
                     p->device, cur);
     return build_otf(p, kernel, normalize, as_stream(stream));
+}
+
+int decon_conv_set_precision(decon_conv* p, int precision, void* stream) {
+    if (!p) return fail(DECON_ERR_NULL, "decon_conv_set_precision: null plan");
+    if (precision != 0 && precision != 1)
+        return fail(DECON_ERR_VALUE, "precision must be 0 (FP32) or 1 (FP16 OTF), got %d", precision);
+    if (precision == 0) {
+        p->precision = 0;
+        return DECON_OK;
+    }
+    if (!zpass_pipelined(*p))
+        return fail(DECON_ERR_UNSUPPORTED,
+                    "mixed precision needs the pipelined axial pass (Fz in {64, 256}, or 128 with "
+                    "Nz <= 64); this plan has Fz = %lld, Nz = %lld",
+                    (long long)p->F[0], (long long)p->N[0]);
+    const int64_t n = p->F[0] * p->F[1] * p->P;
+    int st;
+    if (!p->otf16 && (st = dev_alloc((void**)&p->otf16, (size_t)n * sizeof(__half2), "FP16 OTF"))) return st;
+    if (!p->otf_inv && (st = dev_alloc((void**)&p->otf_inv, (size_t)p->F[0] * sizeof(float), "OTF scales")))
+        return st;
+    DK_TRY(quantize_otf(*p, as_stream(stream)));
+    p->precision = 1;
+    return DECON_OK;
 }
 
 int decon_conv_destroy(decon_conv* p) {

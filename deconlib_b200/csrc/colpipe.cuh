@@ -29,7 +29,9 @@ namespace dk {
 
 __device__ __forceinline__ int p1(int row, int t) { return physw<1>(row, t, 16); }
 
-template <int R, int SPLIT, int MODE>
+// H16: the OTF is read from the FP16 copy and rescaled per kz plane (mixed
+// precision); the transforms and the product stay FP32.
+template <int R, int SPLIT, int MODE, bool H16 = false>
 __global__ void __launch_bounds__(16 * R, 1) k_col_pipe(const __grid_constant__ PipeArgs a) {
     constexpr int LH = R * R;          // sub-transform length
     constexpr int L = LH * SPLIT;      // axis length
@@ -52,6 +54,15 @@ __global__ void __launch_bounds__(16 * R, 1) k_col_pipe(const __grid_constant__ 
     if constexpr (SPLIT == 2) {
 #pragma unroll
         for (int r = 0; r < R; ++r) ws[r] = __ldg(&a.tw[(j + R * r) * a.tws]);
+    }
+
+    // FP16 OTF: this thread's kz planes are fixed, so are their scales
+    float os[H16 ? SPLIT : 1][H16 ? R : 1];
+    if constexpr (H16) {
+#pragma unroll
+        for (int h = 0; h < SPLIT; ++h)
+#pragma unroll
+            for (int r = 0; r < R; ++r) os[h][r] = __ldg(a.otf_inv + SPLIT * (j + R * r) + h);
     }
 
     if (tid == 0) {
@@ -86,14 +97,25 @@ __global__ void __launch_bounds__(16 * R, 1) k_col_pipe(const __grid_constant__ 
         const int o = tile / a.ntiles;
         const int c0 = (tile - o * a.ntiles) * 32;
 
-        float2 ov[OTF ? SPLIT : 1][OTF ? R : 1];
-        if constexpr (OTF) {
+        float2 ov[OTF && !H16 ? SPLIT : 1][OTF && !H16 ? R : 1];
+        if constexpr (OTF && !H16) {
             const float2* op = a.otf + o * a.otf_os + (c0 >> 1) + t;
 #pragma unroll
             for (int h = 0; h < SPLIT; ++h)
 #pragma unroll
                 for (int r = 0; r < R; ++r)
                     ov[h][r] = __ldg(op + (int64_t)(SPLIT * (j + R * r) + h) * a.otf_js);
+        }
+        // FP16 OTF (H16): raw values and plane scales are only loaded here and
+        // converted where they are used, so the loads stay in flight across
+        // the tile wait and the forward transform like the FP32 ones.
+        __half2 oh[H16 ? SPLIT : 1][H16 ? R : 1];
+        if constexpr (OTF && H16) {
+            const __half2* op = a.otf16 + o * a.otf_os + (c0 >> 1) + t;
+#pragma unroll
+            for (int h = 0; h < SPLIT; ++h)
+#pragma unroll
+                for (int r = 0; r < R; ++r) oh[h][r] = __ldg(op + (int64_t)(SPLIT * (j + R * r) + h) * a.otf_js);
         }
         if (!__syncthreads_and(mbar_wait_bounded(&full[s], ph))) return;
 
@@ -136,8 +158,16 @@ __global__ void __launch_bounds__(16 * R, 1) k_col_pipe(const __grid_constant__ 
 #pragma unroll
             for (int h = 0; h < SPLIT; ++h) {
 #pragma unroll
-                for (int r = 0; r < R; ++r)
-                    v[h][r] = MODE == COL_OTF ? cmul(v[h][r], ov[h][r]) : cmulc(v[h][r], ov[h][r]);
+                for (int r = 0; r < R; ++r) {
+                    float2 w;
+                    if constexpr (H16) {
+                        const float2 q = __half22float2(oh[h][r]);
+                        w = make_float2(q.x * os[h][r], q.y * os[h][r]);
+                    } else {
+                        w = ov[h][r];
+                    }
+                    v[h][r] = MODE == COL_OTF ? cmul(v[h][r], w) : cmulc(v[h][r], w);
+                }
                 dft<R, +1>(v[h]);
             }
             __syncthreads();

@@ -485,20 +485,24 @@ bool encode_spectrum_map(CUtensorMap* map, const float2* base, int64_t pitch, in
 // Pipelined kernel for (L, mode, nin, nout), or nullptr.  R x R (SPLIT 1) for
 // L = 64, 256; the half-zero split (SPLIT 2) for L = 128, 512 when the
 // non-zero input / kept output fits in half the axis.
-static void* pick_pipe(int L, int mode, int nin, int nout, int* R, int* split) {
+// h16: the axial (OTF) modes read the FP16 OTF (mixed precision).
+static void* pick_pipe(int L, int mode, int nin, int nout, int* R, int* split, bool h16 = false) {
     const bool otf = mode == COL_OTF || mode == COL_OTF_CONJ;
     const bool half_ok = (mode == COL_FWD && nin <= L / 2) || (mode == COL_INV && nout <= L / 2) ||
                          (otf && nin <= L / 2 && nout <= L / 2);
-#define DK_PIPE(RR, SS)                                                      \
-    do {                                                                     \
-        *R = RR;                                                             \
-        *split = SS;                                                         \
-        switch (mode) {                                                      \
-            case COL_FWD: return (void*)k_col_pipe<RR, SS, COL_FWD>;         \
-            case COL_INV: return (void*)k_col_pipe<RR, SS, COL_INV>;         \
-            case COL_OTF: return (void*)k_col_pipe<RR, SS, COL_OTF>;         \
-            case COL_OTF_CONJ: return (void*)k_col_pipe<RR, SS, COL_OTF_CONJ>; \
-        }                                                                    \
+#define DK_PIPE(RR, SS)                                                                          \
+    do {                                                                                         \
+        *R = RR;                                                                                 \
+        *split = SS;                                                                             \
+        switch (mode) {                                                                          \
+            case COL_FWD: return (void*)k_col_pipe<RR, SS, COL_FWD>;                             \
+            case COL_INV: return (void*)k_col_pipe<RR, SS, COL_INV>;                             \
+            case COL_OTF:                                                                        \
+                return h16 ? (void*)k_col_pipe<RR, SS, COL_OTF, true> : (void*)k_col_pipe<RR, SS, COL_OTF>; \
+            case COL_OTF_CONJ:                                                                   \
+                return h16 ? (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, true>                      \
+                           : (void*)k_col_pipe<RR, SS, COL_OTF_CONJ>;                           \
+        }                                                                                        \
     } while (0)
     if (L == 256) DK_PIPE(16, 1);
     if (L == 64) DK_PIPE(8, 1);
@@ -516,13 +520,17 @@ static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const C
                             int src_jdim, int src_box, int nin, const CUtensorMap& dst, int dst_jdim,
                             int dst_box, int nout, int64_t nouter, cudaStream_t st, int* status) {
     int R = 0, split = 0;
-    void* fn = getenv("DECON_NO_PIPE") ? nullptr : pick_pipe(ax.L, mode, nin, nout, &R, &split);
+    const bool otf_mode = mode == COL_OTF || mode == COL_OTF_CONJ;
+    const bool h16 = otf_mode && p.precision == 1 && p.otf16 != nullptr;
+    void* fn = getenv("DECON_NO_PIPE") ? nullptr : pick_pipe(ax.L, mode, nin, nout, &R, &split, h16);
     if (!fn) return false;
     PipeArgs a;
     memset(&a, 0, sizeof(a));
     a.src = src;
     a.dst = dst;
     a.otf = p.otf;
+    a.otf16 = p.otf16;
+    a.otf_inv = p.otf_inv;
     a.otf_js = p.F[1] * p.P;
     a.otf_os = p.P;
     a.tw = ax.tw;
@@ -548,6 +556,12 @@ static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const C
     *status = launch(fn, grid, nthr, smem, st, &a,
                      (mode == COL_OTF || mode == COL_OTF_CONJ) ? PROF_ZOTF : PROF_COL);
     return true;
+}
+
+bool zpass_pipelined(const ConvPlan& p) {
+    if (!p.tma_z || getenv("DECON_NO_PIPE")) return false;
+    int R = 0, split = 0;
+    return pick_pipe(p.ax_z.L, COL_OTF, (int)p.N[0], (int)p.N[0], &R, &split) != nullptr;
 }
 
 static int launch_col_tma(const ConvPlan& p, const Axis& ax, int mode, const CUtensorMap& src,

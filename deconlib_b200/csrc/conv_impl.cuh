@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_fp16.h>
 
 #include "common.cuh"
 #include "fft_engine.cuh"
@@ -65,6 +66,8 @@ struct ColTmaArgs {
 struct PipeArgs {
     CUtensorMap src, dst;
     const float2* otf;      // OTF base for the axial pass
+    const __half2* otf16;   // mixed precision: FP16 OTF, OTF = otf16 * otf_inv[kz]
+    const float* otf_inv;
     int64_t otf_js, otf_os; // complex-element strides of OTF rows (kz) and planes (ky)
     const float2* tw;       // W_L table, W_L^m = tw[m * tws]
     int tws;
@@ -107,7 +110,18 @@ struct ConvPlan {
     bool tma_y = false, tma_z = false;
     CUtensorMap tm_s1_j1, tm_s2_j1, tm_s2_j2, tm_otf_z;
     int s1_box = 0, s2y_box = 0, s2z_box = 0, otf_box = 0;
+    // Mixed precision (decon_conv_set_precision): the OTF also stored as FP16
+    // complex, scaled per kz plane by a power of two (OTF = otf16 * otf_inv[kz]),
+    // read by the pipelined axial pass instead of the FP32 OTF.
+    int precision = 0;
+    __half2* otf16 = nullptr;
+    float* otf_inv = nullptr;
 };
+
+// Quantise p.otf into p.otf16 / p.otf_inv (capi.cu).
+int quantize_otf(const ConvPlan& p, cudaStream_t st);
+// True when the axial pass of this plan runs the pipelined kernel (conv.cu).
+bool zpass_pipelined(const ConvPlan& p);
 
 bool tma_length_ok(int L);
 bool encode_spectrum_map(CUtensorMap* map, const float2* base, int64_t pitch, int64_t d1, int64_t d2,

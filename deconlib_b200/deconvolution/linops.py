@@ -173,7 +173,7 @@ class LinearFFTConvolver:
     crop in the last (pruned transforms)."""
 
     def __init__(self, kernel, signal_shape: Tuple[int, ...], normalize: bool = True,
-                 fft_shape: Optional[Tuple[int, ...]] = None):
+                 fft_shape: Optional[Tuple[int, ...]] = None, precision: str = "fp32"):
         if isinstance(kernel, torch.Tensor):
             kshape = tuple(int(s) for s in kernel.shape)
         else:
@@ -202,6 +202,21 @@ class LinearFFTConvolver:
         self._plan = _ConvPlan(k, shape3(self.kernel_shape), self._n3, self._f3, normalize,
                                circular=False)
         self.operator_norm_sq = self._plan.norm_sq
+        self.precision = "fp32"
+        if precision != "fp32":
+            self.set_precision(precision)
+
+    def set_precision(self, precision: str) -> "LinearFFTConvolver":
+        """"fp32" or "mixed" (not in the reference): "mixed" stores the OTF as
+        FP16 complex with a power-of-two scale per kz plane for the axial FFT
+        pass; transforms and products stay FP32, reductions FP64.  Raises
+        RuntimeError when this canvas has no pipelined axial pass."""
+        codes = {"fp32": 0, "mixed": 1}
+        if precision not in codes:
+            raise ValueError(f"precision must be 'fp32' or 'mixed', got {precision!r}")
+        _lib.call("decon_conv_set_precision", self._plan.handle, codes[precision], stream())
+        self.precision = precision
+        return self
 
     def set_kernel(self, kernel) -> "LinearFFTConvolver":
         """Replace the kernel by another of the same shape, rebuilding the OTF

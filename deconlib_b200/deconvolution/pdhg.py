@@ -463,13 +463,15 @@ class PDHGRunner:
         return x, final_iter, converged, taus, sigmas, losses
 
 
-def _conv_for(conv, psf, signal_shape):
+def _conv_for(conv, psf, signal_shape, precision="fp32"):
     """A normalised LinearFFTConvolver of ``psf`` on ``signal_shape``: the
     given pooled one with its OTF rebuilt, or a new one."""
     if conv is None:
-        return LinearFFTConvolver(psf, signal_shape=signal_shape, normalize=True)
+        return LinearFFTConvolver(psf, signal_shape=signal_shape, normalize=True, precision=precision)
     if tuple(conv.signal_shape) != tuple(signal_shape) or not conv.normalize:
         raise ValueError(f"pooled convolver is for {conv.signal_shape}, the solve needs {signal_shape}")
+    if conv.precision != precision:
+        conv.set_precision(precision)
     return conv.set_kernel(psf)
 
 
@@ -481,15 +483,19 @@ def solve_pdhg_mlx(observed, psf, alpha: float = 0.01,
                    bin_factors=None, sampling_factors=None, icf_sigmas=None, icf_spacings=None,
                    init=None, verbose: bool = False, callback: Optional[Callable] = None,
                    delta: float = 0.99, eta: float = 0.5, eval_interval: int = 10,
-                   tol: float = 1e-5, min_iter: int = 20, patience: int = 5
-                   ) -> MLXDeconvolutionResult:
-    """PSF entry point of adaptive PDHG (pdhg_mlx.py:507-920)."""
+                   tol: float = 1e-5, min_iter: int = 20, patience: int = 5,
+                   precision: str = "fp32") -> MLXDeconvolutionResult:
+    """PSF entry point of adaptive PDHG (pdhg_mlx.py:507-920).
+
+    ``precision="mixed"`` (not in the reference) stores the OTF as FP16 with
+    per-plane scales (``LinearFFTConvolver.set_precision``)."""
     runner, meta = pdhg_mlx_runner(
         observed, psf, alpha=alpha, regularization=regularization, norm=norm, loss_type=loss_type,
         num_iter=num_iter, background=background, spacing=spacing, bin_factors=bin_factors,
         sampling_factors=sampling_factors, icf_sigmas=icf_sigmas, icf_spacings=icf_spacings,
         init=init, verbose=verbose, callback=callback, delta=delta, eta=eta,
-        eval_interval=eval_interval, tol=tol, min_iter=min_iter, patience=patience)
+        eval_interval=eval_interval, tol=tol, min_iter=min_iter, patience=patience,
+        precision=precision)
     return pdhg_result(runner.run(), meta)
 
 
@@ -509,7 +515,8 @@ def pdhg_mlx_runner(observed, psf, alpha: float = 0.01,
                     init=None, verbose: bool = False, callback: Optional[Callable] = None,
                     delta: float = 0.99, eta: float = 0.5, eval_interval: int = 10,
                     tol: float = 1e-5, min_iter: int = 20, patience: int = 5,
-                    conv: Optional[LinearFFTConvolver] = None, state=None):
+                    conv: Optional[LinearFFTConvolver] = None, state=None,
+                    precision: str = "fp32"):
     """Set-up of ``solve_pdhg_mlx`` without the iterations: returns the
     ``PDHGRunner`` (iterations queued on the current stream by ``iterate``)
     and the result metadata, for callers that interleave solves.
@@ -535,7 +542,7 @@ def pdhg_mlx_runner(observed, psf, alpha: float = 0.01,
                 "For sampling_factors, psf.shape must match the reconstructed "
                 f"high-resolution shape {highres}; got {psf_shape}"
             )
-        conv = _conv_for(conv, psf, highres)
+        conv = _conv_for(conv, psf, highres, precision)
         blur_op = compose(FractionalAreaDownsample(scale=factors), conv)
     elif bin_factors is not None:
         factors = _normalize_bin_factors(bin_factors, ndim)
@@ -549,10 +556,10 @@ def pdhg_mlx_runner(observed, psf, alpha: float = 0.01,
                 "For bin_factors, observed.shape must match psf.shape divided "
                 f"by bin_factors; expected {lowres}, got {tuple(data.shape)}"
             )
-        conv = _conv_for(conv, psf, highres)
+        conv = _conv_for(conv, psf, highres, precision)
         blur_op = compose(FractionalAreaDownsample(scale=factors), conv)
     else:
-        blur_op = _conv_for(conv, psf, tuple(data.shape))
+        blur_op = _conv_for(conv, psf, tuple(data.shape), precision)
         highres = tuple(data.shape)
     r = _compute_spacing_ratio(spacing, ndim)
     reg = _create_regularizer(regularization, ndim, r, norm)

@@ -83,6 +83,15 @@ int decon_conv_create_circular(const float* kernel, const int64_t shape[3], int 
  * (the two FP64 scalars are read back).  Replaces constructing a new
  * FFTConvolver (linops_mlx.py:395-415) for a same-shape kernel. */
 int decon_conv_set_kernel(decon_conv* plan, const float* kernel, int normalize, void* stream);
+/* Storage precision of the OTF read by the axial pass.  0: FP32 (default).
+ * 1 (mixed): the OTF is also kept as FP16 complex with a power-of-two scale
+ * per kz plane (max |OTF| of the plane maps below 2^14, so no plane loses
+ * range), and the pipelined axial pass reads it (half the OTF bytes);
+ * transforms, products and all reductions stay FP32 / FP64.  Needs the
+ * pipelined axial pass (DECON_ERR_UNSUPPORTED otherwise).  decon_conv_set_kernel
+ * requantises.  No reference counterpart: deconlib computes in the FP32 /
+ * complex64 of its arrays (linops_mlx.py:411-429). */
+int decon_conv_set_precision(decon_conv* plan, int precision, void* stream);
 int decon_conv_destroy(decon_conv* plan);
 /* operator_norm_sq = max |OTF|^2 (linops_mlx.py:415). */
 int decon_conv_norm_sq(const decon_conv* plan, double* out);
