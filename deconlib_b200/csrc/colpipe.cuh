@@ -17,9 +17,11 @@
 // The axial pass (MODE = COL_OTF / COL_OTF_CONJ) multiplies by the OTF in
 // registers between the forward and inverse transforms: after the forward
 // second stage a thread holds X at m = j + R r, exactly the points the inverse
-// first stage needs, so that product costs no shared-memory round trip.  The
-// OTF values are prefetched from global memory into registers before the
-// tile's barrier wait.
+// first stage needs.  The FP32 OTF tile (L rows x 16 columns) arrives by TMA
+// in the same ring slot and on the same mbarrier as the spectrum tile, so its
+// loads run NS tiles ahead like the spectrum's; the FP16 OTF of the
+// mixed-precision mode is prefetched from global memory into registers
+// before the tile's barrier wait.
 #pragma once
 
 #include "conv_impl.cuh"
@@ -29,15 +31,22 @@ namespace dk {
 
 __device__ __forceinline__ int p1(int row, int t) { return physw<1>(row, t, 16); }
 
+// Ring slots of k_col_pipe (the host sizes shared memory with the same rule).
+__host__ __device__ constexpr int pipe_slots(int L, bool lean) { return lean ? 1 : (L >= 512 ? 2 : 3); }
+
 // H16: the OTF is read from the FP16 copy and rescaled per kz plane (mixed
 // precision); the transforms and the product stay FP32.
-template <int R, int SPLIT, int MODE, bool H16 = false>
-__global__ void __launch_bounds__(16 * R, 1) k_col_pipe(const __grid_constant__ PipeArgs a) {
+// LEAN (axial pass only): second-stage twiddles in shared memory instead of
+// registers, two ring slots, 128 registers, so two CTAs share an SM.
+template <int R, int SPLIT, int MODE, bool H16 = false, bool LEAN = false>
+__global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_constant__ PipeArgs a) {
     constexpr int LH = R * R;          // sub-transform length
     constexpr int L = LH * SPLIT;      // axis length
-    constexpr int NS = (L >= 512) ? 2 : 3;
+    constexpr int NS = pipe_slots(L, LEAN);
     constexpr bool OTF = (MODE == COL_OTF || MODE == COL_OTF_CONJ);
     constexpr bool INV_FIRST = (MODE == COL_INV);
+    constexpr bool OTFT = OTF && !H16;              // OTF tile staged by TMA
+    constexpr int SLOT = L * 16 * (OTFT ? 2 : 1);   // float2 per ring slot
     constexpr int D1 = INV_FIRST ? +1 : -1;  // direction of the first transform
     extern __shared__ unsigned char smraw[];
     float2* base = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
@@ -45,10 +54,20 @@ __global__ void __launch_bounds__(16 * R, 1) k_col_pipe(const __grid_constant__ 
     const int tid = threadIdx.x, t = tid & 15, j = tid >> 4;
     const int total = a.nouter * a.ntiles;
 
-    // second-stage twiddles W_LH^(r j) = W_L^(SPLIT r j)
-    float2 w2[R];
+    // second-stage twiddles W_LH^(r j) = W_L^(SPLIT r j): registers, or (LEAN)
+    // a shared [R][R] table filled before the first barrier
+    float2 w2r[LEAN ? 1 : R];
+    __shared__ float2 w2s[LEAN ? R : 1][LEAN ? R : 1];
+    if constexpr (LEAN) {
+        for (int q = tid; q < R * R; q += blockDim.x) w2s[q / R][q % R] = __ldg(&a.tw[(SPLIT * (q / R) * (q % R)) * a.tws]);
+    } else {
 #pragma unroll
-    for (int r = 0; r < R; ++r) w2[r] = __ldg(&a.tw[(SPLIT * r * j) * a.tws]);
+        for (int r = 0; r < R; ++r) w2r[r] = __ldg(&a.tw[(SPLIT * r * j) * a.tws]);
+    }
+    auto w2 = [&](int r) -> float2 {
+        if constexpr (LEAN) return w2s[r][j];
+        else return w2r[r];
+    };
     // split twiddles W_L^n, n = j + R r
     float2 ws[SPLIT == 2 ? R : 1];
     if constexpr (SPLIT == 2) {
@@ -74,13 +93,15 @@ __global__ void __launch_bounds__(16 * R, 1) k_col_pipe(const __grid_constant__ 
     auto issue = [&](int tile, int s) {
         const int o = tile / a.ntiles;
         const int c0 = (tile - o * a.ntiles) * 32;
-        float2* buf = base + s * L * 16;
-        mbar_expect_tx(&full[s], (uint32_t)(nbox * a.src_box * 128));
+        float2* buf = base + s * SLOT;
+        mbar_expect_tx(&full[s], (uint32_t)(nbox * a.src_box * 128) + (OTFT ? (uint32_t)(L * 128) : 0u));
         for (int i = 0; i < nbox; ++i) {
             const int r0 = i * a.src_box;
             if (a.src_jdim == 1) tma_load_3d(buf + r0 * 16, &a.src, c0, r0, o, &full[s]);
             else tma_load_3d(buf + r0 * 16, &a.src, c0, o, r0, &full[s]);
         }
+        if constexpr (OTFT)
+            for (int r0 = 0; r0 < L; r0 += a.otf_box) tma_load_3d(buf + L * 16 + r0 * 16, &a.otfmap, c0, o, r0, &full[s]);
     };
     if (tid == 0)
         for (int s = 0; s < NS; ++s) {
@@ -93,19 +114,12 @@ __global__ void __launch_bounds__(16 * R, 1) k_col_pipe(const __grid_constant__ 
         if (tile >= total) break;
         const int s = it % NS;
         const uint32_t ph = (uint32_t)((it / NS) & 1);
-        float2* buf = base + s * L * 16;
+        float2* buf = base + s * SLOT;
+        const float2* obuf = buf + L * 16;  // OTF tile (OTFT)
         const int o = tile / a.ntiles;
         const int c0 = (tile - o * a.ntiles) * 32;
 
-        float2 ov[OTF && !H16 ? SPLIT : 1][OTF && !H16 ? R : 1];
-        if constexpr (OTF && !H16) {
-            const float2* op = a.otf + o * a.otf_os + (c0 >> 1) + t;
-#pragma unroll
-            for (int h = 0; h < SPLIT; ++h)
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-                    ov[h][r] = __ldg(op + (int64_t)(SPLIT * (j + R * r) + h) * a.otf_js);
-        }
+        (void)obuf;
         // FP16 OTF (H16): raw values and plane scales are only loaded here and
         // converted where they are used, so the loads stay in flight across
         // the tile wait and the forward transform like the FP32 ones.
@@ -149,7 +163,7 @@ __global__ void __launch_bounds__(16 * R, 1) k_col_pipe(const __grid_constant__ 
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const float2 x = buf[p1(h * LH + j + R * r, t)];
-                v[h][r] = r == 0 ? x : (D1 < 0 ? cmul(x, w2[r]) : cmulc(x, w2[r]));
+                v[h][r] = r == 0 ? x : (D1 < 0 ? cmul(x, w2(r)) : cmulc(x, w2(r)));
             }
             dft<R, D1>(v[h]);
         }
@@ -164,7 +178,7 @@ __global__ void __launch_bounds__(16 * R, 1) k_col_pipe(const __grid_constant__ 
                         const float2 q = __half22float2(oh[h][r]);
                         w = make_float2(q.x * os[h][r], q.y * os[h][r]);
                     } else {
-                        w = ov[h][r];
+                        w = obuf[p1(SPLIT * (j + R * r) + h, t)];
                     }
                     v[h][r] = MODE == COL_OTF ? cmul(v[h][r], w) : cmulc(v[h][r], w);
                 }
@@ -181,7 +195,7 @@ __global__ void __launch_bounds__(16 * R, 1) k_col_pipe(const __grid_constant__ 
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const float2 x = buf[p1(h * LH + j + R * r, t)];
-                    v[h][r] = r == 0 ? x : cmulc(x, w2[r]);
+                    v[h][r] = r == 0 ? x : cmulc(x, w2(r));
                 }
                 dft<R, +1>(v[h]);
             }

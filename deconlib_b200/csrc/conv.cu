@@ -486,7 +486,8 @@ bool encode_spectrum_map(CUtensorMap* map, const float2* base, int64_t pitch, in
 // L = 64, 256; the half-zero split (SPLIT 2) for L = 128, 512 when the
 // non-zero input / kept output fits in half the axis.
 // h16: the axial (OTF) modes read the FP16 OTF (mixed precision).
-static void* pick_pipe(int L, int mode, int nin, int nout, int* R, int* split, bool h16 = false) {
+static void* pick_pipe(int L, int mode, int nin, int nout, int* R, int* split, bool h16 = false,
+                       bool lean = false) {
     const bool otf = mode == COL_OTF || mode == COL_OTF_CONJ;
     const bool half_ok = (mode == COL_FWD && nin <= L / 2) || (mode == COL_INV && nout <= L / 2) ||
                          (otf && nin <= L / 2 && nout <= L / 2);
@@ -498,10 +499,13 @@ static void* pick_pipe(int L, int mode, int nin, int nout, int* R, int* split, b
             case COL_FWD: return (void*)k_col_pipe<RR, SS, COL_FWD>;                             \
             case COL_INV: return (void*)k_col_pipe<RR, SS, COL_INV>;                             \
             case COL_OTF:                                                                        \
-                return h16 ? (void*)k_col_pipe<RR, SS, COL_OTF, true> : (void*)k_col_pipe<RR, SS, COL_OTF>; \
+                return h16 ? (void*)k_col_pipe<RR, SS, COL_OTF, true>                           \
+                           : (lean ? (void*)k_col_pipe<RR, SS, COL_OTF, false, true>            \
+                                   : (void*)k_col_pipe<RR, SS, COL_OTF>);                       \
             case COL_OTF_CONJ:                                                                   \
                 return h16 ? (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, true>                      \
-                           : (void*)k_col_pipe<RR, SS, COL_OTF_CONJ>;                           \
+                           : (lean ? (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, false, true>       \
+                                   : (void*)k_col_pipe<RR, SS, COL_OTF_CONJ>);                  \
         }                                                                                        \
     } while (0)
     if (L == 256) DK_PIPE(16, 1);
@@ -522,7 +526,11 @@ static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const C
     int R = 0, split = 0;
     const bool otf_mode = mode == COL_OTF || mode == COL_OTF_CONJ;
     const bool h16 = otf_mode && p.precision == 1 && p.otf16 != nullptr;
-    void* fn = getenv("DECON_NO_PIPE") ? nullptr : pick_pipe(ax.L, mode, nin, nout, &R, &split, h16);
+    // axial pass of length 256: the lean two-CTA kernel (measured 153 vs 166 us
+    // at 128x256x256 on the B200); DECON_PIPE_LEAN=0 / 1 overrides
+    const char* le = getenv("DECON_PIPE_LEAN");
+    const bool lean = otf_mode && !h16 && (le ? le[0] == '1' : ax.L == 256);
+    void* fn = getenv("DECON_NO_PIPE") ? nullptr : pick_pipe(ax.L, mode, nin, nout, &R, &split, h16, lean);
     if (!fn) return false;
     PipeArgs a;
     memset(&a, 0, sizeof(a));
@@ -531,6 +539,8 @@ static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const C
     a.otf = p.otf;
     a.otf16 = p.otf16;
     a.otf_inv = p.otf_inv;
+    a.otfmap = p.tm_otf_z;
+    a.otf_box = p.otf_box;
     a.otf_js = p.F[1] * p.P;
     a.otf_os = p.P;
     a.tw = ax.tw;
@@ -544,8 +554,9 @@ static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const C
     a.src_box = src_box;
     a.dst_box = dst_box;
     const int L = ax.L;
-    const int ns = L >= 512 ? 2 : 3;
-    const size_t smem = 1024 + (size_t)ns * L * 16 * sizeof(float2);
+    const int ns = pipe_slots(L, lean);
+    const bool otf_tile = otf_mode && !h16;  // FP32 OTF tile in the ring slot
+    const size_t smem = 1024 + (size_t)ns * L * 16 * sizeof(float2) * (otf_tile ? 2 : 1);
     const int nthr = 16 * R;
     *status = DECON_OK;
     int per_sm = 1;

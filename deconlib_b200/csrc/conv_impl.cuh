@@ -65,6 +65,8 @@ struct ColTmaArgs {
 // Persistent pipelined column pass (k_col_pipe).
 struct PipeArgs {
     CUtensorMap src, dst;
+    CUtensorMap otfmap;     // FP32 OTF [Fz][Fy][P] as TMA boxes (axial pass)
+    int otf_box;
     const float2* otf;      // OTF base for the axial pass
     const __half2* otf16;   // mixed precision: FP16 OTF, OTF = otf16 * otf_inv[kz]
     const float* otf_inv;

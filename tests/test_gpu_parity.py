@@ -255,20 +255,24 @@ def test_pdhg_convergence_bin_plain_operator(D, g32, g64):
 def test_column_pass_variants_agree(D, monkeypatch, shape, fft):
     # The pipelined column kernel (R x R Stockham, half-zero split for 128 /
     # 512), the one-tile TMA kernel (DECON_NO_PIPE) and the plain-load kernel
-    # (DECON_NO_TMA) compute the same transforms with different factorings.
+    # (DECON_NO_TMA) compute the same transforms with different factorings;
+    # DECON_PIPE_LEAN selects the two-CTA axial kernel (twiddles in shared
+    # memory, one ring slot) or the one-CTA kernel (same arithmetic).
     rng = np.random.default_rng(11)
     kshape = tuple(f - n + 1 for n, f in zip(shape, fft))
     k = rng.random(kshape).astype(np.float32)
     x = rng.random(shape).astype(np.float32)
     outs = []
-    for env in ({}, {"DECON_NO_PIPE": "1"}, {"DECON_NO_TMA": "1"}):
-        for key in ("DECON_NO_PIPE", "DECON_NO_TMA"):
+    keys = ("DECON_NO_PIPE", "DECON_NO_TMA", "DECON_PIPE_LEAN")
+    for env in ({}, {"DECON_NO_PIPE": "1"}, {"DECON_NO_TMA": "1"}, {"DECON_PIPE_LEAN": "0"},
+                {"DECON_PIPE_LEAN": "1"}):
+        for key in keys:
             monkeypatch.delenv(key, raising=False)
         for key, val in env.items():
             monkeypatch.setenv(key, val)
         c = D.LinearFFTConvolver(k, shape, fft_shape=fft)
         outs.append((cpu(c.forward(x)), cpu(c.adjoint(x))))
-    for key in ("DECON_NO_PIPE", "DECON_NO_TMA"):
+    for key in keys:
         monkeypatch.delenv(key, raising=False)
     for f, a in outs[1:]:
         assert rel(f, outs[0][0]) < 1e-6
