@@ -36,8 +36,9 @@ __host__ __device__ constexpr int pipe_slots(int L, bool lean) { return lean ? 1
 
 // H16: the OTF is read from the FP16 copy and rescaled per kz plane (mixed
 // precision); the transforms and the product stay FP32.
-// LEAN (axial pass only): second-stage twiddles in shared memory instead of
-// registers, two ring slots, 128 registers, so two CTAs share an SM.
+// LEAN: twiddles in shared memory instead of registers, one ring slot,
+// <= 128 registers, so two CTAs share an SM and one CTA's barriers and loads
+// overlap the other's arithmetic.
 template <int R, int SPLIT, int MODE, bool H16 = false, bool LEAN = false>
 __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_constant__ PipeArgs a) {
     constexpr int LH = R * R;          // sub-transform length
@@ -68,12 +69,21 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
         if constexpr (LEAN) return w2s[r][j];
         else return w2r[r];
     };
-    // split twiddles W_L^n, n = j + R r
-    float2 ws[SPLIT == 2 ? R : 1];
+    // split twiddles W_L^n, n = j + R r: registers, or (LEAN) a shared table
+    float2 wsr[SPLIT == 2 && !LEAN ? R : 1];
+    __shared__ float2 wss[SPLIT == 2 && LEAN ? R * R : 1];
     if constexpr (SPLIT == 2) {
+        if constexpr (LEAN) {
+            for (int q = tid; q < R * R; q += blockDim.x) wss[q] = __ldg(&a.tw[q * a.tws]);
+        } else {
 #pragma unroll
-        for (int r = 0; r < R; ++r) ws[r] = __ldg(&a.tw[(j + R * r) * a.tws]);
+            for (int r = 0; r < R; ++r) wsr[r] = __ldg(&a.tw[(j + R * r) * a.tws]);
+        }
     }
+    auto ws = [&](int r) -> float2 {
+        if constexpr (LEAN) return wss[j + R * r];
+        else return wsr[SPLIT == 2 ? r : 0];
+    };
 
     // FP16 OTF: this thread's kz planes are fixed, so are their scales
     float os[H16 ? SPLIT : 1][H16 ? R : 1];
@@ -141,7 +151,7 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
                 const int n = j + R * r;
                 const float2 x = n < a.nin ? buf[p1(n, t)] : make_float2(0.f, 0.f);
                 v[0][r] = x;
-                if constexpr (SPLIT == 2) v[1][r] = cmul(x, ws[r]);
+                if constexpr (SPLIT == 2) v[1][r] = cmul(x, ws(r));
             }
         } else {
 #pragma unroll
@@ -218,7 +228,7 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
             for (int r = 0; r < R; ++r) {
                 const int n = j + R * r;
                 float2 y = v[0][r];
-                if constexpr (SPLIT == 2) y = cadd(y, cmulc(v[1][r], ws[r]));
+                if constexpr (SPLIT == 2) y = cadd(y, cmulc(v[1][r], ws(r)));
                 if (n < a.nout) buf[p1(n, t)] = y;
             }
         }
