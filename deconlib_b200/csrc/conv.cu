@@ -344,6 +344,8 @@ int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cva
              win.wx == p.N[2] && (reinterpret_cast<uintptr_t>(in) & 15) == 0;
     a.T = p.T_x;
     a.nrows = nz_rows * a.Ny;
+    if (a.ax.L == 64 || a.ax.L == 128 || a.ax.L == 256 || a.ax.L == 512 || a.ax.L == 1024)
+        if (a.T != x_lines(a.ax.L)) return fail(DECON_ERR_UNSUPPORTED, "X pass lines per CTA mismatch");
     {
         const int L = a.ax.L;
         const int64_t nin = p.odd ? std::min<int64_t>(a.Nx, L) : std::min<int64_t>((a.Nx + 1) / 2, L);
@@ -412,6 +414,8 @@ int launch_xc2r(const ConvPlan& p, int epi, const float2* in, Win3 win, float* o
         a.vec4 = full && !p.odd && (p.N[2] % 4) == 0 && al(out) && al(aux0) && al(aux1);
     }
     a.T = p.T_x;
+    if (a.ax.L == 64 || a.ax.L == 128 || a.ax.L == 256 || a.ax.L == 512 || a.ax.L == 1024)
+        if (a.T != x_lines(a.ax.L)) return fail(DECON_ERR_UNSUPPORTED, "X pass lines per CTA mismatch");
     a.scale = (float)(1.0 / ((double)p.F[0] * (double)p.F[1] * (double)p.F[2]));
     a.win = win;
     a.out = out;

@@ -40,12 +40,16 @@ __device__ __forceinline__ int phys(int j, int t, int T) { return j * T + (t ^ (
 // SW = 1: T = 16 lines whose rows are exactly 128 bytes, laid out as the TMA
 // 128-byte swizzle writes them: 16-byte chunk (t / 2) XOR (j mod 8).  Both
 // keep a warp's accesses to consecutive lines at one point conflict-free.
+// SW >= 2: the XOR swizzle with a compile-time T = SW (the shifts and masks
+// fold into the address arithmetic).
 template <int SW>
 __device__ __forceinline__ int physw(int j, int t, int T) {
     if constexpr (SW == 0) {
         return phys(j, t, T);
-    } else {
+    } else if constexpr (SW == 1) {
         return j * 16 + ((((t >> 1) ^ (j & 7)) << 1) | (t & 1));
+    } else {
+        return j * SW + (t ^ (j & (SW - 1)));
     }
 }
 

@@ -82,11 +82,17 @@ __device__ __forceinline__ float fetch_x(const XR2CArgs& a, const RowSrc& r, int
 // pass 1: X R2C
 // ---------------------------------------------------------------------------
 
+// Lines per CTA of the X passes for a compile-time length (the host's rule:
+// T x L <= 8192 complex values and T x L / 32 <= 256 threads, T <= 32).
+__host__ __device__ constexpr int x_lines(int LS) { return LS >= 1024 ? 8 : (LS >= 512 ? 16 : 32); }
+
 template <int PRO, int LS>
-__global__ void __launch_bounds__(kFftThreads) k_xr2c(XR2CArgs a) {
+__global__ void __launch_bounds__(kFftThreads, 3) k_xr2c(XR2CArgs a) {
     extern __shared__ float2 sm[];
     __shared__ RowSrc rsrc[32];  // per-row source (general path)
-    const int T = a.T, L = a.ax.L, tid = threadIdx.x;
+    constexpr int TC = LS > 0 ? x_lines(LS) : 0;  // compile-time lines per CTA
+    const int T = TC > 0 ? TC : a.T, L = LS > 0 ? LS : a.ax.L, tid = threadIdx.x;
+    auto phys = [&](int j, int t, int) { return physw<TC>(j, t, T); };
     const int64_t row0 = (int64_t)blockIdx.x * T;
     // packed points that can be non-zero
     const int nin = a.odd ? (int)(a.Nx < L ? a.Nx : L) : (int)(((a.Nx + 1) >> 1) < L ? ((a.Nx + 1) >> 1) : L);
@@ -94,6 +100,7 @@ __global__ void __launch_bounds__(kFftThreads) k_xr2c(XR2CArgs a) {
         const int q4 = (int)(a.Nx >> 2);  // float4 per row
         const int nq = T * q4;
         constexpr int U = 4;
+        #pragma unroll 1
         for (int c0 = tid; c0 < nq; c0 += U * blockDim.x) {
             float4 v[U];
 #pragma unroll
@@ -127,6 +134,7 @@ __global__ void __launch_bounds__(kFftThreads) k_xr2c(XR2CArgs a) {
             rsrc[tid] = rs;
         }
         __syncthreads();
+        #pragma unroll 1
         for (int q = tid; q < T * nin; q += blockDim.x) {
             const int t = fdiv(q, a.fd_nin), n = q - t * nin;
             const RowSrc rs = rsrc[t];
@@ -143,14 +151,17 @@ __global__ void __launch_bounds__(kFftThreads) k_xr2c(XR2CArgs a) {
     if constexpr (LS == 0) {
         // the runtime-radix path reads every point: zero the padding
         const int nz = L - nin;
+        #pragma unroll 1
         for (int q = tid; q < T * nz; q += blockDim.x) {
             const int t = q / nz;
             sm[phys(nin + (q - t * nz), t, T)] = make_float2(0.f, 0.f);
         }
     }
     __syncthreads();
-    fft_lines<-1, LS>(sm, T, tid % T, tid / T, a.ax, nin);
+    if constexpr (LS > 0) fft_lines_pow2<LS, -1, 1, TC>(sm, T, tid % T, tid / T, a.ax.tw, a.ax.tws, nin);
+    else fft_lines<-1, LS>(sm, T, tid % T, tid / T, a.ax, nin);
     const int H = a.Hx;
+    #pragma unroll 1
     for (int q = tid; q < T * H; q += blockDim.x) {
         const int t = fdiv(q, a.fd_H), k = q - t * H;
         const int64_t row = row0 + t;
@@ -207,9 +218,14 @@ __global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
     __shared__ float2 nyq[32];    // X[M] of each row (even Fx)
     __shared__ int64_t obase[32];  // output index of x = 0 of each row (general path)
     constexpr int64_t kOutside = INT64_MIN;
-    const int T = a.T, L = a.ax.L, tid = threadIdx.x;
+    // a compile-time T here made the kernel spill under the 3-CTA register
+    // cap; the C2R keeps the run-time T
+    constexpr int TC = 0;
+    const int T = TC > 0 ? TC : a.T, L = LS > 0 ? LS : a.ax.L, tid = threadIdx.x;
+    auto phys = [&](int j, int t, int) { return physw<TC>(j, t, T); };
     const int64_t row0 = (int64_t)blockIdx.x * T;
     if (a.odd) {
+        #pragma unroll 1
         for (int q = tid; q < T * L; q += blockDim.x) {
             const int t = fdiv(q, a.fd_L), k = q - t * L;
             const int64_t row = row0 + t;
@@ -229,6 +245,7 @@ __global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
         const int h2 = M >> 1;  // float4 (two complex) per row
         const int nq = T * h2;
         constexpr int U = 4;
+        #pragma unroll 1
         for (int c0 = tid; c0 < nq; c0 += U * blockDim.x) {
             float4 v[U];
 #pragma unroll
@@ -250,6 +267,7 @@ __global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
                 }
             }
         }
+        #pragma unroll 1
         for (int t = tid; t < T; t += blockDim.x) {
             const int64_t row = row0 + t;
             const bool ok = row < a.nrows;
@@ -261,6 +279,7 @@ __global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
         // Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) W_Fx^-k, one
         // thread per pair (k, M - k); irfft ignores Im of DC and Nyquist.
         const int npair = (M >> 1) + 1;
+        #pragma unroll 1
         for (int q = tid; q < T * npair; q += blockDim.x) {
             const int t = fdiv(q, a.fd_npair), k = q - t * npair;
             if (k == 0) {
@@ -293,13 +312,15 @@ __global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
     }
     // outputs beyond the kept x range are not needed
     const int nout = a.odd ? (int)(a.Nx < L ? a.Nx : L) : (int)(((a.Nx + 1) >> 1) < L ? ((a.Nx + 1) >> 1) : L);
-    fft_lines<+1, LS>(sm, T, tid % T, tid / T, a.ax, 1 << 30, nout);
+    if constexpr (LS > 0) fft_lines_pow2<LS, +1, 1, TC>(sm, T, tid % T, tid / T, a.ax.tw, a.ax.tws, 1 << 30, nout);
+    else fft_lines<+1, LS>(sm, T, tid % T, tid / T, a.ax, 1 << 30, nout);
 
     double acc = 0.0;
     const int64_t Nx = a.Nx;
     if (a.vec4) {
         // plain rows, full window: 4 voxels per thread step
         const int q4 = (int)(Nx >> 2), nq = T * q4;
+        #pragma unroll 1
         for (int c = tid; c < nq; c += blockDim.x) {
             const int t = fdiv(c, a.fd_q4), x4 = c - t * q4;
             const int64_t row = row0 + t;
@@ -354,6 +375,7 @@ __global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
         }
         __syncthreads();
         const int nx = (int)Nx;
+        #pragma unroll 1
         for (int q = tid; q < T * nx; q += blockDim.x) {
             const int t = fdiv(q, a.fd_Nx);
             const int x = q - t * nx;
