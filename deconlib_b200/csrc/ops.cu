@@ -67,6 +67,58 @@ __global__ void k_banded_inner(const float* __restrict__ in, float* __restrict__
     }
 }
 
+// inner % 4 == 0 and 16-byte aligned rows: four neighbouring columns per
+// thread as float4 (same per-element float operations as k_banded_inner).
+__global__ void k_banded_inner4(const float* __restrict__ in, float* __restrict__ out, int64_t outer,
+                                int64_t n_in, int64_t inner, int64_t n_out,
+                                const int32_t* __restrict__ idx, const float* __restrict__ w,
+                                int width) {
+    const int64_t q4 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t inner4 = inner >> 2;
+    if (q4 >= inner4) return;
+    const int64_t j = blockIdx.y;
+    const int32_t* ij = idx + j * width;
+    const float* wj = w + j * width;
+    for (int64_t o = blockIdx.z; o < outer; o += gridDim.z) {
+        const float4* base = reinterpret_cast<const float4*>(in + o * n_in * inner) + q4;
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int k = 0; k < width; ++k) {
+            const float wk = __ldg(wj + k);
+            const float4 v = __ldg(base + (int64_t)__ldg(ij + k) * inner4);
+            acc.x = __fadd_rn(acc.x, __fmul_rn(wk, v.x));
+            acc.y = __fadd_rn(acc.y, __fmul_rn(wk, v.y));
+            acc.z = __fadd_rn(acc.z, __fmul_rn(wk, v.z));
+            acc.w = __fadd_rn(acc.w, __fmul_rn(wk, v.w));
+        }
+        reinterpret_cast<float4*>(out + (o * n_out + j) * inner)[q4] = acc;
+    }
+}
+
+// Resampled axis innermost with at most kBandW taps: a thread keeps its
+// output's taps and weights in registers and walks many rows.
+constexpr int kBandW = 8;
+__global__ void k_banded_last_rows(const float* __restrict__ in, float* __restrict__ out, int64_t outer,
+                                   int64_t n_in, int64_t n_out, const int32_t* __restrict__ idx,
+                                   const float* __restrict__ w, int width) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n_out) return;
+    int32_t ij[kBandW];
+    float wj[kBandW];
+#pragma unroll
+    for (int k = 0; k < kBandW; ++k) {
+        ij[k] = k < width ? __ldg(idx + j * width + k) : 0;
+        wj[k] = k < width ? __ldg(w + j * width + k) : 0.f;
+    }
+    for (int64_t o = blockIdx.y; o < outer; o += gridDim.y) {
+        const float* base = in + o * n_in;
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k < kBandW; ++k)
+            if (k < width) acc = __fadd_rn(acc, __fmul_rn(wj[k], __ldg(base + ij[k])));
+        out[o * n_out + j] = acc;
+    }
+}
+
 // Resampled axis innermost (inner == 1): threads along the output axis.
 __global__ void k_banded_last(const float* __restrict__ in, float* __restrict__ out, int64_t outer,
                               int64_t n_in, int64_t n_out, const int32_t* __restrict__ idx,
@@ -240,13 +292,25 @@ int decon_banded_axis(const float* in, float* out, int64_t outer, int64_t n_in, 
     if (n == 0) return DECON_OK;
     const cudaStream_t st = as_stream(stream);
     if (inner == 1) {
-        dim3 g((unsigned)cdiv(n_out, 256), (unsigned)std::min<int64_t>(outer, 65535));
-        k_banded_last<<<g, 256, 0, st>>>(in, out, outer, n_in, n_out, idx, w, width);
+        if (width <= kBandW) {
+            // enough CTAs to fill the GPU, each walking many rows
+            const int64_t gx = cdiv(n_out, 256);
+            const int64_t gy = std::max<int64_t>(1, std::min<int64_t>(outer, cdiv((int64_t)sm_count() * 16, gx)));
+            dim3 g((unsigned)gx, (unsigned)gy);
+            k_banded_last_rows<<<g, 256, 0, st>>>(in, out, outer, n_in, n_out, idx, w, width);
+        } else {
+            dim3 g((unsigned)cdiv(n_out, 256), (unsigned)std::min<int64_t>(outer, 65535));
+            k_banded_last<<<g, 256, 0, st>>>(in, out, outer, n_in, n_out, idx, w, width);
+        }
     } else {
-        const int thr = inner >= 256 ? 256 : (int)round_up(inner, 32);
         if (n_out > 65535) return fail(DECON_ERR_UNSUPPORTED, "resampled axis longer than 65535");
-        dim3 g((unsigned)cdiv(inner, thr), (unsigned)n_out, (unsigned)std::min<int64_t>(outer, 65535));
-        k_banded_inner<<<g, thr, 0, st>>>(in, out, outer, n_in, inner, n_out, idx, w, width);
+        const bool v4 = (inner % 4) == 0 && (reinterpret_cast<uintptr_t>(in) & 15) == 0 &&
+                        (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+        const int64_t cols = v4 ? inner / 4 : inner;
+        const int thr = cols >= 256 ? 256 : (int)round_up(cols, 32);
+        dim3 g((unsigned)cdiv(cols, thr), (unsigned)n_out, (unsigned)std::min<int64_t>(outer, 65535));
+        if (v4) k_banded_inner4<<<g, thr, 0, st>>>(in, out, outer, n_in, inner, n_out, idx, w, width);
+        else k_banded_inner<<<g, thr, 0, st>>>(in, out, outer, n_in, inner, n_out, idx, w, width);
     }
     DK_LAUNCHED();
     return DECON_OK;

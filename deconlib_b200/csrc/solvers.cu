@@ -219,12 +219,21 @@ __device__ double fold_slot(const PdhgDev* s, int slot) {
 // The Malitsky-Pock scalar step (pdhg_mlx.py:749-857) in FP64, one CTA.
 __global__ void __launch_bounds__(256) k_step(PdhgDev* s) {
     if (s->stop) return;
-    const double dx2 = fold_slot(s, kSlotDx2);
-    const double xc2 = fold_slot(s, kSlotXc2);
-    const double xn2 = fold_slot(s, kSlotXn2);
-    const double dA2 = fold_slot(s, kSlotDA2);
-    const double dL2 = fold_slot(s, kSlotDL2);
+    // the five FP64 sums folded at once, one warp per slot (fixed order)
+    __shared__ double red[5];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < 5) {
+        const int slot = warp == 0 ? kSlotDx2 : warp == 1 ? kSlotXc2 : warp == 2 ? kSlotXn2
+                       : warp == 3 ? kSlotDA2 : kSlotDL2;
+        const double* p = s->partials + slot * kPdhgGrid;
+        double v = 0.0;
+        for (int i = lane; i < kPdhgGrid; i += 32) v += p[i];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp] = v;
+    }
+    __syncthreads();
     if (threadIdx.x != 0) return;
+    const double dx2 = red[0], xc2 = red[1], xn2 = red[2], dA2 = red[3], dL2 = red[4];
     const int k = s->k;
     const double tau = s->tau, sigma = s->sigma, theta = s->theta, ss = s->step_scale;
     const double dK2 = dA2 + dL2;
