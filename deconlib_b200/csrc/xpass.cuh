@@ -213,14 +213,14 @@ __device__ __forceinline__ void epilogue(const XC2RArgs& a, int64_t i, float v, 
 }
 
 template <int EPI, int LS>
-__global__ void __launch_bounds__(kFftThreads) k_xc2r(XC2RArgs a) {
+__global__ void __launch_bounds__(kFftThreads, 2) k_xc2r(XC2RArgs a) {
     extern __shared__ float2 sm[];
     __shared__ float2 nyq[32];    // X[M] of each row (even Fx)
     __shared__ int64_t obase[32];  // output index of x = 0 of each row (general path)
     constexpr int64_t kOutside = INT64_MIN;
-    // a compile-time T here made the kernel spill under the 3-CTA register
-    // cap; the C2R keeps the run-time T
-    constexpr int TC = 0;
+    // compile-time lines per CTA from L = 512 on (measured 211 -> 198 us at
+    // Fx = 1024); at L = 256 it brought no gain and spilled the loss epilogues
+    constexpr int TC = LS >= 512 ? x_lines(LS) : 0;
     const int T = TC > 0 ? TC : a.T, L = LS > 0 ? LS : a.ax.L, tid = threadIdx.x;
     auto phys = [&](int j, int t, int) { return physw<TC>(j, t, T); };
     const int64_t row0 = (int64_t)blockIdx.x * T;

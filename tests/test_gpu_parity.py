@@ -251,7 +251,8 @@ def test_pdhg_convergence_bin_plain_operator(D, g32, g64):
 @pytest.mark.parametrize("shape,fft", [((64, 128, 128), (128, 256, 256)),
                                        ((128, 256, 256), (256, 512, 512)),
                                        ((20, 60, 40), (64, 128, 128)),
-                                       ((30, 100, 90), (64, 256, 256))])
+                                       ((30, 100, 90), (64, 256, 256)),
+                                       ((8, 24, 500), (16, 64, 1024))])
 def test_column_pass_variants_agree(D, monkeypatch, shape, fft):
     # The pipelined column kernel (R x R Stockham, half-zero split for 128 /
     # 512), the one-tile TMA kernel (DECON_NO_PIPE) and the plain-load kernel
@@ -321,3 +322,18 @@ def test_kernel_shared_memory_opt_in_never_shrinks(D):
     c = cpu(big.forward(x))
     assert rel(b, a) < 1e-5
     np.testing.assert_array_equal(a, c)
+
+
+@pytest.mark.parametrize("fx", [1024, 2048])
+def test_long_x_axis_matches_fp64_fft(D, fx):
+    # X passes of packed length 512 and 1024 (compile-time lines per CTA)
+    rng = np.random.default_rng(12)
+    n, k = (6, 20, fx // 2), (3, 5, fx // 4)
+    x = rng.random(n)
+    ker = rng.random(k)
+    f = (8, 24, fx)
+    ref_f = np.fft.irfftn(np.fft.rfftn(x, f) * np.fft.rfftn(
+        np.asarray(D.pad_corner_origin_kernel(ker / ker.sum(), f)), f), f)[:n[0], :n[1], :n[2]]
+    c = D.LinearFFTConvolver(ker.astype(np.float32), n, fft_shape=f)
+    got = cpu(c.forward(x.astype(np.float32)))
+    assert rel(got, ref_f) < 2e-6
