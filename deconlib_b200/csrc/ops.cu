@@ -109,6 +109,8 @@ __global__ void k_banded_last_rows(const float* __restrict__ in, float* __restri
         ij[k] = k < width ? __ldg(idx + j * width + k) : 0;
         wj[k] = k < width ? __ldg(w + j * width + k) : 0.f;
     }
+    // rows are independent: unrolled so that several rows' gathers are in flight
+#pragma unroll 4
     for (int64_t o = blockIdx.y; o < outer; o += gridDim.y) {
         const float* base = in + o * n_in;
         float acc = 0.f;
