@@ -32,7 +32,7 @@ namespace dk {
 __device__ __forceinline__ int p1(int row, int t) { return physw<1>(row, t, 16); }
 
 // Ring slots of k_col_pipe (the host sizes shared memory with the same rule).
-__host__ __device__ constexpr int pipe_slots(int L, bool lean) { return lean ? 1 : (L >= 512 ? 2 : 3); }
+__host__ __device__ constexpr int pipe_slots(int L, bool lean) { return lean ? 2 : (L >= 512 ? 2 : 3); }
 
 // H16: the OTF is read from the FP16 copy and rescaled per kz plane (mixed
 // precision); the transforms and the product stay FP32.
@@ -47,11 +47,15 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
     constexpr bool OTF = (MODE == COL_OTF || MODE == COL_OTF_CONJ);
     constexpr bool INV_FIRST = (MODE == COL_INV);
     constexpr bool OTFT = OTF && !H16;              // OTF tile staged by TMA
-    constexpr int SLOT = L * 16 * (OTFT ? 2 : 1);   // float2 per ring slot
+    // LEAN axial pass: one OTF buffer beside a two-slot spectrum ring, loaded
+    // for the next tile as soon as the current tile's product is done
+    constexpr bool OTF1 = OTFT && LEAN;
+    constexpr int SLOT = L * 16 * (OTFT && !OTF1 ? 2 : 1);  // float2 per ring slot
     constexpr int D1 = INV_FIRST ? +1 : -1;  // direction of the first transform
     extern __shared__ unsigned char smraw[];
     float2* base = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
     __shared__ uint64_t full[NS];
+    __shared__ uint64_t obar;  // OTF1: the OTF buffer arrived
     const int tid = threadIdx.x, t = tid & 15, j = tid >> 4;
     const int total = a.nouter * a.ntiles;
 
@@ -94,8 +98,10 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
             for (int r = 0; r < R; ++r) os[h][r] = __ldg(a.otf_inv + SPLIT * (j + R * r) + h);
     }
 
+    float2* otf1 = base + NS * SLOT;  // OTF1 buffer
     if (tid == 0) {
         for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
+        if constexpr (OTF1) mbar_init(&obar, 1);
         fence_proxy_async_smem();
     }
     __syncthreads();
@@ -104,20 +110,29 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
         const int o = tile / a.ntiles;
         const int c0 = (tile - o * a.ntiles) * 32;
         float2* buf = base + s * SLOT;
-        mbar_expect_tx(&full[s], (uint32_t)(nbox * a.src_box * 128) + (OTFT ? (uint32_t)(L * 128) : 0u));
+        mbar_expect_tx(&full[s], (uint32_t)(nbox * a.src_box * 128) + (OTFT && !OTF1 ? (uint32_t)(L * 128) : 0u));
         for (int i = 0; i < nbox; ++i) {
             const int r0 = i * a.src_box;
             if (a.src_jdim == 1) tma_load_3d(buf + r0 * 16, &a.src, c0, r0, o, &full[s]);
             else tma_load_3d(buf + r0 * 16, &a.src, c0, o, r0, &full[s]);
         }
-        if constexpr (OTFT)
+        if constexpr (OTFT && !OTF1)
             for (int r0 = 0; r0 < L; r0 += a.otf_box) tma_load_3d(buf + L * 16 + r0 * 16, &a.otfmap, c0, o, r0, &full[s]);
     };
-    if (tid == 0)
+    auto issue_otf = [&](int tile) {
+        const int o = tile / a.ntiles;
+        const int c0 = (tile - o * a.ntiles) * 32;
+        mbar_expect_tx(&obar, (uint32_t)(L * 128));
+        for (int r0 = 0; r0 < L; r0 += a.otf_box) tma_load_3d(otf1 + r0 * 16, &a.otfmap, c0, o, r0, &obar);
+    };
+    if (tid == 0) {
         for (int s = 0; s < NS; ++s) {
             const int tile = blockIdx.x + s * gridDim.x;
             if (tile < total) issue(tile, s);
         }
+        if constexpr (OTF1)
+            if ((int)blockIdx.x < total) issue_otf(blockIdx.x);
+    }
 
     for (int it = 0;; ++it) {
         const int tile = blockIdx.x + it * gridDim.x;
@@ -125,7 +140,7 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
         const int s = it % NS;
         const uint32_t ph = (uint32_t)((it / NS) & 1);
         float2* buf = base + s * SLOT;
-        const float2* obuf = buf + L * 16;  // OTF tile (OTFT)
+        const float2* obuf = OTF1 ? otf1 : buf + L * 16;  // OTF tile (OTFT)
         const int o = tile / a.ntiles;
         const int c0 = (tile - o * a.ntiles) * 32;
 
@@ -178,6 +193,8 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
             dft<R, D1>(v[h]);
         }
         if constexpr (OTF) {
+            if constexpr (OTF1)
+                if (!__syncthreads_and(mbar_wait_bounded(&obar, (uint32_t)(it & 1)))) return;
             // X at m = j + R r  ->  x OTF  ->  inverse stage 1 in registers
 #pragma unroll
             for (int h = 0; h < SPLIT; ++h) {
@@ -195,6 +212,10 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
                 dft<R, +1>(v[h]);
             }
             __syncthreads();
+            if constexpr (OTF1) {
+                // every thread has read the OTF buffer: refill it for the next tile
+                if (tid == 0 && tile + (int)gridDim.x < total) issue_otf(tile + gridDim.x);
+            }
 #pragma unroll
             for (int h = 0; h < SPLIT; ++h)
 #pragma unroll

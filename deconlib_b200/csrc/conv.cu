@@ -559,8 +559,10 @@ static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const C
     a.dst_box = dst_box;
     const int L = ax.L;
     const int ns = pipe_slots(L, lean);
-    const bool otf_tile = otf_mode && !h16;  // FP32 OTF tile in the ring slot
-    const size_t smem = 1024 + (size_t)ns * L * 16 * sizeof(float2) * (otf_tile ? 2 : 1);
+    const bool otf_tile = otf_mode && !h16;  // FP32 OTF tile: in each ring slot, or (lean) one buffer
+    const size_t tile_bytes = (size_t)L * 16 * sizeof(float2);
+    const size_t smem = 1024 + (size_t)ns * tile_bytes * (otf_tile && !lean ? 2 : 1) +
+                        (otf_tile && lean ? tile_bytes : 0);
     const int nthr = 16 * R;
     *status = DECON_OK;
     int per_sm = 1;
