@@ -458,6 +458,67 @@ def run_mixed(D, iters=200):
 # ---------------------------------------------------------------------------
 
 
+def run_psf(reps=20, shape=(128, 256, 256), dxy=0.0425, dz=0.05):
+    """Widefield PSF synthesis (pupil_to_psf) on the device for the PDHG
+    workload's grid: an anti-aliased NA-1.4 pupil with a seeded smooth phase,
+    FFT-order z.  Device time by CUDA events over ``reps`` calls (inputs
+    resident); the NumPy loop of the same formula (psf/widefield.py:53-73)
+    timed on two planes and scaled to nz, and the device PSF's relative error
+    on those planes."""
+    import numpy as np
+    import torch
+
+    from deconlib_b200 import _lib
+    from deconlib_b200.deconvolution._device import stream
+
+    nz, ny, nx = shape
+    ky = np.fft.fftfreq(ny, dxy)[:, None]
+    kx = np.fft.fftfreq(nx, dxy)[None, :]
+    k = np.sqrt(kx * kx + ky * ky)
+    kmax = 1.4 / 0.525
+    w = np.clip((kmax - k) * max(ny, nx) * dxy + 0.5, 0.0, 1.0)
+    kz = np.sqrt(np.maximum((1.515 / 0.525) ** 2 - k * k, 0.0))
+    rho = np.clip(k / kmax, 0, 1)
+    pupil = (w * np.exp(0.7j * (6 * rho ** 4 - 6 * rho ** 2 + 1))).astype(np.complex64)
+    z = np.fft.fftfreq(nz) * nz * dz
+    pd = torch.from_numpy(pupil).cuda()
+    kzd = torch.from_numpy(kz).cuda()
+    zd = torch.from_numpy(z).cuda()
+    out = torch.empty(shape, device="cuda")
+    lib = _lib.load()
+
+    def call():
+        _lib.call("decon_pupil_to_psf", pd.data_ptr(), kzd.data_ptr(), zd.data_ptr(), nz, ny, nx, 1,
+                  out.data_ptr(), stream())
+
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    n0 = lib.decon_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        call()
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    launches = (lib.decon_launch_count() - n0) / reps
+    t = time.perf_counter()
+    ref = np.empty((2, ny, nx))
+    for i in range(2):
+        a = np.fft.ifft2(pupil.astype(np.complex128) * np.exp(2j * np.pi * kz * z[i]))
+        ref[i] = a.real ** 2 + a.imag ** 2
+    np_ms = (time.perf_counter() - t) / 2 * nz * 1e3
+    tot = nz * ny * nx * np.sum(np.abs(pupil.astype(np.complex128)) ** 2) / (ny * nx) ** 2
+    got = out[:2].double().cpu().numpy()
+    err = float(np.linalg.norm(got - ref / tot) / np.linalg.norm(ref / tot))
+    vox = nz * ny * nx
+    return {"shape": list(shape), "ms": ms, "gvox_per_s": vox / ms / 1e6,
+            "algorithmic_bytes_per_voxel": 20, "achieved_gbs": 20 * vox / ms / 1e6,
+            "launches_per_call": launches, "numpy_ms_estimate": np_ms,
+            "rel_l2_vs_fp64_planes01": err}
+
+
 def zpass_bytes(n_shape, f_shape):
     nz = n_shape[0]
     fz, fy, fx = f_shape
@@ -643,6 +704,8 @@ def run_ours(args, ws, rank, local):
         line["batched"] = run_batched(D, args.batch_iters)
     if args.mixed_iters > 0:
         line["mixed"] = run_mixed(D, args.mixed_iters)
+    if args.psf_reps > 0:
+        line["psf_synthesis"] = run_psf(args.psf_reps)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_pdhg(psf, obs, iters=1)
     if rank == 0:
@@ -795,7 +858,9 @@ def main():
                     help="RL iterations of the batched tiled workload (0: skip it)")
     ap.add_argument("--serve-jobs", type=int, default=16,
                     help="jobs in the served request stream (0: skip the serving measurement)")
-    ap.add_argument("--mode", choices=["full", "conv", "pdhg", "serve", "batch", "mixed"],
+    ap.add_argument("--psf-reps", type=int, default=20,
+                    help="timed pupil_to_psf calls at 128x256x256 (0: skip the PSF synthesis line)")
+    ap.add_argument("--mode", choices=["full", "conv", "pdhg", "serve", "batch", "mixed", "psf"],
                     default="full",
                     help="conv: only warm-up + steps forward/adjoint convolutions of the PDHG "
                          "operator; pdhg: only the timed PDHG iterations (small, fixed launch "
@@ -825,6 +890,12 @@ def main():
 
         torch.cuda.set_device(local)
         print(json.dumps({"mode": "mixed", **run_mixed(D, max(args.mixed_iters, 10))}), flush=True)
+        return
+    if args.mode == "psf":
+        import torch
+
+        torch.cuda.set_device(local)
+        print(json.dumps({"mode": "psf", **run_psf(max(args.psf_reps, 1))}), flush=True)
         return
     if args.mode == "batch":
         import torch

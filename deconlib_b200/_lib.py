@@ -46,6 +46,7 @@ _SIGS = {
     "decon_rl_iteration": (C.c_int, [_p, _p, C.c_float, _p, _p, _p, _p, _p]),
     "decon_rl_predict": (C.c_int, [_p, _p, C.c_float, _p, _p, _p, _p]),
     "decon_rl_run": (C.c_int, [_p, _p, C.c_float, _p, _p, _p, C.c_int, _p]),
+    "decon_pupil_to_psf": (C.c_int, [_p, _p, _p, _i64, _i64, _i64, C.c_int, _p, _p]),
     "decon_batch_rl_create": (C.c_int, [C.c_int, _p, _p, _p, _p, _p, _p, C.c_int, C.POINTER(_p)]),
     "decon_batch_rl_setup": (C.c_int, [_p, _p, _p]),
     "decon_batch_rl_run": (C.c_int, [_p, C.c_int, C.c_int, _p]),

@@ -226,7 +226,7 @@ static ProfState g_prof;
 // to the largest size launched so far (a launch with less shared memory must
 // not lower it under another plan's larger launches).  Later launches,
 // including launches recorded into a CUDA graph, only look the entries up.
-static int kernel_prepare(void* fn, size_t smem, int nthr, int* per_sm) {
+int kernel_prepare(void* fn, size_t smem, int nthr, int* per_sm) {
     static std::mutex mu;
     static std::map<std::tuple<int, void*, size_t, int>, int> done;
     static std::map<std::pair<int, void*>, size_t> opt_in;

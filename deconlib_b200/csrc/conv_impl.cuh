@@ -125,6 +125,10 @@ int quantize_otf(const ConvPlan& p, cudaStream_t st);
 // True when the axial pass of this plan runs the pipelined kernel (conv.cu).
 bool zpass_pipelined(const ConvPlan& p);
 
+// Shared-memory opt-in (only ever raised per device and kernel) and cached
+// occupancy for a launch shape (conv.cu).
+int kernel_prepare(void* fn, size_t smem, int nthr, int* per_sm);
+
 bool tma_length_ok(int L);
 bool encode_spectrum_map(CUtensorMap* map, const float2* base, int64_t pitch, int64_t d1, int64_t d2,
                          int b1, int b2);

@@ -135,6 +135,19 @@ int decon_rl_predict(decon_conv* plan, const float* observed, float background, 
 int decon_rl_run(decon_conv* plan, const float* observed, float background, const float* sens,
                  float* x, float* ratio, int iterations, void* stream);
 
+/* ---- PSF synthesis (psf/widefield.py:18-73 pupil_to_psf) -----------------
+ * psf[z][y][x] = |IFFT2(pupil * exp(2 pi i kz z_z))|^2 for nz planes, on the
+ * device: pupil complex64 [ny][nx] (interleaved floats, DC at the corner),
+ * kz float64 [ny][nx], z float64 [nz], psf float32 [nz][ny][nx] (all device
+ * pointers).  normalize != 0 scales to unit sum (total from Parseval:
+ * nz ny nx sum|pupil|^2, in FP64), else applies numpy's ifft2 factor
+ * 1 / (ny nx)^2.  ny, nx <= 8192 and 7-smooth.  Stream-ordered: the inputs
+ * must stay valid until the work on `stream` completes; complex scratch of at
+ * most 256 MB (or one plane) comes from a library-owned stream-ordered pool.
+ * The first call for an axis length uploads its twiddle table synchronously. */
+int decon_pupil_to_psf(const float* pupil, const double* kz, const double* z, int64_t nz,
+                       int64_t ny, int64_t nx, int normalize, float* psf, void* stream);
+
 /* ---- batched RL: many independent problems in one CUDA graph ------------
  * Problem i has its own plan (distinct plans; a plan's scratch spectra serve
  * one problem), observation, background and x / sens / ratio buffers of its

@@ -7,7 +7,9 @@ Run from the repository root, in the container that holds the reference:
 The reference imports ``mlx.core``; ``tests/golden/mlx_standin`` supplies a
 NumPy stand-in for the names it calls.  The script runs itself twice in
 subprocesses, once in float32 and once with ``DECON_STANDIN_FP64=1``, and
-writes ``tests/golden/golden_fp32.npz`` and ``golden_fp64.npz``.  The
+writes ``tests/golden/golden_fp32.npz`` and ``golden_fp64.npz``; a third
+subprocess runs the reference's NumPy ``pupil_to_psf`` into
+``golden_psf.npz``.  The
 fixtures are small (volumes of at most 16x32x32) so the CPU oracle replays
 them in seconds.  Nothing on the GPU side reads the reference at run time;
 the fixtures are what travels.
@@ -302,15 +304,58 @@ def _run(out_path):
     print(f"wrote {out_path}: {len(g)} arrays")
 
 
+def _run_psf(out_path):
+    """pupil_to_psf cases: inputs (pupil, kz, z), the normalize flag and the
+    reference's PSF.  pupil_to_psf is plain NumPy; the stand-in is on the path
+    only because the package's imports name ``mlx.core``."""
+    from deconlib.psf import Optics, make_geometry, make_pupil, pupil_to_psf
+    from deconlib.psf.aberrations import (IndexMismatch, ZernikeAberration, ZernikeMode,
+                                         apply_aberrations)
+    from deconlib.utils import fft_coords
+
+    cases = [  # (nz, ny, nx), dz, dxy, apodize, aberrated, normalize
+        ((16, 64, 64), 0.1, 0.085, False, False, True),
+        ((7, 36, 50), 0.2, 0.1, False, True, False),
+        ((6, 120, 256), 0.15, 0.065, True, True, True),
+        ((1, 48, 63), 0.1, 0.09, True, False, True),
+    ]
+    g = {}
+    for i, (shape, dz, dxy, apod, aberr, norm) in enumerate(cases):
+        optics = Optics(wavelength=0.525, na=1.4, ni=1.515, ns=1.334)
+        geom = make_geometry(shape[1:], dxy, optics)
+        pupil = make_pupil(geom, apodize=apod)
+        if aberr:
+            pupil = apply_aberrations(
+                pupil, geom, optics,
+                [IndexMismatch(depth=6.0),
+                 ZernikeAberration({ZernikeMode.SPHERICAL: 0.4, ZernikeMode.COMA_X: 0.3})])
+        z = fft_coords(shape[0], dz)
+        psf = pupil_to_psf(pupil, geom, z, normalize=norm)
+        g[f"psf{i}_pupil"] = np.asarray(pupil, np.complex128)
+        g[f"psf{i}_kz"] = np.asarray(geom.kz, np.float64)
+        g[f"psf{i}_z"] = np.asarray(z, np.float64)
+        g[f"psf{i}_normalize"] = np.array(bool(norm))
+        g[f"psf{i}_psf"] = np.asarray(psf, np.float32)
+    g["psf_cases"] = np.array(len(cases))
+    np.savez_compressed(out_path, **g)
+    print(f"wrote {out_path}: {len(g)} arrays")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--worker", choices=["fp32", "fp64"], default=None)
+    ap.add_argument("--worker", choices=["fp32", "fp64", "psf"], default=None)
     a = ap.parse_args()
+    if a.worker == "psf":
+        sys.path[:0] = [STANDIN, a.reference]
+        _run_psf(os.path.join(HERE, "golden_psf.npz"))
+        return
     if a.worker:
         sys.path[:0] = [STANDIN, a.reference]
         _run(os.path.join(HERE, f"golden_{a.worker}.npz"))
         return
+    subprocess.run([sys.executable, os.path.abspath(__file__), "--reference", a.reference,
+                    "--worker", "psf"], check=True)
     for mode in ("fp32", "fp64"):
         env = dict(os.environ)
         env["DECON_STANDIN_FP64"] = "1" if mode == "fp64" else "0"

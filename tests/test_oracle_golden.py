@@ -187,3 +187,16 @@ def test_pdhg_convergence_bin_plain_operator(gold):
     np.testing.assert_allclose(r["sigma_history"], g["pdo_sigma"], rtol=tol(dt, 1e-4, 1e-9))
     np.testing.assert_allclose(r["loss_history"], g["pdo_loss"], rtol=tol(dt, 1e-4, 1e-9))
     assert len(seen) == 15
+
+
+def test_pupil_to_psf():
+    """oracle/psf.py against the reference's pupil_to_psf on four pupils
+    (plain, aberrated, apodised; 7-smooth and power-of-two planes; with and
+    without normalisation).  Fixtures are float32: agreement to ~3e-8."""
+    from oracle import psf as P
+
+    g = np.load(os.path.join(HERE, "golden", "golden_psf.npz"))
+    for i in range(int(g["psf_cases"])):
+        r = P.pupil_to_psf(g[f"psf{i}_pupil"], g[f"psf{i}_kz"], g[f"psf{i}_z"],
+                           bool(g[f"psf{i}_normalize"]))
+        assert rel(r, g[f"psf{i}_psf"]) < 1e-7, i
