@@ -519,6 +519,44 @@ def run_psf(reps=20, shape=(128, 256, 256), dxy=0.0425, dz=0.05):
             "rel_l2_vs_fp64_planes01": err}
 
 
+def run_nlcg(D, iters=50):
+    """Nonlinear CG (nlcg_with_operator) on the RL workload (128x256x256,
+    LinearFFTConvolver, background 10), unregularised and with a Hessian
+    smoothness prior (beta 1e-4), stopping rules off so every solve runs its
+    iterations.  The steady-state time per iteration is the difference of a
+    10-iteration and an ``iters``-iteration solve (CUDA events around each
+    whole solve, its one host read per iteration included)."""
+    import torch
+
+    psf, obs = rl_inputs(D)
+    lib = __import__("deconlib_b200._lib", fromlist=["load"]).load()
+    n = int(np.prod(OBJ))
+    out = {"workload": "rl_object128x256x256_beads_shells", "convolutions_per_iter": 3}
+    op = D.LinearFFTConvolver(psf, OBJ)
+    for tag, reg, beta in (("plain", None, 0.0), ("hessian", D.Hessian3D(), 1e-4)):
+        def solve(k):
+            return D.nlcg_with_operator(obs, op, num_iter=k, background=10.0, regularizer=reg,
+                                        reg_weight=beta, slack=0.0, tol=0.0, min_iter=10 ** 9)
+
+        solve(3)
+        times, launches = {}, {}
+        for k in (10, iters):
+            torch.cuda.synchronize()
+            n0 = lib.decon_launch_count()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = solve(k)
+            e1.record()
+            e1.synchronize()
+            times[k] = e0.elapsed_time(e1)
+            launches[k] = lib.decon_launch_count() - n0
+        ms = (times[iters] - times[10]) / (iters - 10)
+        out[tag] = {"ms_per_iter": ms, "voxel_iter_per_s": n / (ms / 1e3),
+                    "launches_per_iter": (launches[iters] - launches[10]) / (iters - 10),
+                    "iterations": res.iterations, "final_loss": res.loss_history[-1]}
+    return out
+
+
 def zpass_bytes(n_shape, f_shape):
     nz = n_shape[0]
     fz, fy, fx = f_shape
@@ -706,6 +744,8 @@ def run_ours(args, ws, rank, local):
         line["mixed"] = run_mixed(D, args.mixed_iters)
     if args.psf_reps > 0:
         line["psf_synthesis"] = run_psf(args.psf_reps)
+    if args.nlcg_iters > 0:
+        line["nlcg"] = run_nlcg(D, args.nlcg_iters)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_pdhg(psf, obs, iters=1)
     if rank == 0:
@@ -860,7 +900,10 @@ def main():
                     help="jobs in the served request stream (0: skip the serving measurement)")
     ap.add_argument("--psf-reps", type=int, default=20,
                     help="timed pupil_to_psf calls at 128x256x256 (0: skip the PSF synthesis line)")
-    ap.add_argument("--mode", choices=["full", "conv", "pdhg", "serve", "batch", "mixed", "psf"],
+    ap.add_argument("--nlcg-iters", type=int, default=50,
+                    help="NLCG iterations per timed solve at 128x256x256 (0: skip the NLCG line)")
+    ap.add_argument("--mode", choices=["full", "conv", "pdhg", "serve", "batch", "mixed", "psf",
+                                       "nlcg"],
                     default="full",
                     help="conv: only warm-up + steps forward/adjoint convolutions of the PDHG "
                          "operator; pdhg: only the timed PDHG iterations (small, fixed launch "
@@ -890,6 +933,14 @@ def main():
 
         torch.cuda.set_device(local)
         print(json.dumps({"mode": "mixed", **run_mixed(D, max(args.mixed_iters, 10))}), flush=True)
+        return
+    if args.mode == "nlcg":
+        import torch
+
+        import deconlib_b200.deconvolution as D
+
+        torch.cuda.set_device(local)
+        print(json.dumps({"mode": "nlcg", **run_nlcg(D, max(args.nlcg_iters, 11))}), flush=True)
         return
     if args.mode == "psf":
         import torch

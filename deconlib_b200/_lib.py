@@ -47,6 +47,20 @@ _SIGS = {
     "decon_rl_predict": (C.c_int, [_p, _p, C.c_float, _p, _p, _p, _p]),
     "decon_rl_run": (C.c_int, [_p, _p, C.c_float, _p, _p, _p, C.c_int, _p]),
     "decon_pupil_to_psf": (C.c_int, [_p, _p, _p, _i64, _i64, _i64, C.c_int, _p, _p]),
+    "decon_nlcg_create": (C.c_int, [_p]),
+    "decon_nlcg_destroy": (C.c_int, [_p]),
+    "decon_nlcg_init": (C.c_int, [_p, _p, _p, _i64, C.c_int, _p]),
+    "decon_nlcg_model": (C.c_int, [_p, _p, _p, C.c_float, _p, _i64, _p]),
+    "decon_nlcg_products": (C.c_int, [_p, C.c_int, C.c_float, _p, _p, _p, _p, _p, _p, _i64, _p]),
+    "decon_nlcg_gram": (C.c_int, [_p, _p, _p, _p, _i64, _p]),
+    "decon_nlcg_newton": (C.c_int, [_p, _p, _p, _p, _p, C.c_float, C.c_float, C.c_double, C.c_int,
+                                    C.c_int, _i64, _p]),
+    "decon_nlcg_accept": (C.c_int, [_p, _p, _p, _p, _p, C.c_float, C.c_float, _p, _p, _i64, _p, _p, _p,
+                                    _p, _i64, _p]),
+    "decon_nlcg_energy": (C.c_int, [_p, _p, _i64, _p]),
+    "decon_nlcg_gradient": (C.c_int, [_p, _p, _p, _p, _p, _p, C.c_float, C.c_float, _p, _i64, _p]),
+    "decon_nlcg_quad": (C.c_int, [_p, _p, _p, _p, _i64, _p, _p, _i64, C.c_float, _p]),
+    "decon_nlcg_read": (C.c_int, [_p, _p, _p]),
     "decon_batch_rl_create": (C.c_int, [C.c_int, _p, _p, _p, _p, _p, _p, C.c_int, C.POINTER(_p)]),
     "decon_batch_rl_setup": (C.c_int, [_p, _p, _p]),
     "decon_batch_rl_run": (C.c_int, [_p, C.c_int, C.c_int, _p]),

@@ -1,0 +1,452 @@
+// Nonlinear conjugate gradients for Poisson maximum likelihood, f = s^2
+// (deconlib's nlcg_mlx.py: Schaefer, Schuster & Herz 2001 objective,
+// Fletcher-Reeves directions, exact Newton-Raphson step length).
+//
+// The convolutions and the regulariser run through the operators the caller
+// passes; this file holds every other pass of an iteration, each one fused
+// elementwise kernel with its FP64 sums:
+//
+//   k_nlcg_products   d <- r + gamma d (or d as given), s d, d^2
+//   k_nlcg_gram       six inner products of C f, C(s d), C(d^2)
+//   k_nlcg_newton     one Newton-Raphson refinement of the step length: the
+//                     data sums of phi'(lam), phi''(lam); the last CTA adds
+//                     the regulariser's terms (polynomials in lam of the Gram
+//                     entries) and updates lam on the device
+//   k_nlcg_accept_d   model m(lam) = Kss + 2 lam K(sd) + lam^2 K(dd) + b, the
+//                     gradient weight 1 - g / m, objective and I-divergence sums
+//   k_nlcg_accept_o   s + lam d and its square
+//   k_nlcg_gradient   r = -(2 s K^T w + 4 beta s C^T C f), |r|^2, the
+//                     I-divergence between successive f and sum f
+//
+// Every reduction is deterministic: each CTA writes its FP64 partials, and
+// the last CTA to finish (a ticket counter, no waiting) folds them in block
+// order.  The Newton loop runs on the device (lam never leaves HBM), so an
+// iteration needs one host read, after the speculative gradient.
+#include <cfloat>
+
+#include "conv_impl.cuh"
+
+namespace dk {
+
+constexpr int kNlThreads = 256;
+constexpr int kNlMaxBlocks = 1184;  // 148 SMs x 8
+constexpr int kNlSlots = 6;
+
+struct NlcgDev {
+    double lam;
+    int done;        // Newton stopped: degenerate curvature or non-finite step
+    int newton_run;  // refinements performed
+    double gram[6];  // <A,A> <A,B> <A,C> <B,B> <B,C> <C,C> for A = Cf, B = C(sd), C = C(dd)
+    double data[3];  // sum m, sum g ln max(m, eps), sum of Poisson I-divergence terms
+    double reg[1];   // sum (C f)^2
+    double obj[3];   // sum r^2, I-divergence(f_prev, f), sum f
+    double quad[2];  // helper sums
+    double nt[3];    // Newton data sums (last refinement)
+    unsigned ticket;
+};
+
+__device__ __forceinline__ int64_t gstride() { return (int64_t)gridDim.x * blockDim.x; }
+__device__ __forceinline__ int64_t gtid() { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
+
+// Block sums of v[0..NS) into partials; the last CTA folds them (block order,
+// FP64) into out[0..NS) and re-arms the ticket.  Returns true in the last CTA.
+template <int NS>
+__device__ bool fold_last(double (&v)[NS], double* __restrict__ part, unsigned* ticket,
+                          double* out) {
+    __shared__ bool last;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const double t = block_sum(v[s]);
+        if (threadIdx.x == 0) part[s * gridDim.x + blockIdx.x] = t;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int s = warp; s < NS; s += blockDim.x >> 5) {
+        double acc = 0.0;
+        for (int b = lane; b < (int)gridDim.x; b += 32) acc += __ldcg(&part[s * gridDim.x + b]);
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) out[s] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *ticket = 0;
+    return true;
+}
+
+// f0 = max(x, 1e-6), s = sqrt(f0), f = s s; or (from_s) f = s s alone.
+__global__ void k_nlcg_init(const float* __restrict__ x, float* __restrict__ s, float* __restrict__ f,
+                            int64_t n, int from_s) {
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        float sv;
+        if (from_s) {
+            sv = x[i];
+        } else {
+            sv = sqrtf(fmaxf(x[i], 1e-6f));
+            s[i] = sv;
+        }
+        f[i] = sv * sv;
+    }
+}
+
+// Data-space terms of a model m: w = 1 - g / max(m, eps); sums of m,
+// g ln max(m, eps) and the Poisson I-divergence (rl_mlx.py:58-80, eps 1e-6).
+__device__ __forceinline__ void model_terms(float m, float g, float eps, float& w, double (&v)[3]) {
+    const float mm = fmaxf(m, eps);
+    w = 1.0f - g / mm;
+    v[0] += (double)m;
+    v[1] += (double)(g * logf(mm));
+    const float gs = fmaxf(g, 1e-6f), ms = fmaxf(m, 1e-6f);
+    v[2] += (double)(g * logf(gs / ms) - (g - ms));
+}
+
+__global__ void k_nlcg_model(const float* __restrict__ m, const float* __restrict__ g, float eps,
+                             float* __restrict__ w, int64_t n, double* part, NlcgDev* dev) {
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        float wi;
+        model_terms(m[i], g[i], eps, wi, v);
+        if (w) w[i] = wi;
+    }
+    fold_last<3>(v, part, &dev->ticket, dev->data);
+}
+
+// mode 0: direction d as given; mode 1: d_out = r + gamma d.  sd = s d, dd = d d.
+// Arms the Newton state (lam = 0).
+__global__ void k_nlcg_products(int mode, float gamma, const float* __restrict__ s,
+                                const float* __restrict__ d, const float* __restrict__ r,
+                                float* __restrict__ d_out, float* __restrict__ sd,
+                                float* __restrict__ dd, int64_t n, NlcgDev* dev) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        dev->lam = 0.0;
+        dev->done = 0;
+        dev->newton_run = 0;
+    }
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        float dv = d[i];
+        if (mode == 1) {
+            dv = r[i] + gamma * dv;
+            d_out[i] = dv;
+        }
+        sd[i] = s[i] * dv;
+        dd[i] = dv * dv;
+    }
+}
+
+__global__ void k_nlcg_gram(const float* __restrict__ a, const float* __restrict__ b,
+                            const float* __restrict__ c, int64_t n, double* part, NlcgDev* dev) {
+    double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        const double x = a[i], y = b[i], z = c[i];
+        v[0] += x * x;
+        v[1] += x * y;
+        v[2] += x * z;
+        v[3] += y * y;
+        v[4] += y * z;
+        v[5] += z * z;
+    }
+    fold_last<6>(v, part, &dev->ticket, dev->gram);
+}
+
+// One refinement (nlcg_mlx.py:262-291): data sums at the current lam, then
+// lam <- lam - phi' / phi'' in the last CTA.
+__global__ void k_nlcg_newton(const float* __restrict__ m, const float* __restrict__ ksd,
+                              const float* __restrict__ kdd, const float* __restrict__ g, float b,
+                              float eps, double beta, int use_reg, int64_t n, double* part,
+                              NlcgDev* dev) {
+    if (dev->done) return;  // every CTA reads the same flag: all return or none
+    const double lam = dev->lam;
+    const float c1 = (float)(2.0 * lam), c2 = (float)(lam * lam), lf = (float)lam;
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        const float kss = m[i] - b, sdv = ksd[i], ddv = kdd[i], gv = g[i];
+        const float ml = fmaxf(kss + c1 * sdv + c2 * ddv + b, eps);
+        const float sl = sdv + lf * ddv;
+        const float wl = 1.0f - gv / ml;
+        v[0] += (double)(sl * wl);
+        v[1] += (double)(ddv * wl);
+        v[2] += (double)(gv * (sl * sl) / (ml * ml));
+    }
+    if (!fold_last<3>(v, part, &dev->ticket, dev->nt)) return;
+    if (threadIdx.x != 0) return;
+    double d1 = 2.0 * dev->nt[0];
+    double d2 = 2.0 * dev->nt[1] + 4.0 * dev->nt[2];
+    if (use_reg) {
+        // u = A + 2 lam B + lam^2 C, B_lam = B + lam C (regulariser images of
+        // f(lam) and of its lam-derivative / 2): the sums are polynomials in lam.
+        const double* G = dev->gram;  // AA AB AC BB BC CC
+        const double l = lam, l2 = lam * lam, l3 = l2 * lam;
+        const double u_b = G[1] + l * (G[2] + 2.0 * G[3]) + 3.0 * l2 * G[4] + l3 * G[5];
+        const double b_b = G[3] + 2.0 * l * G[4] + l2 * G[5];
+        const double u_c = G[2] + 2.0 * l * G[4] + l2 * G[5];
+        d1 += 4.0 * beta * u_b;
+        d2 += 8.0 * beta * b_b + 4.0 * beta * u_c;
+    }
+    dev->newton_run += 1;
+    if (!isfinite(d2) || fabs(d2) < (double)eps) {
+        dev->done = 1;
+        return;
+    }
+    const double next = lam - d1 / d2;
+    dev->lam = next;
+    if (!isfinite(next)) dev->done = 1;
+}
+
+// The trial point's model and its data terms (nlcg_mlx.py:297-298, 96-111).
+__global__ void k_nlcg_accept_d(const float* __restrict__ m, const float* __restrict__ ksd,
+                                const float* __restrict__ kdd, const float* __restrict__ g, float b,
+                                float eps, float* __restrict__ m_new, float* __restrict__ w_new,
+                                int64_t n, double* part, NlcgDev* dev) {
+    const double lam = dev->lam;
+    const float c1 = (float)(2.0 * lam), c2 = (float)(lam * lam);
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        const float kss = m[i] - b;
+        const float mn = kss + c1 * ksd[i] + c2 * kdd[i] + b;
+        m_new[i] = mn;
+        float wi;
+        model_terms(mn, g[i], eps, wi, v);
+        if (w_new) w_new[i] = wi;
+    }
+    fold_last<3>(v, part, &dev->ticket, dev->data);
+}
+
+__global__ void k_nlcg_accept_o(const float* __restrict__ s, const float* __restrict__ d,
+                                float* __restrict__ s_new, float* __restrict__ f_new, int64_t n,
+                                const NlcgDev* dev) {
+    const float lf = (float)dev->lam;
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        const float sn = s[i] + lf * d[i];
+        s_new[i] = sn;
+        f_new[i] = sn * sn;
+    }
+}
+
+__global__ void k_nlcg_energy(const float* __restrict__ a, int64_t n, double* part, NlcgDev* dev) {
+    double v[1] = {0.0};
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        const double x = a[i];
+        v[0] += x * x;
+    }
+    fold_last<1>(v, part, &dev->ticket, dev->reg);
+}
+
+// r = -(2 s K^T w [+ 4 beta s C^T C f]) (nlcg_mlx.py:105-115), sum r^2 (skipped
+// without ktw); with f_prev: the I-divergence of f against f_prev
+// (nlcg_mlx.py:303-323); sum f.
+__global__ void k_nlcg_gradient(const float* __restrict__ s, const float* __restrict__ f,
+                                const float* __restrict__ f_prev, const float* __restrict__ ktw,
+                                const float* __restrict__ ctcf, float c4b, float eps,
+                                float* __restrict__ r, int64_t n, double* part, NlcgDev* dev) {
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        if (ktw) {
+            const float sv = s[i];
+            float grad = (2.0f * sv) * ktw[i];
+            if (ctcf) grad = grad + (c4b * sv) * ctcf[i];
+            const float rv = -grad;
+            r[i] = rv;
+            v[0] += (double)rv * (double)rv;
+        }
+        const float fc = f[i];
+        if (f_prev) {
+            const float fp = f_prev[i];
+            v[1] += (double)(fp * (logf(fmaxf(fp, eps)) - logf(fmaxf(fc, eps))) - fp + fc);
+        }
+        v[2] += (double)fc;
+    }
+    fold_last<3>(v, part, &dev->ticket, dev->obj);
+}
+
+// Quadratic-form helper sums (nlcg_mlx.py:181-193):
+// quad[0] = sum (g / max(m m, eps)) K(sd)^2, quad[1] = sum a d^2.
+__global__ void k_nlcg_quad(const float* __restrict__ g, const float* __restrict__ m,
+                            const float* __restrict__ ksd, int64_t nd, const float* __restrict__ a,
+                            const float* __restrict__ d, int64_t no, float eps, double* part,
+                            NlcgDev* dev) {
+    double v[2] = {0.0, 0.0};
+    for (int64_t i = gtid(); i < nd; i += gstride()) {
+        const float mv = m[i], kv = ksd[i];
+        v[0] += (double)((g[i] / fmaxf(mv * mv, eps)) * (kv * kv));
+    }
+    for (int64_t i = gtid(); i < no; i += gstride()) {
+        const float dv = d[i];
+        v[1] += (double)(a[i] * (dv * dv));
+    }
+    fold_last<2>(v, part, &dev->ticket, dev->quad);
+}
+
+static int nl_blocks(int64_t n) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>(kNlMaxBlocks, cdiv(n, (int64_t)kNlThreads * 4)));
+}
+
+}  // namespace dk
+
+using namespace dk;
+
+struct decon_nlcg {
+    NlcgDev* dev = nullptr;
+    double* part = nullptr;
+    NlcgDev* host = nullptr;  // pinned mirror for decon_nlcg_read
+};
+
+static int nl_free(decon_nlcg* h) {
+    if (!h) return DECON_OK;
+    cudaFree(h->dev);
+    cudaFree(h->part);
+    cudaFreeHost(h->host);
+    delete h;
+    return DECON_OK;
+}
+
+extern "C" {
+
+int decon_nlcg_create(decon_nlcg** out) {
+    if (!out) return fail(DECON_ERR_NULL, "null pointer");
+    *out = nullptr;
+    decon_nlcg* h = new decon_nlcg();
+    if (cudaMalloc(&h->dev, sizeof(NlcgDev)) != cudaSuccess ||
+        cudaMalloc(&h->part, sizeof(double) * kNlSlots * kNlMaxBlocks) != cudaSuccess ||
+        cudaMallocHost(&h->host, sizeof(NlcgDev)) != cudaSuccess) {
+        cudaGetLastError();
+        nl_free(h);
+        return fail(DECON_ERR_OOM, "decon_nlcg_create: allocation failed");
+    }
+    if (cudaMemset(h->dev, 0, sizeof(NlcgDev)) != cudaSuccess) {
+        nl_free(h);
+        return fail(DECON_ERR_CUDA, "decon_nlcg_create: memset failed");
+    }
+    *out = h;
+    return DECON_OK;
+}
+
+int decon_nlcg_destroy(decon_nlcg* h) { return nl_free(h); }
+
+int decon_nlcg_init(const float* x, float* s, float* f, int64_t n, int from_s, void* stream) {
+    if (!x || !f || (!from_s && !s)) return fail(DECON_ERR_NULL, "null pointer");
+    if (n <= 0) return DECON_OK;
+    k_nlcg_init<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(x, s, f, n, from_s);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_nlcg_model(decon_nlcg* h, const float* m, const float* g, float eps, float* w, int64_t n,
+                     void* stream) {
+    if (!h || !m || !g) return fail(DECON_ERR_NULL, "null pointer");
+    if (n <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_model: empty data");
+    k_nlcg_model<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(m, g, eps, w, n, h->part, h->dev);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_nlcg_products(decon_nlcg* h, int mode, float gamma, const float* s, const float* d,
+                        const float* r, float* d_out, float* sd, float* dd, int64_t n, void* stream) {
+    if (!h || !s || !d || !sd || !dd || (mode == 1 && (!r || !d_out)))
+        return fail(DECON_ERR_NULL, "null pointer");
+    if (mode != 0 && mode != 1) return fail(DECON_ERR_VALUE, "decon_nlcg_products: mode must be 0 or 1");
+    if (n <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_products: empty object");
+    k_nlcg_products<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(mode, gamma, s, d, r, d_out, sd,
+                                                                        dd, n, h->dev);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_nlcg_gram(decon_nlcg* h, const float* a, const float* b, const float* c, int64_t n,
+                    void* stream) {
+    if (!h || !a || !b || !c) return fail(DECON_ERR_NULL, "null pointer");
+    if (n <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_gram: empty");
+    k_nlcg_gram<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(a, b, c, n, h->part, h->dev);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_nlcg_newton(decon_nlcg* h, const float* m, const float* ksd, const float* kdd, const float* g,
+                      float background, float eps, double beta, int use_reg, int newton_iters,
+                      int64_t n, void* stream) {
+    if (!h || !m || !ksd || !kdd || !g) return fail(DECON_ERR_NULL, "null pointer");
+    if (n <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_newton: empty data");
+    const cudaStream_t st = as_stream(stream);
+    for (int it = 0; it < newton_iters; ++it) {
+        k_nlcg_newton<<<nl_blocks(n), kNlThreads, 0, st>>>(m, ksd, kdd, g, background, eps, beta, use_reg,
+                                                          n, h->part, h->dev);
+        DK_LAUNCHED();
+    }
+    return DECON_OK;
+}
+
+int decon_nlcg_accept(decon_nlcg* h, const float* m, const float* ksd, const float* kdd, const float* g,
+                      float background, float eps, float* m_new, float* w_new, int64_t nd,
+                      const float* s, const float* d, float* s_new, float* f_new, int64_t no,
+                      void* stream) {
+    if (!h || !m || !ksd || !kdd || !g || !m_new) return fail(DECON_ERR_NULL, "null pointer");
+    if (nd <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_accept: empty data");
+    const cudaStream_t st = as_stream(stream);
+    k_nlcg_accept_d<<<nl_blocks(nd), kNlThreads, 0, st>>>(m, ksd, kdd, g, background, eps, m_new, w_new,
+                                                         nd, h->part, h->dev);
+    DK_LAUNCHED();
+    if (s) {
+        if (!d || !s_new || !f_new) return fail(DECON_ERR_NULL, "null pointer");
+        k_nlcg_accept_o<<<nl_blocks(no), kNlThreads, 0, st>>>(s, d, s_new, f_new, no, h->dev);
+        DK_LAUNCHED();
+    }
+    return DECON_OK;
+}
+
+int decon_nlcg_energy(decon_nlcg* h, const float* a, int64_t n, void* stream) {
+    if (!h || !a) return fail(DECON_ERR_NULL, "null pointer");
+    if (n <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_energy: empty");
+    k_nlcg_energy<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(a, n, h->part, h->dev);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_nlcg_gradient(decon_nlcg* h, const float* s, const float* f, const float* f_prev,
+                        const float* ktw, const float* ctcf, float c4b, float eps, float* r, int64_t n,
+                        void* stream) {
+    if (!h || !f || (ktw && (!s || !r))) return fail(DECON_ERR_NULL, "null pointer");
+    if (n <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_gradient: empty object");
+    k_nlcg_gradient<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(s, f, f_prev, ktw, ctcf, c4b, eps,
+                                                                       r, n, h->part, h->dev);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_nlcg_quad(decon_nlcg* h, const float* g, const float* m, const float* ksd, int64_t nd,
+                    const float* a, const float* d, int64_t no, float eps, void* stream) {
+    if (!h || !g || !m || !ksd || !a || !d) return fail(DECON_ERR_NULL, "null pointer");
+    if (nd <= 0 || no <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_quad: empty");
+    const int64_t big = std::max(nd, no);
+    k_nlcg_quad<<<nl_blocks(big), kNlThreads, 0, as_stream(stream)>>>(g, m, ksd, nd, a, d, no, eps,
+                                                                     h->part, h->dev);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+// Synchronises `stream` and returns the scalars: out[0] lam, [1] Newton
+// stopped (0/1), [2] refinements run, [3..5] data sums (sum m,
+// sum g ln max(m, eps), sum I-divergence terms), [6] regulariser energy,
+// [7..9] sum r^2, I-divergence between iterates, sum f, [10..11] quadratic-form
+// sums, [12..17] Gram entries.
+int decon_nlcg_read(decon_nlcg* h, double* out, void* stream) {
+    if (!h || !out) return fail(DECON_ERR_NULL, "null pointer");
+    const cudaStream_t st = as_stream(stream);
+    DK_CUDA(cudaMemcpyAsync(h->host, h->dev, sizeof(NlcgDev), cudaMemcpyDeviceToHost, st));
+    DK_CUDA(cudaStreamSynchronize(st));
+    const NlcgDev& v = *h->host;
+    out[0] = v.lam;
+    out[1] = v.done;
+    out[2] = v.newton_run;
+    for (int i = 0; i < 3; ++i) out[3 + i] = v.data[i];
+    out[6] = v.reg[0];
+    for (int i = 0; i < 3; ++i) out[7 + i] = v.obj[i];
+    out[10] = v.quad[0];
+    out[11] = v.quad[1];
+    for (int i = 0; i < 6; ++i) out[12 + i] = v.gram[i];
+    return DECON_OK;
+}
+
+}  // extern "C"

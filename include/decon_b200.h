@@ -135,6 +135,56 @@ int decon_rl_predict(decon_conv* plan, const float* observed, float background, 
 int decon_rl_run(decon_conv* plan, const float* observed, float background, const float* sens,
                  float* x, float* ratio, int iterations, void* stream);
 
+/* ---- nonlinear conjugate gradients (deconvolution/nlcg_mlx.py:326-545) ----
+ * The passes of nlcg_with_operator other than the caller's operators (the
+ * convolutions and the regulariser): each is one fused elementwise kernel
+ * with deterministic FP64 sums kept in the handle's device scalars.  The
+ * Newton-Raphson step length (nlcg_step_length, :197-300) runs on the device
+ * (decon_nlcg_newton); decon_nlcg_read is the one synchronising call.  All
+ * arrays are device float32; "data" arrays have the observation's size nd,
+ * "object" arrays the reconstruction's size no.  eps is the reference's 1e-10. */
+typedef struct decon_nlcg decon_nlcg;
+int decon_nlcg_create(decon_nlcg** out);
+int decon_nlcg_destroy(decon_nlcg* h);
+/* s = sqrt(max(x, 1e-6)), f = s^2 (:431-439); from_s != 0: f = x^2 only. */
+int decon_nlcg_init(const float* x, float* s, float* f, int64_t n, int from_s, void* stream);
+/* w = 1 - g / max(m, eps) (w may be NULL) and the data sums of model m. */
+int decon_nlcg_model(decon_nlcg* h, const float* m, const float* g, float eps, float* w, int64_t n,
+                     void* stream);
+/* mode 0: direction d; mode 1: d_out = r + gamma d (:517).  sd = s d, dd = d^2.
+ * Resets the device step length to 0. */
+int decon_nlcg_products(decon_nlcg* h, int mode, float gamma, const float* s, const float* d,
+                        const float* r, float* d_out, float* sd, float* dd, int64_t n, void* stream);
+/* Gram matrix of the regulariser images C f, C(s d), C(d^2) (n values each). */
+int decon_nlcg_gram(decon_nlcg* h, const float* a, const float* b, const float* c, int64_t n,
+                    void* stream);
+/* newton_iters refinements of the step length (:262-291); the regulariser
+ * terms come from the Gram entries when use_reg != 0. */
+int decon_nlcg_newton(decon_nlcg* h, const float* m, const float* ksd, const float* kdd, const float* g,
+                      float background, float eps, double beta, int use_reg, int newton_iters,
+                      int64_t n, void* stream);
+/* m_new = (m - b) + 2 lam K(sd) + lam^2 K(dd) + b (:297), w_new and the data
+ * sums; with s != NULL also s_new = s + lam d, f_new = s_new^2 (:398-399). */
+int decon_nlcg_accept(decon_nlcg* h, const float* m, const float* ksd, const float* kdd, const float* g,
+                      float background, float eps, float* m_new, float* w_new, int64_t nd,
+                      const float* s, const float* d, float* s_new, float* f_new, int64_t no,
+                      void* stream);
+/* sum a^2 (the regulariser energy ||C f||^2). */
+int decon_nlcg_energy(decon_nlcg* h, const float* a, int64_t n, void* stream);
+/* r = -(2 s ktw + c4b s ctcf) (ctcf may be NULL; c4b = 4 beta) and sum r^2
+ * (ktw NULL: no gradient), sum f and, with f_prev, the I-divergence between
+ * f_prev and f (:303-323). */
+int decon_nlcg_gradient(decon_nlcg* h, const float* s, const float* f, const float* f_prev,
+                        const float* ktw, const float* ctcf, float c4b, float eps, float* r, int64_t n,
+                        void* stream);
+/* sum (g / max(m^2, eps)) ksd^2 and sum a d^2 (nlcg_hessian_quadform, :181-193). */
+int decon_nlcg_quad(decon_nlcg* h, const float* g, const float* m, const float* ksd, int64_t nd,
+                    const float* a, const float* d, int64_t no, float eps, void* stream);
+/* Synchronise and read the 18 scalars: lam, Newton stopped, refinements run,
+ * data sums [3], regulariser energy, sum r^2, I-divergence, sum f, quadratic
+ * sums [2], Gram entries [6]. */
+int decon_nlcg_read(decon_nlcg* h, double* out, void* stream);
+
 /* ---- PSF synthesis (psf/widefield.py:18-73 pupil_to_psf) -----------------
  * psf[z][y][x] = |IFFT2(pupil * exp(2 pi i kz z_z))|^2 for nz planes, on the
  * device: pupil complex64 [ny][nx] (interleaved floats, DC at the corner),

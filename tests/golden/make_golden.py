@@ -9,7 +9,8 @@ NumPy stand-in for the names it calls.  The script runs itself twice in
 subprocesses, once in float32 and once with ``DECON_STANDIN_FP64=1``, and
 writes ``tests/golden/golden_fp32.npz`` and ``golden_fp64.npz``; a third
 subprocess runs the reference's NumPy ``pupil_to_psf`` into
-``golden_psf.npz``.  The
+``golden_psf.npz``.  The NLCG fixtures go to ``golden_nlcg_fp32.npz`` and
+``golden_nlcg_fp64.npz``.  The
 fixtures are small (volumes of at most 16x32x32) so the CPU oracle replays
 them in seconds.  Nothing on the GPU side reads the reference at run time;
 the fixtures are what travels.
@@ -341,14 +342,99 @@ def _run_psf(out_path):
     print(f"wrote {out_path}: {len(g)} arrays")
 
 
+def _run_nlcg(out_path):
+    """Nonlinear CG (nlcg_mlx.py): full solves on plain, regularised and
+    composed operators, and the helper functions at a fixed point."""
+    import mlx.core as mx
+    from deconlib.deconvolution import (
+        Crop, FractionalAreaDownsample, Gradient3D, Hessian3D, LinearFFTConvolver, compose,
+    )
+    from deconlib.deconvolution.nlcg_mlx import (
+        i_divergence_between, nlcg_gradient, nlcg_hessian_quadform, nlcg_objective,
+        nlcg_step_length, nlcg_with_operator,
+    )
+
+    g = {}
+    shape = (16, 32, 32)
+    psf = _psf(shape, 0.1, 0.085)
+    g["psf"] = psf
+    truth = _beads(shape, 40, seed=5)
+    blur = np.asarray(np.array(LinearFFTConvolver(psf, shape).forward(mx.array(truth))), np.float64)
+    obs = np.random.default_rng(6).poisson(blur / blur.max() * 500.0 + 10.0).astype(np.float32)
+    g["obs"] = obs
+
+    def rec(name, res):
+        g[name + "_x"] = np.array(res.restored)
+        g[name + "_pred"] = np.array(res.pred)
+        g[name + "_loss"] = np.array(res.loss_history)
+        g[name + "_iters"] = np.array(res.iterations)
+        g[name + "_converged"] = np.array(res.converged)
+
+    op = LinearFFTConvolver(psf, shape)
+    rec("plain", nlcg_with_operator(obs, op, num_iter=15, background=10.0, eval_interval=4,
+                                    min_iter=100))
+    # discrepancy-principle stop (a loose slack makes it trigger early)
+    rec("stop", nlcg_with_operator(obs, op, num_iter=40, background=10.0, slack=6.0, min_iter=3))
+    rec("hess", nlcg_with_operator(obs, op, num_iter=12, background=10.0, regularizer=Hessian3D(),
+                                   reg_weight=1e-3, tol=1e-4, min_iter=5, eval_interval=3))
+    # Eq. 17 stop: relative change of successive iterates under a loose tol
+    rec("tol", nlcg_with_operator(obs, op, num_iter=40, background=10.0, regularizer=Hessian3D(),
+                                  reg_weight=1e-3, tol=3e-2, min_iter=5))
+    rec("grad", nlcg_with_operator(obs, op, num_iter=10, background=10.0,
+                                   regularizer=Gradient3D(r=0.85), reg_weight=2e-3,
+                                   restart_interval=4, min_iter=100, eval_interval=2))
+    init = np.full(shape, float(obs.mean()), np.float32)
+    rec("init", nlcg_with_operator(obs, op, num_iter=6, background=10.0, init=init, min_iter=100,
+                                   newton_iters=2))
+    # composed operators: a crop (padded domain) and a 2x fractional-area downsample
+    opc = compose(Crop(shape, (12, 26, 28), start=(2, 3, 2)), LinearFFTConvolver(psf, shape))
+    obs_c = obs[2:14, 3:29, 2:30].copy()
+    g["obs_c"] = obs_c
+    rec("crop", nlcg_with_operator(obs_c, opc, num_iter=8, background=10.0, min_iter=100))
+    fwd = compose(FractionalAreaDownsample(2.0, in_shape=shape), LinearFFTConvolver(psf, shape))
+    b = np.asarray(np.array(fwd.forward(mx.array(_beads(shape, 60, seed=7)))), np.float64)
+    obs_d = np.random.default_rng(8).poisson(b / b.max() * 500.0 + 5.0).astype(np.float32)
+    g["obs_d"] = obs_d
+    rec("down", nlcg_with_operator(obs_d, fwd, num_iter=8, background=5.0, min_iter=100,
+                                   regularizer=Hessian3D(r=0.5), reg_weight=1e-3))
+
+    # helpers at a fixed point s, direction d
+    rng = np.random.default_rng(9)
+    s = (rng.random(shape, dtype=np.float32) * 20 + 1).astype(np.float32)
+    d = (rng.standard_normal(shape).astype(np.float32) * 0.5).astype(np.float32)
+    g["h_s"], g["h_d"] = s, d
+    for tag, reg, beta in (("n", None, 0.0), ("r", Hessian3D(), 1e-3)):
+        g[f"h{tag}_obj"] = np.array(nlcg_objective(mx.array(s), op, mx.array(obs), 10.0, reg, beta))
+        grad, aux = nlcg_gradient(mx.array(s), op, mx.array(obs), 10.0, reg, beta)
+        g[f"h{tag}_grad"] = np.array(grad)
+        g[f"h{tag}_quad"] = np.array(nlcg_hessian_quadform(mx.array(s), mx.array(d), op, mx.array(obs),
+                                                           10.0, reg, beta, aux=aux))
+        f = mx.array(s) * mx.array(s)
+        lam, m_lam = nlcg_step_length(mx.array(s), mx.array(d), f, aux[0], op, mx.array(obs), 10.0,
+                                      reg, beta)
+        g[f"h{tag}_lam"] = np.array(lam)
+        g[f"h{tag}_mlam"] = np.array(m_lam)
+    f1 = rng.random(shape, dtype=np.float32) + 0.1
+    f2 = f1 * (1 + 0.1 * rng.standard_normal(shape).astype(np.float32))
+    g["h_f1"], g["h_f2"] = f1, f2
+    g["h_idiv"] = np.array(i_divergence_between(mx.array(f1), mx.array(f2)))
+
+    np.savez_compressed(out_path, **{k: np.asarray(v) for k, v in g.items()})
+    print(f"wrote {out_path}: {len(g)} arrays")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--worker", choices=["fp32", "fp64", "psf"], default=None)
+    ap.add_argument("--worker", choices=["fp32", "fp64", "psf", "nlcg32", "nlcg64"], default=None)
     a = ap.parse_args()
     if a.worker == "psf":
         sys.path[:0] = [STANDIN, a.reference]
         _run_psf(os.path.join(HERE, "golden_psf.npz"))
+        return
+    if a.worker in ("nlcg32", "nlcg64"):
+        sys.path[:0] = [STANDIN, a.reference]
+        _run_nlcg(os.path.join(HERE, f"golden_nlcg_fp{a.worker[4:]}.npz"))
         return
     if a.worker:
         sys.path[:0] = [STANDIN, a.reference]
@@ -359,8 +445,9 @@ def main():
     for mode in ("fp32", "fp64"):
         env = dict(os.environ)
         env["DECON_STANDIN_FP64"] = "1" if mode == "fp64" else "0"
-        subprocess.run([sys.executable, os.path.abspath(__file__), "--reference", a.reference,
-                        "--worker", mode], check=True, env=env)
+        for w in (mode, "nlcg" + mode[2:]):
+            subprocess.run([sys.executable, os.path.abspath(__file__), "--reference", a.reference,
+                            "--worker", w], check=True, env=env)
 
 
 if __name__ == "__main__":

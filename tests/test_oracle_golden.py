@@ -200,3 +200,89 @@ def test_pupil_to_psf():
         r = P.pupil_to_psf(g[f"psf{i}_pupil"], g[f"psf{i}_kz"], g[f"psf{i}_z"],
                            bool(g[f"psf{i}_normalize"]))
         assert rel(r, g[f"psf{i}_psf"]) < 1e-7, i
+
+
+@pytest.fixture(scope="module", params=["fp32", "fp64"])
+def nl_gold(request):
+    g = np.load(os.path.join(HERE, "golden", f"golden_nlcg_{request.param}.npz"))
+    dt = np.float32 if request.param == "fp32" else np.float64
+    return g, dt
+
+
+def _nl_ops(g, dt):
+    shape = (16, 32, 32)
+    conv = ops.LinearFFTConvolver(g["psf"], shape, dtype=dt)
+    return dict(
+        conv=conv,
+        crop=ops.compose(ops.Crop(shape, (12, 26, 28), start=(2, 3, 2)), conv),
+        down=ops.compose(ops.FractionalAreaDownsample(2.0, in_shape=shape, dtype=dt), conv),
+    )
+
+
+NL_CASES = {  # name: (observation key, operator, keyword arguments)
+    "plain": ("obs", "conv", dict(num_iter=15, background=10.0, eval_interval=4, min_iter=100)),
+    "stop": ("obs", "conv", dict(num_iter=40, background=10.0, slack=6.0, min_iter=3)),
+    "hess": ("obs", "conv", dict(num_iter=12, background=10.0, reg="hess", reg_weight=1e-3, tol=1e-4,
+                                 min_iter=5, eval_interval=3)),
+    "tol": ("obs", "conv", dict(num_iter=40, background=10.0, reg="hess", reg_weight=1e-3, tol=3e-2,
+                                min_iter=5)),
+    "grad": ("obs", "conv", dict(num_iter=10, background=10.0, reg="grad", reg_weight=2e-3,
+                                 restart_interval=4, min_iter=100, eval_interval=2)),
+    "init": ("obs", "conv", dict(num_iter=6, background=10.0, init="mean", min_iter=100,
+                                 newton_iters=2)),
+    "crop": ("obs_c", "crop", dict(num_iter=8, background=10.0, min_iter=100)),
+    "down": ("obs_d", "down", dict(num_iter=8, background=5.0, min_iter=100, reg="hess05",
+                                   reg_weight=1e-3)),
+}
+
+
+def nl_kwargs(g, dt, kw):
+    kw = dict(kw)
+    reg = kw.pop("reg", None)
+    if reg == "hess":
+        kw["regularizer"] = ops.Hessian3D(1.0, dt)
+    elif reg == "hess05":
+        kw["regularizer"] = ops.Hessian3D(0.5, dt)
+    elif reg == "grad":
+        kw["regularizer"] = ops.Gradient3D(0.85, dt)
+    if kw.get("init") == "mean":
+        kw["init"] = np.full((16, 32, 32), float(g["obs"].mean()), np.float32)
+    return kw
+
+
+@pytest.mark.parametrize("name", list(NL_CASES))
+def test_nlcg(nl_gold, name):
+    """oracle/nlcg.py against the reference's nlcg_with_operator: the same
+    iteration count, stop decision and loss history; iterates to float32
+    round-off (the trajectory amplifies it over the iterations) or ~1e-9 in
+    float64."""
+    from oracle import nlcg
+
+    g, dt = nl_gold
+    obs_key, op_key, kw = NL_CASES[name]
+    r = nlcg.nlcg_with_operator(g[obs_key], _nl_ops(g, dt)[op_key], dtype=dt, **nl_kwargs(g, dt, kw))
+    assert r["iterations"] == int(g[name + "_iters"])
+    assert r["converged"] == bool(g[name + "_converged"])
+    assert rel(r["restored"], g[name + "_x"]) < tol(dt, 2e-4, 1e-9)
+    assert rel(r["pred"], g[name + "_pred"]) < tol(dt, 2e-5, 1e-10)
+    np.testing.assert_allclose(r["loss_history"], g[name + "_loss"], rtol=tol(dt, 1e-4, 1e-9))
+
+
+def test_nlcg_helpers(nl_gold):
+    from oracle import nlcg
+
+    g, dt = nl_gold
+    conv = _nl_ops(g, dt)["conv"]
+    s, d, y = g["h_s"].astype(dt), g["h_d"].astype(dt), g["obs"].astype(dt)
+    for tag, reg, beta in (("n", None, 0.0), ("r", ops.Hessian3D(1.0, dt), 1e-3)):
+        assert nlcg.nlcg_objective(s, conv, y, 10.0, reg, beta, dtype=dt) == pytest.approx(
+            float(g[f"h{tag}_obj"]), rel=tol(dt, 1e-6, 1e-12))
+        grad, aux = nlcg.nlcg_gradient(s, conv, y, 10.0, reg, beta, dtype=dt)
+        assert rel(grad, g[f"h{tag}_grad"]) < tol(dt, 1e-5, 1e-11)
+        q = nlcg.nlcg_hessian_quadform(s, d, conv, y, 10.0, reg, beta, aux=aux, dtype=dt)
+        assert q == pytest.approx(float(g[f"h{tag}_quad"]), rel=tol(dt, 1e-5, 1e-11))
+        lam, m_lam = nlcg.nlcg_step_length(s, d, s * s, aux[0], conv, y, 10.0, reg, beta, dtype=dt)
+        assert lam == pytest.approx(float(g[f"h{tag}_lam"]), rel=tol(dt, 1e-4, 1e-10))
+        assert rel(m_lam, g[f"h{tag}_mlam"]) < tol(dt, 1e-6, 1e-12)
+    v = nlcg.i_divergence_between(g["h_f1"].astype(dt), g["h_f2"].astype(dt))
+    assert v == pytest.approx(float(g["h_idiv"]), rel=tol(dt, 1e-5, 1e-12))
