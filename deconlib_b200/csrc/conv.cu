@@ -352,6 +352,7 @@ int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cva
         a.fd_q4 = make_fastdiv(std::max<int64_t>(1, a.Nx / 4));
         a.fd_H = make_fastdiv(a.Hx);
         a.fd_nin = make_fastdiv(std::max<int64_t>(1, nin));
+        a.fd_np = make_fastdiv(L / 2 + 1);
     }
     const int nthr = threads_for(a.T, a.ax);
     const int64_t nblk = cdiv(a.nrows, a.T);

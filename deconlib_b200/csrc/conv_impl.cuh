@@ -41,7 +41,7 @@ struct XR2CArgs {
     int Hx, odd, T, vec4;
     Axis ax;            // length Fx/2 (even Fx) or Fx (odd)
     const float2* twx;  // W_Fx table
-    FastDiv fd_q4, fd_H, fd_nin;  // Nx / 4, Hx, packed non-zero points
+    FastDiv fd_q4, fd_H, fd_nin, fd_np;  // Nx / 4, Hx, packed non-zero points, L / 2 + 1
 };
 
 struct ColArgs {

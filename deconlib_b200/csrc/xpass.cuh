@@ -161,23 +161,33 @@ __global__ void __launch_bounds__(kFftThreads, 3) k_xr2c(XR2CArgs a) {
     if constexpr (LS > 0) fft_lines_pow2<LS, -1, 1, TC>(sm, T, tid % T, tid / T, a.ax.tw, a.ax.tws, nin);
     else fft_lines<-1, LS>(sm, T, tid % T, tid / T, a.ax, nin);
     const int H = a.Hx;
-    #pragma unroll 1
-    for (int q = tid; q < T * H; q += blockDim.x) {
-        const int t = fdiv(q, a.fd_H), k = q - t * H;
-        const int64_t row = row0 + t;
-        if (row >= a.nrows) continue;
-        float2 X;
-        if (a.odd) {
-            X = sm[phys(k, t, T)];
-        } else {
-            const int M = L;
-            const float2 zk = sm[phys(k == M ? 0 : k, t, T)];
-            const float2 zm = cconj(sm[phys(k == 0 ? 0 : M - k, t, T)]);
+    if (a.odd) {
+        #pragma unroll 1
+        for (int q = tid; q < T * H; q += blockDim.x) {
+            const int t = fdiv(q, a.fd_H), k = q - t * H;
+            const int64_t row = row0 + t;
+            if (row < a.nrows) a.out[row * a.P + k] = sm[phys(k, t, T)];
+        }
+    } else {
+        // X[k] = e + W^k o and X[M-k] = conj(e) + W^(M-k) conj(o) with
+        // e = (Z[k] + conj Z[M-k]) / 2, o = -i (Z[k] - conj Z[M-k]) / 2: one
+        // thread per pair (k, M - k), the same float operations as the
+        // single-output form (X[M] pairs with X[0], indices mod M).
+        const int M = L, np = (M >> 1) + 1;
+        #pragma unroll 1
+        for (int q = tid; q < T * np; q += blockDim.x) {
+            const int t = fdiv(q, a.fd_np), k = q - t * np;
+            const int64_t row = row0 + t;
+            if (row >= a.nrows) continue;
+            const int km = M - k;  // partner output (M for k = 0)
+            const float2 zk = sm[phys(k, t, T)];
+            const float2 zm = cconj(sm[phys(k == 0 ? 0 : km, t, T)]);
             const float2 e = cscale(cadd(zk, zm), 0.5f);
             const float2 o = rot90<-1>(cscale(csub(zk, zm), 0.5f));
-            X = cadd(e, cmul(__ldg(&a.twx[k]), o));
+            float2* orow = a.out + row * a.P;
+            if (k < H) orow[k] = cadd(e, cmul(__ldg(&a.twx[k]), o));
+            if (km != k && km < H) orow[km] = cadd(cconj(e), cmul(__ldg(&a.twx[km]), cconj(o)));
         }
-        a.out[row * a.P + k] = X;
     }
 }
 
