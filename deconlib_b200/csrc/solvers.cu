@@ -710,8 +710,8 @@ int decon_pdhg_hess_dual(decon_pdhg* h, float* y2, const float* xc, const float*
     const int64_t n = d.nz * d.ny * d.nx;
     (void)n;
     const TileGeo tg(d);
-    const void* fn = norm == 0 ? (const void*)k_hess_dual_p<0> : (const void*)k_hess_dual_p<1>;
     int per_sm = 1;
+    const void* fn = norm == 0 ? (const void*)k_hess_dual_p<0> : (const void*)k_hess_dual_p<1>;
     DK_TRY(smem_prepare(fn, DualLayout::bytes, &per_sm));
     const int grid = (int)std::min<int64_t>(tg.ntiles, (int64_t)sm_count() * per_sm);
     if (norm == 0)
@@ -740,10 +740,11 @@ int decon_pdhg_hess_dk(decon_pdhg* h, const float* ax_new, const float* ax_cur, 
     W6 w;
     hessian_weights(r, w.w);
     int per_sm = 1;
-    DK_TRY(smem_prepare((const void*)k_hess_dk_p, DkLayout::bytes, &per_sm));
-    const int grid = std::min(kPdhgGrid, sm_count() * per_sm);
-    k_hess_dk_p<<<grid, 256, DkLayout::bytes, as_stream(stream)>>>(
-        h->dev, ax_new, ax_cur, m, xn, xc, Dims{shape[0], shape[1], shape[2]}, w, kSlotDA2, kSlotDL2);
+    const Dims d{shape[0], shape[1], shape[2]};
+    DK_TRY(smem_prepare((const void*)k_hess_dk_r, 0, &per_sm));
+    const int grid = (int)std::min<int64_t>(kPdhgGrid, std::max<int64_t>(TileGeo(d).ntiles, 1));
+    k_hess_dk_r<<<grid, 256, 0, as_stream(stream)>>>(h->dev, ax_new, ax_cur, m, xn, xc, d, w, kSlotDA2,
+                                                    kSlotDL2);
     DK_LAUNCHED();
     return DECON_OK;
 }
