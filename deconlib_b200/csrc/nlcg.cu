@@ -18,11 +18,14 @@
 //   k_nlcg_gradient   r = -(2 s K^T w + 4 beta s C^T C f), |r|^2, the
 //                     I-divergence between successive f and sum f
 //
-// Every reduction is deterministic: each CTA writes its FP64 partials, and
+// Element-wise passes move four values per thread and array with float4
+// loads and stores when the arrays are 16-byte aligned (ew4).  Every
+// reduction is deterministic: each CTA writes its FP64 partials, and
 // the last CTA to finish (a ticket counter, no waiting) folds them in block
 // order.  The Newton loop runs on the device (lam never leaves HBM), so an
 // iteration needs one host read, after the speculative gradient.
 #include <cfloat>
+#include <initializer_list>
 
 #include "conv_impl.cuh"
 
@@ -78,19 +81,54 @@ __device__ bool fold_last(double (&v)[NS], double* __restrict__ part, unsigned* 
     return true;
 }
 
+// Element-wise loop over n values of NI inputs and NO outputs: groups of four
+// with float4 loads and stores when `vec` (every pointer 16-byte aligned),
+// then the remainder one by one.  f(in[NI], out[NO]) handles one element;
+// a null input reads 0, a null output is not stored.
+template <int NI, int NO, class F>
+__device__ __forceinline__ void ew4(int64_t n, const float* const (&in)[NI], float* const (&out)[NO],
+                                    bool vec, F&& f) {
+    const int64_t ng = vec ? n / 4 : 0;
+    for (int64_t gi = gtid(); gi < ng; gi += gstride()) {
+        float4 a[NI];
+#pragma unroll
+        for (int k = 0; k < NI; ++k)
+            a[k] = in[k] ? __ldg(reinterpret_cast<const float4*>(in[k]) + gi) : make_float4(0.f, 0.f, 0.f, 0.f);
+        float o[NO][4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            float x[NI], y[NO];
+#pragma unroll
+            for (int k = 0; k < NI; ++k) x[k] = e == 0 ? a[k].x : e == 1 ? a[k].y : e == 2 ? a[k].z : a[k].w;
+            f(x, y);
+#pragma unroll
+            for (int k = 0; k < NO; ++k) o[k][e] = y[k];
+        }
+#pragma unroll
+        for (int k = 0; k < NO; ++k)
+            if (out[k]) reinterpret_cast<float4*>(out[k])[gi] = make_float4(o[k][0], o[k][1], o[k][2], o[k][3]);
+    }
+    for (int64_t i = 4 * ng + gtid(); i < n; i += gstride()) {
+        float x[NI], y[NO];
+#pragma unroll
+        for (int k = 0; k < NI; ++k) x[k] = in[k] ? in[k][i] : 0.f;
+        f(x, y);
+#pragma unroll
+        for (int k = 0; k < NO; ++k)
+            if (out[k]) out[k][i] = y[k];
+    }
+}
+
 // f0 = max(x, 1e-6), s = sqrt(f0), f = s s; or (from_s) f = s s alone.
 __global__ void k_nlcg_init(const float* __restrict__ x, float* __restrict__ s, float* __restrict__ f,
-                            int64_t n, int from_s) {
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        float sv;
-        if (from_s) {
-            sv = x[i];
-        } else {
-            sv = sqrtf(fmaxf(x[i], 1e-6f));
-            s[i] = sv;
-        }
-        f[i] = sv * sv;
-    }
+                            int64_t n, int from_s, int vec) {
+    const float* in[1] = {x};
+    float* out[2] = {from_s ? nullptr : s, f};
+    ew4(n, in, out, vec, [&](const float* v, float* o) {
+        const float sv = from_s ? v[0] : sqrtf(fmaxf(v[0], 1e-6f));
+        o[0] = sv;
+        o[1] = sv * sv;
+    });
 }
 
 // Data-space terms of a model m: w = 1 - g / max(m, eps); sums of m,
@@ -105,13 +143,11 @@ __device__ __forceinline__ void model_terms(float m, float g, float eps, float& 
 }
 
 __global__ void k_nlcg_model(const float* __restrict__ m, const float* __restrict__ g, float eps,
-                             float* __restrict__ w, int64_t n, double* part, NlcgDev* dev) {
+                             float* __restrict__ w, int64_t n, int vec, double* part, NlcgDev* dev) {
     double v[3] = {0.0, 0.0, 0.0};
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        float wi;
-        model_terms(m[i], g[i], eps, wi, v);
-        if (w) w[i] = wi;
-    }
+    const float* in[2] = {m, g};
+    float* out[1] = {w};
+    ew4(n, in, out, vec, [&](const float* x, float* o) { model_terms(x[0], x[1], eps, o[0], v); });
     fold_last<3>(v, part, &dev->ticket, dev->data);
 }
 
@@ -120,35 +156,36 @@ __global__ void k_nlcg_model(const float* __restrict__ m, const float* __restric
 __global__ void k_nlcg_products(int mode, float gamma, const float* __restrict__ s,
                                 const float* __restrict__ d, const float* __restrict__ r,
                                 float* __restrict__ d_out, float* __restrict__ sd,
-                                float* __restrict__ dd, int64_t n, NlcgDev* dev) {
+                                float* __restrict__ dd, int64_t n, int vec, NlcgDev* dev) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         dev->lam = 0.0;
         dev->done = 0;
         dev->newton_run = 0;
     }
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        float dv = d[i];
-        if (mode == 1) {
-            dv = r[i] + gamma * dv;
-            d_out[i] = dv;
-        }
-        sd[i] = s[i] * dv;
-        dd[i] = dv * dv;
-    }
+    const float* in[3] = {s, d, mode == 1 ? r : nullptr};
+    float* out[3] = {mode == 1 ? d_out : nullptr, sd, dd};
+    ew4(n, in, out, vec, [&](const float* x, float* o) {
+        const float dv = mode == 1 ? x[2] + gamma * x[1] : x[1];
+        o[0] = dv;
+        o[1] = x[0] * dv;
+        o[2] = dv * dv;
+    });
 }
 
 __global__ void k_nlcg_gram(const float* __restrict__ a, const float* __restrict__ b,
-                            const float* __restrict__ c, int64_t n, double* part, NlcgDev* dev) {
+                            const float* __restrict__ c, int64_t n, int vec, double* part, NlcgDev* dev) {
     double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        const double x = a[i], y = b[i], z = c[i];
+    const float* in[3] = {a, b, c};
+    float* out[1] = {nullptr};
+    ew4(n, in, out, vec, [&](const float* q, float*) {
+        const double x = q[0], y = q[1], z = q[2];
         v[0] += x * x;
         v[1] += x * y;
         v[2] += x * z;
         v[3] += y * y;
         v[4] += y * z;
         v[5] += z * z;
-    }
+    });
     fold_last<6>(v, part, &dev->ticket, dev->gram);
 }
 
@@ -156,21 +193,23 @@ __global__ void k_nlcg_gram(const float* __restrict__ a, const float* __restrict
 // lam <- lam - phi' / phi'' in the last CTA.
 __global__ void k_nlcg_newton(const float* __restrict__ m, const float* __restrict__ ksd,
                               const float* __restrict__ kdd, const float* __restrict__ g, float b,
-                              float eps, double beta, int use_reg, int64_t n, double* part,
+                              float eps, double beta, int use_reg, int64_t n, int vec, double* part,
                               NlcgDev* dev) {
     if (dev->done) return;  // every CTA reads the same flag: all return or none
     const double lam = dev->lam;
     const float c1 = (float)(2.0 * lam), c2 = (float)(lam * lam), lf = (float)lam;
     double v[3] = {0.0, 0.0, 0.0};
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        const float kss = m[i] - b, sdv = ksd[i], ddv = kdd[i], gv = g[i];
+    const float* in[4] = {m, ksd, kdd, g};
+    float* out[1] = {nullptr};
+    ew4(n, in, out, vec, [&](const float* x, float*) {
+        const float kss = x[0] - b, sdv = x[1], ddv = x[2], gv = x[3];
         const float ml = fmaxf(kss + c1 * sdv + c2 * ddv + b, eps);
         const float sl = sdv + lf * ddv;
         const float wl = 1.0f - gv / ml;
         v[0] += (double)(sl * wl);
         v[1] += (double)(ddv * wl);
         v[2] += (double)(gv * (sl * sl) / (ml * ml));
-    }
+    });
     if (!fold_last<3>(v, part, &dev->ticket, dev->nt)) return;
     if (threadIdx.x != 0) return;
     double d1 = 2.0 * dev->nt[0];
@@ -200,38 +239,42 @@ __global__ void k_nlcg_newton(const float* __restrict__ m, const float* __restri
 __global__ void k_nlcg_accept_d(const float* __restrict__ m, const float* __restrict__ ksd,
                                 const float* __restrict__ kdd, const float* __restrict__ g, float b,
                                 float eps, float* __restrict__ m_new, float* __restrict__ w_new,
-                                int64_t n, double* part, NlcgDev* dev) {
+                                int64_t n, int vec, double* part, NlcgDev* dev) {
     const double lam = dev->lam;
     const float c1 = (float)(2.0 * lam), c2 = (float)(lam * lam);
     double v[3] = {0.0, 0.0, 0.0};
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        const float kss = m[i] - b;
-        const float mn = kss + c1 * ksd[i] + c2 * kdd[i] + b;
-        m_new[i] = mn;
-        float wi;
-        model_terms(mn, g[i], eps, wi, v);
-        if (w_new) w_new[i] = wi;
-    }
+    const float* in[4] = {m, ksd, kdd, g};
+    float* out[2] = {m_new, w_new};
+    ew4(n, in, out, vec, [&](const float* x, float* o) {
+        const float kss = x[0] - b;
+        const float mn = kss + c1 * x[1] + c2 * x[2] + b;
+        o[0] = mn;
+        model_terms(mn, x[3], eps, o[1], v);
+    });
     fold_last<3>(v, part, &dev->ticket, dev->data);
 }
 
 __global__ void k_nlcg_accept_o(const float* __restrict__ s, const float* __restrict__ d,
-                                float* __restrict__ s_new, float* __restrict__ f_new, int64_t n,
+                                float* __restrict__ s_new, float* __restrict__ f_new, int64_t n, int vec,
                                 const NlcgDev* dev) {
     const float lf = (float)dev->lam;
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        const float sn = s[i] + lf * d[i];
-        s_new[i] = sn;
-        f_new[i] = sn * sn;
-    }
+    const float* in[2] = {s, d};
+    float* out[2] = {s_new, f_new};
+    ew4(n, in, out, vec, [&](const float* x, float* o) {
+        const float sn = x[0] + lf * x[1];
+        o[0] = sn;
+        o[1] = sn * sn;
+    });
 }
 
-__global__ void k_nlcg_energy(const float* __restrict__ a, int64_t n, double* part, NlcgDev* dev) {
+__global__ void k_nlcg_energy(const float* __restrict__ a, int64_t n, int vec, double* part, NlcgDev* dev) {
     double v[1] = {0.0};
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        const double x = a[i];
-        v[0] += x * x;
-    }
+    const float* in[1] = {a};
+    float* out[1] = {nullptr};
+    ew4(n, in, out, vec, [&](const float* x, float*) {
+        const double q = x[0];
+        v[0] += q * q;
+    });
     fold_last<1>(v, part, &dev->ticket, dev->reg);
 }
 
@@ -241,24 +284,28 @@ __global__ void k_nlcg_energy(const float* __restrict__ a, int64_t n, double* pa
 __global__ void k_nlcg_gradient(const float* __restrict__ s, const float* __restrict__ f,
                                 const float* __restrict__ f_prev, const float* __restrict__ ktw,
                                 const float* __restrict__ ctcf, float c4b, float eps,
-                                float* __restrict__ r, int64_t n, double* part, NlcgDev* dev) {
+                                float* __restrict__ r, int64_t n, int vec, double* part, NlcgDev* dev) {
     double v[3] = {0.0, 0.0, 0.0};
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        if (ktw) {
-            const float sv = s[i];
-            float grad = (2.0f * sv) * ktw[i];
-            if (ctcf) grad = grad + (c4b * sv) * ctcf[i];
+    const bool has_g = ktw != nullptr, has_c = ctcf != nullptr, has_p = f_prev != nullptr;
+    const float* in[5] = {has_g ? s : nullptr, f, f_prev, ktw, ctcf};
+    float* out[1] = {has_g ? r : nullptr};
+    ew4(n, in, out, vec, [&](const float* x, float* o) {
+        o[0] = 0.f;
+        if (has_g) {
+            const float sv = x[0];
+            float grad = (2.0f * sv) * x[3];
+            if (has_c) grad = grad + (c4b * sv) * x[4];
             const float rv = -grad;
-            r[i] = rv;
+            o[0] = rv;
             v[0] += (double)rv * (double)rv;
         }
-        const float fc = f[i];
-        if (f_prev) {
-            const float fp = f_prev[i];
+        const float fc = x[1];
+        if (has_p) {
+            const float fp = x[2];
             v[1] += (double)(fp * (logf(fmaxf(fp, eps)) - logf(fmaxf(fc, eps))) - fp + fc);
         }
         v[2] += (double)fc;
-    }
+    });
     fold_last<3>(v, part, &dev->ticket, dev->obj);
 }
 
@@ -282,6 +329,13 @@ __global__ void k_nlcg_quad(const float* __restrict__ g, const float* __restrict
 
 static int nl_blocks(int64_t n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(kNlMaxBlocks, cdiv(n, (int64_t)kNlThreads * 4)));
+}
+
+// 1 when every non-null pointer is 16-byte aligned (float4 path of ew4).
+static int al16(std::initializer_list<const void*> ps) {
+    for (const void* p : ps)
+        if (p && (reinterpret_cast<uintptr_t>(p) & 15) != 0) return 0;
+    return 1;
 }
 
 }  // namespace dk
@@ -329,7 +383,7 @@ int decon_nlcg_destroy(decon_nlcg* h) { return nl_free(h); }
 int decon_nlcg_init(const float* x, float* s, float* f, int64_t n, int from_s, void* stream) {
     if (!x || !f || (!from_s && !s)) return fail(DECON_ERR_NULL, "null pointer");
     if (n <= 0) return DECON_OK;
-    k_nlcg_init<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(x, s, f, n, from_s);
+    k_nlcg_init<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(x, s, f, n, from_s, al16({x, s, f}));
     DK_LAUNCHED();
     return DECON_OK;
 }
@@ -338,7 +392,8 @@ int decon_nlcg_model(decon_nlcg* h, const float* m, const float* g, float eps, f
                      void* stream) {
     if (!h || !m || !g) return fail(DECON_ERR_NULL, "null pointer");
     if (n <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_model: empty data");
-    k_nlcg_model<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(m, g, eps, w, n, h->part, h->dev);
+    k_nlcg_model<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(m, g, eps, w, n, al16({m, g, w}),
+                                                                     h->part, h->dev);
     DK_LAUNCHED();
     return DECON_OK;
 }
@@ -349,8 +404,9 @@ int decon_nlcg_products(decon_nlcg* h, int mode, float gamma, const float* s, co
         return fail(DECON_ERR_NULL, "null pointer");
     if (mode != 0 && mode != 1) return fail(DECON_ERR_VALUE, "decon_nlcg_products: mode must be 0 or 1");
     if (n <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_products: empty object");
+    const int vec = al16({s, d, mode == 1 ? r : nullptr, mode == 1 ? d_out : nullptr, sd, dd});
     k_nlcg_products<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(mode, gamma, s, d, r, d_out, sd,
-                                                                        dd, n, h->dev);
+                                                                        dd, n, vec, h->dev);
     DK_LAUNCHED();
     return DECON_OK;
 }
@@ -359,7 +415,8 @@ int decon_nlcg_gram(decon_nlcg* h, const float* a, const float* b, const float* 
                     void* stream) {
     if (!h || !a || !b || !c) return fail(DECON_ERR_NULL, "null pointer");
     if (n <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_gram: empty");
-    k_nlcg_gram<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(a, b, c, n, h->part, h->dev);
+    k_nlcg_gram<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(a, b, c, n, al16({a, b, c}), h->part,
+                                                                    h->dev);
     DK_LAUNCHED();
     return DECON_OK;
 }
@@ -372,7 +429,7 @@ int decon_nlcg_newton(decon_nlcg* h, const float* m, const float* ksd, const flo
     const cudaStream_t st = as_stream(stream);
     for (int it = 0; it < newton_iters; ++it) {
         k_nlcg_newton<<<nl_blocks(n), kNlThreads, 0, st>>>(m, ksd, kdd, g, background, eps, beta, use_reg,
-                                                          n, h->part, h->dev);
+                                                          n, al16({m, ksd, kdd, g}), h->part, h->dev);
         DK_LAUNCHED();
     }
     return DECON_OK;
@@ -386,11 +443,13 @@ int decon_nlcg_accept(decon_nlcg* h, const float* m, const float* ksd, const flo
     if (nd <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_accept: empty data");
     const cudaStream_t st = as_stream(stream);
     k_nlcg_accept_d<<<nl_blocks(nd), kNlThreads, 0, st>>>(m, ksd, kdd, g, background, eps, m_new, w_new,
-                                                         nd, h->part, h->dev);
+                                                         nd, al16({m, ksd, kdd, g, m_new, w_new}), h->part,
+                                                         h->dev);
     DK_LAUNCHED();
     if (s) {
         if (!d || !s_new || !f_new) return fail(DECON_ERR_NULL, "null pointer");
-        k_nlcg_accept_o<<<nl_blocks(no), kNlThreads, 0, st>>>(s, d, s_new, f_new, no, h->dev);
+        k_nlcg_accept_o<<<nl_blocks(no), kNlThreads, 0, st>>>(s, d, s_new, f_new, no,
+                                                             al16({s, d, s_new, f_new}), h->dev);
         DK_LAUNCHED();
     }
     return DECON_OK;
@@ -399,7 +458,7 @@ int decon_nlcg_accept(decon_nlcg* h, const float* m, const float* ksd, const flo
 int decon_nlcg_energy(decon_nlcg* h, const float* a, int64_t n, void* stream) {
     if (!h || !a) return fail(DECON_ERR_NULL, "null pointer");
     if (n <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_energy: empty");
-    k_nlcg_energy<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(a, n, h->part, h->dev);
+    k_nlcg_energy<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(a, n, al16({a}), h->part, h->dev);
     DK_LAUNCHED();
     return DECON_OK;
 }
@@ -409,8 +468,9 @@ int decon_nlcg_gradient(decon_nlcg* h, const float* s, const float* f, const flo
                         void* stream) {
     if (!h || !f || (ktw && (!s || !r))) return fail(DECON_ERR_NULL, "null pointer");
     if (n <= 0) return fail(DECON_ERR_VALUE, "decon_nlcg_gradient: empty object");
+    const int vec = al16({ktw ? s : nullptr, f, f_prev, ktw, ctcf, ktw ? r : nullptr});
     k_nlcg_gradient<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(s, f, f_prev, ktw, ctcf, c4b, eps,
-                                                                       r, n, h->part, h->dev);
+                                                                       r, n, vec, h->part, h->dev);
     DK_LAUNCHED();
     return DECON_OK;
 }
