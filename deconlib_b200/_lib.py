@@ -60,6 +60,8 @@ _SIGS = {
     "decon_nlcg_energy": (C.c_int, [_p, _p, _i64, _p]),
     "decon_nlcg_gradient": (C.c_int, [_p, _p, _p, _p, _p, _p, C.c_float, C.c_float, _p, _i64, _p]),
     "decon_nlcg_quad": (C.c_int, [_p, _p, _p, _p, _i64, _p, _p, _i64, C.c_float, _p]),
+    "decon_nlcg_hess_gram": (C.c_int, [_p, _p, _p, _p, _p, C.c_float, _p]),
+    "decon_nlcg_hess_energy": (C.c_int, [_p, _p, _p, C.c_float, _p]),
     "decon_nlcg_read": (C.c_int, [_p, _p, _p]),
     "decon_batch_rl_create": (C.c_int, [C.c_int, _p, _p, _p, _p, _p, _p, C.c_int, C.POINTER(_p)]),
     "decon_batch_rl_setup": (C.c_int, [_p, _p, _p]),

@@ -28,6 +28,7 @@
 #include <initializer_list>
 
 #include "conv_impl.cuh"
+#include "zwalk.cuh"
 
 namespace dk {
 
@@ -309,6 +310,52 @@ __global__ void k_nlcg_gradient(const float* __restrict__ s, const float* __rest
     fold_last<3>(v, part, &dev->ticket, dev->obj);
 }
 
+// Hessian3D regulariser without materialising its images (the 6-component
+// fields C f, C(s d), C(d^2)): their Gram matrix and ||C f||^2 with the
+// components evaluated on the fly by the register z-walk (zwalk.cuh), whose
+// float operations are the operator's.
+struct Fields3 {
+    float a, b, c;
+};
+
+__global__ void __launch_bounds__(256) k_nlcg_hess_gram(const float* __restrict__ f,
+                                                        const float* __restrict__ sd,
+                                                        const float* __restrict__ dd, Dims d, W6 w,
+                                                        double* part, NlcgDev* dev) {
+    double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    hess_zwalk<3>(
+        d, w, [&](int64_t i) { return Fields3{__ldg(f + i), __ldg(sd + i), __ldg(dd + i)}; },
+        [](const Fields3& r, int k) { return k == 0 ? r.a : (k == 1 ? r.b : r.c); },
+        [&](int64_t, const float (*h)[6]) {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const double x = h[0][q], y = h[1][q], z = h[2][q];
+                v[0] += x * x;
+                v[1] += x * y;
+                v[2] += x * z;
+                v[3] += y * y;
+                v[4] += y * z;
+                v[5] += z * z;
+            }
+        });
+    fold_last<6>(v, part, &dev->ticket, dev->gram);
+}
+
+__global__ void __launch_bounds__(256) k_nlcg_hess_energy(const float* __restrict__ f, Dims d, W6 w,
+                                                          double* part, NlcgDev* dev) {
+    double v[1] = {0.0};
+    hess_zwalk<1>(
+        d, w, [&](int64_t i) { return __ldg(f + i); }, [](const float& r, int) { return r; },
+        [&](int64_t, const float (*h)[6]) {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const double x = h[0][q];
+                v[0] += x * x;
+            }
+        });
+    fold_last<1>(v, part, &dev->ticket, dev->reg);
+}
+
 // Quadratic-form helper sums (nlcg_mlx.py:181-193):
 // quad[0] = sum (g / max(m m, eps)) K(sd)^2, quad[1] = sum a d^2.
 __global__ void k_nlcg_quad(const float* __restrict__ g, const float* __restrict__ m,
@@ -471,6 +518,41 @@ int decon_nlcg_gradient(decon_nlcg* h, const float* s, const float* f, const flo
     const int vec = al16({ktw ? s : nullptr, f, f_prev, ktw, ctcf, ktw ? r : nullptr});
     k_nlcg_gradient<<<nl_blocks(n), kNlThreads, 0, as_stream(stream)>>>(s, f, f_prev, ktw, ctcf, c4b, eps,
                                                                        r, n, vec, h->part, h->dev);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+static int hess_grid(const Dims& d, const void* fn) {
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, 0) != cudaSuccess) {
+        cudaGetLastError();
+        occ = 1;
+    }
+    const int64_t cap = std::min<int64_t>(kNlMaxBlocks, (int64_t)sm_count() * std::max(occ, 1));
+    return (int)std::max<int64_t>(1, std::min<int64_t>(TileGeo(d).ntiles, cap));
+}
+
+int decon_nlcg_hess_gram(decon_nlcg* h, const float* f, const float* sd, const float* dd,
+                         const int64_t shape[3], float r, void* stream) {
+    if (!h || !f || !sd || !dd || !shape) return fail(DECON_ERR_NULL, "null pointer");
+    if (shape[0] < 1 || shape[1] < 1 || shape[2] < 1) return fail(DECON_ERR_VALUE, "decon_nlcg_hess_gram: empty");
+    const Dims d{shape[0], shape[1], shape[2]};
+    W6 w;
+    hessian_weights(r, w.w);
+    k_nlcg_hess_gram<<<hess_grid(d, (const void*)k_nlcg_hess_gram), 256, 0, as_stream(stream)>>>(
+        f, sd, dd, d, w, h->part, h->dev);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+int decon_nlcg_hess_energy(decon_nlcg* h, const float* f, const int64_t shape[3], float r, void* stream) {
+    if (!h || !f || !shape) return fail(DECON_ERR_NULL, "null pointer");
+    if (shape[0] < 1 || shape[1] < 1 || shape[2] < 1) return fail(DECON_ERR_VALUE, "decon_nlcg_hess_energy: empty");
+    const Dims d{shape[0], shape[1], shape[2]};
+    W6 w;
+    hessian_weights(r, w.w);
+    k_nlcg_hess_energy<<<hess_grid(d, (const void*)k_nlcg_hess_energy), 256, 0, as_stream(stream)>>>(
+        f, d, w, h->part, h->dev);
     DK_LAUNCHED();
     return DECON_OK;
 }

@@ -31,52 +31,10 @@
 
 #include "solvers.cuh"
 #include "stencil.cuh"
+#include "zwalk.cuh"
 
 namespace dk {
 
-constexpr int kTX = 32, kTY = 8, kHX = kTX + 2, kHY = kTY + 2, kPL = kHX * kHY;
-constexpr int kZChunk = 16;
-
-struct TileGeo {
-    int64_t ntx, nty, ntz, ntiles;
-    __host__ __device__ TileGeo(const Dims& d)
-        : ntx((d.nx + kTX - 1) / kTX), nty((d.ny + kTY - 1) / kTY),
-          ntz((d.nz + kZChunk - 1) / kZChunk), ntiles(0) {
-        ntiles = ntx * nty * ntz;
-    }
-};
-
-__device__ __forceinline__ int sidx(int64_t yy, int64_t xx, int64_t y0, int64_t x0) {
-    return (int)((yy - y0 + 1) * kHX + (xx - x0 + 1));
-}
-
-// This thread's (up to two) halo-plane elements: fixed (row, column) of the
-// staged tile, loaded into registers one plane ahead of use.
-struct StageSlots {
-    int q[2];
-    int64_t off[2];  // in-plane offset (clamped y, x)
-    bool ok[2];
-    __device__ __forceinline__ StageSlots(int64_t x0, int64_t y0, const Dims& d) {
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            q[u] = threadIdx.x + u * blockDim.x;
-            ok[u] = q[u] < kPL;
-            const int ly = q[u] / kHX, lx = q[u] - ly * kHX;
-            off[u] = clampi(y0 - 1 + ly, d.ny) * d.nx + clampi(x0 - 1 + lx, d.nx);
-        }
-    }
-    // f(plane_offset + in_plane_offset) for plane zz
-    template <class F>
-    __device__ __forceinline__ void load(float r[2], const F& f, int64_t zz, int64_t plane) const {
-#pragma unroll
-        for (int u = 0; u < 2; ++u) r[u] = ok[u] ? f(zz * plane + off[u]) : 0.f;
-    }
-    __device__ __forceinline__ void store(float* p, const float r[2]) const {
-#pragma unroll
-        for (int u = 0; u < 2; ++u)
-            if (ok[u]) p[q[u]] = r[u];
-    }
-};
 
 // Hessian components at tile-local (ly, lx) (1-based, halo at 0 and kT+1)
 // from staged planes: clamping is already in the staged values, so the taps
@@ -360,89 +318,6 @@ __device__ __forceinline__ void put_slot(PdhgDev* s, int slot, double v) {
         for (int i = gridDim.x + threadIdx.x; i < kPdhgGrid; i += blockDim.x) s->partials[slot * kPdhgGrid + i] = 0.0;
 }
 
-// Hessian of a field over this CTA's tiles with the z axis walked in
-// registers.  Each thread owns (up to two) positions of the 34 x 10 tile +
-// halo plane and keeps the field at z - 1, z, z + 1 of them in registers (the
-// raw loads of the next plane one plane ahead); per plane it publishes the
-// three values its neighbours' stencils take from it: the field, the half
-// central z-difference (f(z+1) - f(z-1)) / 2 and the second z-difference.
-// Planes are double-buffered, so a plane costs one CTA barrier.  Every float
-// operation is hess6_smem's, evaluated by the owner of an operand instead of
-// its reader, so the components equal hess6_smem's bit for bit.
-//   raw(i)   -> float2: the loads behind the field at linear index i
-//   val(r)   -> float:  the field from them
-//   body(i, h): voxel i of the tile interior with its six weighted components
-template <class Raw, class Val, class Body>
-__device__ __forceinline__ void hess_zwalk(const Dims& d, const W6& w, const Raw& raw, const Val& val,
-                                           const Body& body) {
-    __shared__ float sp[2][kPL], sh[2][kPL], sz[2][kPL];
-    const int64_t plane = d.ny * d.nx;
-    const TileGeo g(d);
-    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-    const int c = (ty + 1) * kHX + (tx + 1);
-    const int n = c - kHX, so = c + kHX, wv = c - 1, e = c + 1;
-    int buf = 0;
-    for (int64_t tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
-        const int64_t bx = tile % g.ntx, r = tile / g.ntx, by = r % g.nty, bz = r / g.nty;
-        const int64_t x0 = bx * kTX, y0 = by * kTY, z0 = bz * kZChunk;
-        const int64_t z1 = min(z0 + kZChunk, d.nz);
-        const bool in = x0 + tx < d.nx && y0 + ty < d.ny;
-        const int64_t ipl = (y0 + ty) * d.nx + (x0 + tx);
-        const StageSlots st(x0, y0, d);
-        float vm[2], vc[2];
-        float2 rq[2];
-        {
-            const int64_t zb = clampi(z0 - 1, d.nz), zq = clampi(z0 + 1, d.nz);
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                vm[u] = vc[u] = 0.f;
-                rq[u] = make_float2(0.f, 0.f);
-                if (st.ok[u]) {
-                    vm[u] = val(raw(zb * plane + st.off[u]));
-                    vc[u] = val(raw(z0 * plane + st.off[u]));
-                    rq[u] = raw(zq * plane + st.off[u]);
-                }
-            }
-        }
-        for (int64_t z = z0; z < z1; ++z) {
-            float vp[2];
-            const int64_t zq = clampi(z + 2, d.nz);
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                vp[u] = val(rq[u]);
-                if (st.ok[u] && z + 1 < z1) rq[u] = raw(zq * plane + st.off[u]);
-                if (st.ok[u]) {
-                    sp[buf][st.q[u]] = vc[u];
-                    sh[buf][st.q[u]] = (vp[u] - vm[u]) / 2.f;
-                    sz[buf][st.q[u]] = d2v(vm[u], vc[u], vp[u]);
-                }
-            }
-            __syncthreads();
-            if (in) {
-                const float* P = sp[buf];
-                const float* Hz = sh[buf];
-                const float cv = P[c];
-                float h[6];
-                h[0] = sz[buf][c] * w.w[0];
-                h[1] = d2v(P[n], cv, P[so]) * w.w[1];
-                h[2] = d2v(P[wv], cv, P[e]) * w.w[2];
-                h[3] = ((Hz[so] - Hz[n]) / 2.f) * w.w[3];
-                h[4] = ((Hz[e] - Hz[wv]) / 2.f) * w.w[4];
-                const float dy_xp = (P[so + 1] - P[n + 1]) / 2.f;
-                const float dy_xm = (P[so - 1] - P[n - 1]) / 2.f;
-                h[5] = ((dy_xp - dy_xm) / 2.f) * w.w[5];
-                body(z * plane + ipl, h);
-            }
-            buf ^= 1;
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                vm[u] = vc[u];
-                vc[u] = vp[u];
-            }
-        }
-    }
-}
-
 // ||A x_new - A x||^2 and ||H (x_new - x)||^2 (z axis walked in registers).
 __global__ void __launch_bounds__(256) k_hess_dk_r(PdhgDev* s, const float* __restrict__ axn,
                                                    const float* __restrict__ axc, int64_t m,
@@ -456,14 +331,14 @@ __global__ void __launch_bounds__(256) k_hess_dk_r(PdhgDev* s, const float* __re
         const double dd = (double)axn[i] - (double)axc[i];
         a2 += dd * dd;
     }
-    hess_zwalk(
+    hess_zwalk<1>(
         d, w, [&](int64_t i) { return make_float2(__ldg(xn + i), __ldg(xc + i)); },
-        [](float2 r) { return r.x - r.y; },
-        [&](int64_t, const float* h) {
+        [](const float2& r, int) { return r.x - r.y; },
+        [&](int64_t, const float (*h)[6]) {
             // the six squares of one voxel in FP32, the sum over voxels in FP64
             float v = 0.f;
 #pragma unroll
-            for (int k = 0; k < 6; ++k) v = fmaf(h[k], h[k], v);
+            for (int k = 0; k < 6; ++k) v = fmaf(h[0][k], h[0][k], v);
             l2 += (double)v;
         });
     put_slot(s, slot_a, a2);

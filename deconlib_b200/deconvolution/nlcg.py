@@ -10,7 +10,9 @@ COSM), with the same stopping rules (discrepancy principle, Eq. 17).
 
 Device path: the caller's ``blur_op`` and ``regularizer`` apply the
 convolutions and the smoothness operator (three convolutions per iteration
-at steady state); every other pass is one fused kernel of libdecon_b200
+at steady state; for ``Hessian3D`` the Gram matrix and energy of its images
+are evaluated on the fly by ``decon_nlcg_hess_*`` and only C^T C f is formed);
+every other pass is one fused kernel of libdecon_b200
 (``decon_nlcg_*``) with FP64 sums.  The Newton refinements update the step
 length on the device, so an iteration synchronises with the host once: each
 step is carried through to the new gradient speculatively and kept only if
@@ -31,6 +33,7 @@ import torch
 
 from .. import _lib
 from ._device import empty, fill, stream, to_device
+from .linops import Hessian3D
 
 __all__ = ["NLCGResult", "nlcg_objective", "nlcg_gradient", "nlcg_hessian_quadform",
            "nlcg_step_length", "i_divergence_between", "nlcg_with_operator", "nlcg_solver"]
@@ -116,6 +119,22 @@ def _use_reg(regularizer, reg_weight):
     return regularizer is not None and float(reg_weight) != 0.0
 
 
+def _fused(reg, x) -> bool:
+    """Hessian3D on a 3-D object: its Gram matrix and energy are evaluated on
+    the fly (decon_nlcg_hess_*), the 6-component images are never stored."""
+    return isinstance(reg, Hessian3D) and x.dim() == 3
+
+
+def _energy(h, reg, x):
+    """||C x||^2 into the handle's regulariser slot."""
+    if _fused(reg, x):
+        _lib.call("decon_nlcg_hess_energy", h.h, _lib.ptr(x), _lib.i64arr(tuple(x.shape)),
+                  C.c_float(reg.r), stream())
+    else:
+        cx = _fwd(reg, x)
+        _lib.call("decon_nlcg_energy", h.h, _lib.ptr(cx), cx.numel(), stream())
+
+
 def nlcg_objective(s, blur_op, observed, background: float = 0.0, regularizer=None,
                    reg_weight: float = 0.0, eps: float = 1e-10) -> float:
     """phi(s) = sum(Kf) - sum(g ln(Kf + b)) + beta ||C f||^2, f = s^2 (nlcg_mlx.py:118-134)."""
@@ -128,8 +147,7 @@ def nlcg_objective(s, blur_op, observed, background: float = 0.0, regularizer=No
     _lib.call("decon_nlcg_model", h.h, _lib.ptr(m), _lib.ptr(g), C.c_float(eps), None, g.numel(),
               stream())
     if use_reg:
-        cf = _fwd(regularizer, f)
-        _lib.call("decon_nlcg_energy", h.h, _lib.ptr(cf), cf.numel(), stream())
+        _energy(h, regularizer, f)
     return float(_objective(h.read(), float(reg_weight), use_reg))
 
 
@@ -187,8 +205,7 @@ def nlcg_hessian_quadform(s, d, blur_op, observed, background: float = 0.0, regu
     q = h.read()["quad"]
     quad = 4.0 * q[0] + 2.0 * q[1]
     if use_reg:
-        csd = _fwd(regularizer, sd)
-        _lib.call("decon_nlcg_energy", h.h, _lib.ptr(csd), csd.numel(), stream())
+        _energy(h, regularizer, sd)
         _lib.call("decon_nlcg_quad", h.h, _lib.ptr(g), _lib.ptr(m), _lib.ptr(ksd), g.numel(),
                   _lib.ptr(ctcf), _lib.ptr(d), d.numel(), C.c_float(eps), stream())
         sc = h.read()
@@ -205,16 +222,21 @@ def _products(h, mode, gamma, s, d, r):
     return d_out, sd, dd
 
 
-def _line(h, s, d_sd_dd, f_cf, m, g, blur_op, regularizer, b, beta, use_reg, newton_iters, eps):
-    """K(sd), K(dd) [, the regulariser's Gram matrix] and the Newton refinements."""
+def _line(h, s, d_sd_dd, f, cf, m, g, blur_op, regularizer, b, beta, use_reg, newton_iters, eps):
+    """K(sd), K(dd) [, the regulariser's Gram matrix of C f, C(sd), C(dd); cf =
+    C f when the images are materialised] and the Newton refinements."""
     _, sd, dd = d_sd_dd
     ksd = _fwd(blur_op, sd)
     kdd = _fwd(blur_op, dd)
     if use_reg:
-        csd = _fwd(regularizer, sd)
-        cdd = _fwd(regularizer, dd)
-        _lib.call("decon_nlcg_gram", h.h, _lib.ptr(f_cf), _lib.ptr(csd), _lib.ptr(cdd), csd.numel(),
-                  stream())
+        if _fused(regularizer, f):
+            _lib.call("decon_nlcg_hess_gram", h.h, _lib.ptr(f), _lib.ptr(sd), _lib.ptr(dd),
+                      _lib.i64arr(tuple(f.shape)), C.c_float(regularizer.r), stream())
+        else:
+            csd = _fwd(regularizer, sd)
+            cdd = _fwd(regularizer, dd)
+            _lib.call("decon_nlcg_gram", h.h, _lib.ptr(cf), _lib.ptr(csd), _lib.ptr(cdd), csd.numel(),
+                      stream())
     _lib.call("decon_nlcg_newton", h.h, _lib.ptr(m), _lib.ptr(ksd), _lib.ptr(kdd), _lib.ptr(g),
               C.c_float(b), C.c_float(eps), C.c_double(beta), int(use_reg), int(newton_iters),
               g.numel(), stream())
@@ -233,8 +255,8 @@ def nlcg_step_length(s, d, f, m, blur_op, observed, background: float = 0.0, reg
     use_reg = _use_reg(regularizer, reg_weight)
     h = _Scalars()
     prods = _products(h, 0, 0.0, s, d, None)
-    cf = _fwd(regularizer, f) if use_reg else None
-    ksd, kdd = _line(h, s, prods, cf, m, g, blur_op, regularizer, b, beta, use_reg, newton_iters, eps)
+    cf = _fwd(regularizer, f) if use_reg and not _fused(regularizer, f) else None
+    ksd, kdd = _line(h, s, prods, f, cf, m, g, blur_op, regularizer, b, beta, use_reg, newton_iters, eps)
     m_lam = empty(g.shape)
     _lib.call("decon_nlcg_accept", h.h, _lib.ptr(m), _lib.ptr(ksd), _lib.ptr(kdd), _lib.ptr(g),
               C.c_float(b), C.c_float(eps), _lib.ptr(m_lam), None, g.numel(), None, None, None, None,
@@ -284,10 +306,14 @@ def nlcg_with_operator(observed, blur_op, num_iter: int = 50, background: float 
     m = _model(blur_op, f, b)
     if tuple(m.shape) != tuple(g.shape):
         raise ValueError(f"blur_op.forward produced {tuple(m.shape)}, observed is {tuple(g.shape)}")
+    fused = use_reg and _fused(reg, f)
     cf = None
     if use_reg:
-        cf = _fwd(reg, f)
-        _lib.call("decon_nlcg_energy", h.h, _lib.ptr(cf), cf.numel(), stream())
+        if fused:
+            _energy(h, reg, f)
+        else:
+            cf = _fwd(reg, f)
+            _lib.call("decon_nlcg_energy", h.h, _lib.ptr(cf), cf.numel(), stream())
     r, _, _ = _gradient_parts(h, s, f, m, g, blur_op, reg, beta, use_reg, eps)
     sc = h.read()
     phi0 = _objective(sc, beta, use_reg)
@@ -298,7 +324,7 @@ def nlcg_with_operator(observed, blur_op, num_iter: int = 50, background: float 
         """One trial step along d (mode 0) or r + gamma d (mode 1), carried
         through to the new gradient; None if rejected (nlcg_mlx.py:462-489)."""
         prods = _products(h, mode, gamma, s, d_in, r)
-        ksd, kdd = _line(h, s, prods, cf, m, g, blur_op, reg, b, beta, use_reg, newton_iters, eps)
+        ksd, kdd = _line(h, s, prods, f, cf, m, g, blur_op, reg, b, beta, use_reg, newton_iters, eps)
         d_used = prods[0]
         m_new = empty(g.shape)
         w_new = empty(g.shape)
@@ -309,9 +335,13 @@ def nlcg_with_operator(observed, blur_op, num_iter: int = 50, background: float 
                   _lib.ptr(d_used), _lib.ptr(s_new), _lib.ptr(f_new), no, stream())
         cf_new = ctcf_new = None
         if use_reg:
-            cf_new = _fwd(reg, f_new)
-            _lib.call("decon_nlcg_energy", h.h, _lib.ptr(cf_new), cf_new.numel(), stream())
-            ctcf_new = _adj(reg, cf_new)
+            if fused:
+                _energy(h, reg, f_new)
+                ctcf_new = _adj(reg, _fwd(reg, f_new))
+            else:
+                cf_new = _fwd(reg, f_new)
+                _lib.call("decon_nlcg_energy", h.h, _lib.ptr(cf_new), cf_new.numel(), stream())
+                ctcf_new = _adj(reg, cf_new)
         ktw = _adj(blur_op, w_new)
         r_new = empty(s.shape)
         _lib.call("decon_nlcg_gradient", h.h, _lib.ptr(s_new), _lib.ptr(f_new), _lib.ptr(f),

@@ -177,6 +177,13 @@ int decon_nlcg_energy(decon_nlcg* h, const float* a, int64_t n, void* stream);
 int decon_nlcg_gradient(decon_nlcg* h, const float* s, const float* f, const float* f_prev,
                         const float* ktw, const float* ctcf, float c4b, float eps, float* r, int64_t n,
                         void* stream);
+/* Hessian3D regulariser (spacing ratio r) evaluated on the fly, its images
+ * never stored: the Gram matrix of H f, H(s d), H(d^2) (replaces
+ * decon_nlcg_gram on materialised images) and ||H f||^2 (decon_nlcg_energy).
+ * shape = (nz, ny, nx) of the object arrays. */
+int decon_nlcg_hess_gram(decon_nlcg* h, const float* f, const float* sd, const float* dd,
+                         const int64_t shape[3], float r, void* stream);
+int decon_nlcg_hess_energy(decon_nlcg* h, const float* f, const int64_t shape[3], float r, void* stream);
 /* sum (g / max(m^2, eps)) ksd^2 and sum a d^2 (nlcg_hessian_quadform, :181-193). */
 int decon_nlcg_quad(decon_nlcg* h, const float* g, const float* m, const float* ksd, int64_t nd,
                     const float* a, const float* d, int64_t no, float eps, void* stream);
