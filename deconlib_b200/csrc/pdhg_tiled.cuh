@@ -373,22 +373,18 @@ __global__ void __launch_bounds__(256) k_hess_regloss_p(PdhgDev* s, const float*
     put_slot(s, slot, acc);
 }
 
-// x_new = max(0, x - tau (A^T y1 + H^T y2)) with H^T y2 from staged planes:
-// components 0, 3, 4 (read at z -+ 1) in rings of three planes, components
-// 1, 2, 5 (read in plane z only) one plane each.
-__global__ void __launch_bounds__(256) k_hess_primal_t(PdhgDev* s, const float* __restrict__ xc,
-                                                       const float* __restrict__ aty,
-                                                       const float* __restrict__ y2,
-                                                       float* __restrict__ xn, Dims d, W6 w,
-                                                       int s_dx2, int s_xc2, int s_xn2) {
-    if (s->stop) return;
+// H^T y2 over this CTA's tiles from staged planes: components 0, 3, 4 (read
+// at z -+ 1) in rings of three planes, components 1, 2, 5 (read in plane z
+// only) one plane each, a one-plane register prefetch.  body(i, lt) receives
+// the adjoint at interior voxel i (the float operations of hess_adj_gen).
+template <class Body>
+__device__ __forceinline__ void hess_adj_walk(const float* __restrict__ y2, const Dims& d, const W6& w,
+                                              const Body& body) {
     __shared__ float rz[3][3][kPL];  // components 0, 3, 4
     __shared__ float pz[3][kPL];     // components 1, 2, 5
-    const float tau = (float)s->tau;
     const int64_t n = d.nz * d.ny * d.nx, plane = d.ny * d.nx;
     const TileGeo g(d);
     const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-    double dx2 = 0.0, xc2 = 0.0, xn2 = 0.0;
     auto comp = [&](int c) { return [=](int64_t i) -> float { return __ldg(y2 + c * n + i); }; };
     const auto c0 = comp(0), c1 = comp(1), c2 = comp(2), c3 = comp(3), c4 = comp(4), c5 = comp(5);
     for (int64_t tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
@@ -449,25 +445,45 @@ __global__ void __launch_bounds__(256) k_hess_primal_t(PdhgDev* s, const float* 
             if (in) {
                 e.zlo = z == 0 ? -1.f : 1.f;
                 e.zhi = z == d.nz - 1 ? -1.f : 1.f;
-                const int64_t i = z * plane + ipl;
-                const float a = xc[i];
                 const float lt = hess_adj_smem(rz[0][sp], rz[0][sc], rz[0][sn], pz[0], pz[1],
                                                rz[1][sp], rz[1][sn], rz[2][sp], rz[2][sn], pz[2],
                                                ty + 1, tx + 1, e, w.w);
-                const float gr = aty[i] + lt;
-                const float v = fmaxf(a - tau * gr, 0.f);
-                xn[i] = v;
-                const float dd = v - a;
-                dx2 += (double)dd * dd;
-                xc2 += (double)a * a;
-                xn2 += (double)v * v;
+                body(z * plane + ipl, lt);
             }
             __syncthreads();
         }
     }
+}
+
+// x_new = max(0, x - tau (A^T y1 + H^T y2)) and its FP64 sums.
+__global__ void __launch_bounds__(256) k_hess_primal_t(PdhgDev* s, const float* __restrict__ xc,
+                                                       const float* __restrict__ aty,
+                                                       const float* __restrict__ y2,
+                                                       float* __restrict__ xn, Dims d, W6 w,
+                                                       int s_dx2, int s_xc2, int s_xn2) {
+    if (s->stop) return;
+    const float tau = (float)s->tau;
+    double dx2 = 0.0, xc2 = 0.0, xn2 = 0.0;
+    hess_adj_walk(y2, d, w, [&](int64_t i, float lt) {
+        const float a = xc[i];
+        const float gr = aty[i] + lt;
+        const float v = fmaxf(a - tau * gr, 0.f);
+        xn[i] = v;
+        const float dd = v - a;
+        dx2 += (double)dd * dd;
+        xc2 += (double)a * a;
+        xn2 += (double)v * v;
+    });
     put_slot(s, s_dx2, dx2);
     put_slot(s, s_xc2, xc2);
     put_slot(s, s_xn2, xn2);
+}
+
+// Hessian3D.adjoint of six stored components on the staged tile walk:
+// bit-identical to the per-voxel global-memory form (hess_adj_gen).
+__global__ void __launch_bounds__(256) k_hessian_adj_t(const float* __restrict__ hw, float* __restrict__ out,
+                                                       Dims d, W6 w) {
+    hess_adj_walk(hw, d, w, [&](int64_t i, float lt) { out[i] = lt; });
 }
 
 }  // namespace dk

@@ -499,6 +499,13 @@ __global__ void k_clamp_min(const float* __restrict__ a, float lo, float* __rest
         out[i] = fmaxf(a[i], lo);
 }
 
+int hess_adjoint_tiled(const float* hw, float* out, const Dims& d, const W6& w, cudaStream_t st) {
+    const int64_t grid = std::min<int64_t>(TileGeo(d).ntiles, (int64_t)sm_count() * 4);
+    k_hessian_adj_t<<<(unsigned)std::max<int64_t>(grid, 1), 256, 0, st>>>(hw, out, d, w);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
 }  // namespace dk
 
 using namespace dk;

@@ -166,4 +166,8 @@ struct W6 {
     float w[6];
 };
 
+// Hessian3D.adjoint of six stored components hw[c * n + i] on the tiled,
+// staged walk of the fused PDHG kernels (solvers.cu).
+int hess_adjoint_tiled(const float* hw, float* out, const Dims& d, const W6& w, cudaStream_t st);
+
 }  // namespace dk
