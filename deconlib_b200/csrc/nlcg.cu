@@ -327,16 +327,21 @@ __global__ void __launch_bounds__(256) k_nlcg_hess_gram(const float* __restrict_
         d, w, [&](int64_t i) { return Fields3{__ldg(f + i), __ldg(sd + i), __ldg(dd + i)}; },
         [](const Fields3& r, int k) { return k == 0 ? r.a : (k == 1 ? r.b : r.c); },
         [&](int64_t, const float (*h)[6]) {
+            // the six-component products of one voxel in FP32, the sum over
+            // voxels in FP64
+            float p[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
             for (int q = 0; q < 6; ++q) {
-                const double x = h[0][q], y = h[1][q], z = h[2][q];
-                v[0] += x * x;
-                v[1] += x * y;
-                v[2] += x * z;
-                v[3] += y * y;
-                v[4] += y * z;
-                v[5] += z * z;
+                const float x = h[0][q], y = h[1][q], z = h[2][q];
+                p[0] = fmaf(x, x, p[0]);
+                p[1] = fmaf(x, y, p[1]);
+                p[2] = fmaf(x, z, p[2]);
+                p[3] = fmaf(y, y, p[3]);
+                p[4] = fmaf(y, z, p[4]);
+                p[5] = fmaf(z, z, p[5]);
             }
+#pragma unroll
+            for (int q = 0; q < 6; ++q) v[q] += (double)p[q];
         });
     fold_last<6>(v, part, &dev->ticket, dev->gram);
 }
@@ -347,11 +352,10 @@ __global__ void __launch_bounds__(256) k_nlcg_hess_energy(const float* __restric
     hess_zwalk<1>(
         d, w, [&](int64_t i) { return __ldg(f + i); }, [](const float& r, int) { return r; },
         [&](int64_t, const float (*h)[6]) {
+            float p = 0.f;
 #pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                const double x = h[0][q];
-                v[0] += x * x;
-            }
+            for (int q = 0; q < 6; ++q) p = fmaf(h[0][q], h[0][q], p);
+            v[0] += (double)p;
         });
     fold_last<1>(v, part, &dev->ticket, dev->reg);
 }
