@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include <map>
 #include "conv_impl.cuh"
 
 namespace dk {
@@ -38,6 +39,39 @@ int fail(int code, const char* fmt, ...) {
     return code;
 }
 
+static cudaStream_t setup_stream() {
+    static std::mutex mu;
+    static std::map<int, cudaStream_t> streams;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = streams.find(dev);
+    if (it != streams.end()) return it->second;
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    streams[dev] = s;
+    return s;
+}
+
+int upload_blocking(void* dst, const void* src, size_t bytes) {
+    const cudaStream_t s = setup_stream();
+    if (!s) return fail(DECON_ERR_CUDA, "set-up stream creation failed");
+    DK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    DK_CUDA(cudaStreamSynchronize(s));
+    return DECON_OK;
+}
+
+int memset_blocking(void* dst, int value, size_t bytes) {
+    const cudaStream_t s = setup_stream();
+    if (!s) return fail(DECON_ERR_CUDA, "set-up stream creation failed");
+    DK_CUDA(cudaMemsetAsync(dst, value, bytes, s));
+    DK_CUDA(cudaStreamSynchronize(s));
+    return DECON_OK;
+}
+
 int sm_count() {
     static int cached[64] = {0};
     int dev = 0;
@@ -62,7 +96,7 @@ static int make_twiddles(int L, float2** out) {
         h[m] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
     DK_CUDA(cudaMalloc(out, h.size() * sizeof(float2)));
-    DK_CUDA(cudaMemcpy(*out, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    DK_TRY(upload_blocking(*out, h.data(), h.size() * sizeof(float2)));
     return DECON_OK;
 }
 

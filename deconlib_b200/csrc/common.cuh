@@ -68,6 +68,16 @@ inline int64_t round_up(int64_t a, int64_t b) { return cdiv(a, b) * b; }
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// Copy / fill device memory and return only once the bytes are in place,
+// visible to work on every stream.  For set-up data that several streams may
+// read (twiddle tables, fresh solver state): a plain cudaMemcpy from pageable
+// memory or a cudaMemset runs on the legacy default stream, which does not
+// order against non-blocking streams, and may still be in flight when another
+// stream's kernel reads the buffer.  Uses a private non-blocking stream per
+// device and synchronises only that stream.
+int upload_blocking(void* dst, const void* src, size_t bytes);
+int memset_blocking(void* dst, int value, size_t bytes);
+
 // ---- complex helpers -------------------------------------------------------
 __host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) {
     return make_float2(a.x + b.x, a.y + b.y);

@@ -421,7 +421,7 @@ int decon_nlcg_create(decon_nlcg** out) {
         nl_free(h);
         return fail(DECON_ERR_OOM, "decon_nlcg_create: allocation failed");
     }
-    if (cudaMemset(h->dev, 0, sizeof(NlcgDev)) != cudaSuccess) {
+    if (memset_blocking(h->dev, 0, sizeof(NlcgDev)) != DECON_OK) {
         nl_free(h);
         return fail(DECON_ERR_CUDA, "decon_nlcg_create: memset failed");
     }

@@ -125,7 +125,8 @@ __global__ void __launch_bounds__(kFftThreads) k_psf_rows(const PsfRowArgs a) {
 }
 
 // Twiddle tables W_L^m = exp(-2 pi i m / L) per (device, L), kept for the
-// life of the process (the first call for a length uploads it synchronously).
+// life of the process (the first call for a length uploads it and waits for
+// the copy, so every stream may read the table).
 static int psf_twiddles(int L, const float2** out) {
     static std::mutex mu;
     static std::map<std::pair<int, int>, float2*> cache;
@@ -141,7 +142,7 @@ static int psf_twiddles(int L, const float2** out) {
         }
         float2* d = nullptr;
         DK_CUDA(cudaMalloc(&d, h.size() * sizeof(float2)));
-        if (cudaMemcpy(d, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
+        if (upload_blocking(d, h.data(), h.size() * sizeof(float2)) != DECON_OK) {
             cudaFree(d);
             return fail(DECON_ERR_CUDA, "decon_pupil_to_psf: twiddle upload failed");
         }

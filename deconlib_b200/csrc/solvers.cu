@@ -586,12 +586,13 @@ int decon_pdhg_create(int num_iter, double step_scale, double delta, double eta,
     double* base = reinterpret_cast<double*>(reinterpret_cast<char*>(h->mem) + sizeof(PdhgDev));
     const PdhgDev d = pdhg_initial(num_iter, step_scale, delta, eta, tol, min_iter, patience, base, nh);
     h->dev = reinterpret_cast<PdhgDev*>(h->mem);
-    e = cudaMemcpy(h->dev, &d, sizeof(d), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(base, 0, (size_t)(4 * nh + kPdhgSlots * kPdhgGrid) * sizeof(double));
-    if (e != cudaSuccess) {
+    // complete before the call returns: the solve may run on any stream
+    int st = upload_blocking(h->dev, &d, sizeof(d));
+    if (st == DECON_OK) st = memset_blocking(base, 0, (size_t)(4 * nh + kPdhgSlots * kPdhgGrid) * sizeof(double));
+    if (st != DECON_OK) {
         cudaFree(h->mem);
         delete h;
-        return fail(DECON_ERR_CUDA, "PDHG state init failed: %s", cudaGetErrorString(e));
+        return st;
     }
     *out = h;
     return DECON_OK;

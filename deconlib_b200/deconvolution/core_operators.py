@@ -112,6 +112,23 @@ class Crop:
 # ---------------------------------------------------------------------------
 
 _BANDS = {}
+_TABLE_STREAM = {}
+
+
+def _upload_table(a: np.ndarray) -> torch.Tensor:
+    """A device copy of a host table that every stream may read at once: the
+    copy runs on a private stream that is synchronised before the table is
+    cached.  (Uploaded on the caller's stream, a table first used by one job
+    could be read by a concurrent job on another stream before its copy
+    landed.)"""
+    dev = torch.cuda.current_device()
+    st = _TABLE_STREAM.get(dev)
+    if st is None:
+        st = _TABLE_STREAM[dev] = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        t = torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
+    st.synchronize()
+    return t
 
 
 def banded_overlap_weights(n_large: int, n_small: int):
@@ -128,7 +145,7 @@ def _device_band(n_large: int, n_small: int, scale: float = 1.0):
             # FractionalAreaUpsample pre-scales by n_small / n_large in float32
             w_f = (w_f * np.float32(scale)).astype(np.float32)
             w_a = (w_a * np.float32(scale)).astype(np.float32)
-        hit = tuple(torch.from_numpy(np.ascontiguousarray(a)).to("cuda") for a in (i_f, w_f, i_a, w_a))
+        hit = tuple(_upload_table(a) for a in (i_f, w_f, i_a, w_a))
         _BANDS[key] = hit
     return hit
 
