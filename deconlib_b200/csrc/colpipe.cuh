@@ -211,6 +211,12 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
                 }
                 dft<R, +1>(v[h]);
             }
+            // The refill below is a TMA (async-proxy) write over what every
+            // thread just read through the generic proxy: each thread orders
+            // its reads before it with a proxy fence, then the barrier.
+            // Without the fence the refill could land under a slow warp's
+            // reads when other kernels share the SM.
+            if constexpr (OTF1) fence_proxy_async_smem();
             __syncthreads();
             if constexpr (OTF1) {
                 // every thread has read the OTF buffer: refill it for the next tile

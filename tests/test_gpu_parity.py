@@ -337,3 +337,29 @@ def test_long_x_axis_matches_fp64_fft(D, fx):
     c = D.LinearFFTConvolver(ker.astype(np.float32), n, fft_shape=f)
     got = cpu(c.forward(x.astype(np.float32)))
     assert rel(got, ref_f) < 2e-6
+
+
+def test_axial_pass_bit_identical_under_concurrent_streams(D):
+    # Convolutions whose axial pass runs the two-CTA pipelined kernel (Fz =
+    # 256), queued on four streams at once so that their CTAs share SMs, must
+    # give exactly the single-stream result: the kernel's TMA refill of its
+    # OTF buffer is ordered after every thread's reads by a proxy fence.
+    rng = np.random.default_rng(21)
+    shape = (128, 160, 96)
+    psf = rng.random(shape).astype(np.float32)
+    xs = [torch.from_numpy(rng.random(shape, dtype=np.float32)).cuda() for _ in range(4)]
+    convs = [D.LinearFFTConvolver(psf, shape) for _ in range(4)]
+    assert convs[0].fft_shape[0] == 256
+    ref = [(c.forward(x), c.adjoint(x)) for c, x in zip(convs, xs)]
+    torch.cuda.synchronize()
+    streams = [torch.cuda.Stream() for _ in range(4)]
+    for _ in range(6):
+        outs = []
+        for st, c, x in zip(streams, convs, xs):
+            st.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(st):
+                outs.append([(c.forward(x), c.adjoint(x)) for _ in range(3)])
+        torch.cuda.synchronize()
+        for (f0, a0), reps in zip(ref, outs):
+            for f, a in reps:
+                assert torch.equal(f, f0) and torch.equal(a, a0)
