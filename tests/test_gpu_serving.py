@@ -82,3 +82,37 @@ def test_realtime_arrivals_overlap_on_the_device():
     assert rep.max_concurrent >= 2
     for r in rep.results:
         assert r.finished >= r.admitted >= r.arrival - 1e-3
+
+
+def test_mix_with_the_two_cta_axial_pass_is_bit_identical():
+    """PDHG jobs whose axial canvas is 256 (object depth 128) run the two-CTA
+    pipelined axial kernel; served beside RL jobs on other streams (other
+    kernels sharing the SMs) every result must equal the job alone bit for
+    bit."""
+    from deconlib_b200 import synth
+    from deconlib_b200.serving import DeconServer, Job
+
+    rng = np.random.default_rng(7)
+    jobs = []
+    for i in range(4):
+        shp = (128, 64 + 16 * i, 96)
+        psf = synth.widefield_psf(shp, 0.05, 0.0425, depth=float(rng.uniform(0, 10)))
+        truth = synth.beads(shp, 60, rng)
+        obs = synth.poisson_observation(truth[::2, ::2, ::2] + 0.05, 400.0, 5.0, rng)
+        opts = dict(alpha=1e-3, regularization="hessian", sampling_factors=2.0,
+                    spacing=(0.05, 0.0425, 0.0425), tol=0.0)
+        jobs.append(Job(job_id=i, kind="pdhg", observed=obs, psf=psf, num_iter=40, arrival=0.0,
+                        background=5.0, options=opts))
+    for i in range(4, 8):
+        shp = (60 + 4 * i, 120, 100)
+        psf = synth.widefield_psf(shp, 0.1, 0.085)
+        truth = synth.beads(shp, 60, rng)
+        obs = synth.poisson_observation(truth + 0.05, 300.0, 5.0, rng)
+        jobs.append(Job(job_id=i, kind="rl", observed=obs, psf=psf, num_iter=40, arrival=0.0,
+                        background=5.0))
+    alone = [_alone(j) for j in jobs]
+    for _ in range(3):
+        rep = DeconServer(budget_bytes=150 * 10**9, max_active=8, chunk=4).run(jobs, realtime=False)
+        for job, res, (ref, iters) in zip(jobs, rep.results, alone):
+            assert res.iterations == iters
+            assert np.array_equal(res.restored, ref), (job.job_id, float(np.abs(res.restored - ref).max()))
