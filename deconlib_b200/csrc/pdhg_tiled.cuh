@@ -17,9 +17,11 @@
 // results equal the untiled kernels bit for bit.
 //
 // The primal update (k_hess_primal_t: six staged y2 components, x and
-// A^T y1) keeps a one-plane register prefetch and static three-plane rings:
-// eight CTAs fit an SM, and on the B200 this measured faster than the
-// pipelined form, whose six deep rings cost occupancy and issue slots.
+// A^T y1) keeps a one-plane register prefetch and static three-plane rings
+// (hess_adj_walk, shared with the standalone Hessian3D adjoint): two CTAs of
+// 116 registers per SM, which on the B200 measured faster than the pipelined
+// form (six deep rings cost occupancy and issue slots) and than 80- or
+// 64-register builds at three or four CTAs per SM.
 //
 // ||H (x_new - x)||^2 (k_hess_dk_r) walks z in registers instead
 // (hess_zwalk): each thread keeps three planes of its halo positions and
@@ -34,7 +36,6 @@
 #include "zwalk.cuh"
 
 namespace dk {
-
 
 // Hessian components at tile-local (ly, lx) (1-based, halo at 0 and kT+1)
 // from staged planes: clamping is already in the staged values, so the taps
