@@ -226,8 +226,18 @@ __global__ void __launch_bounds__(256) k_step(PdhgDev* s) {
         const int slot = warp == 0 ? kSlotDx2 : warp == 1 ? kSlotXc2 : warp == 2 ? kSlotXn2
                        : warp == 3 ? kSlotDA2 : kSlotDL2;
         const double* p = s->partials + slot * kPdhgGrid;
+        // all of a lane's partials loaded at once, then summed in index order
+        // (the same sums as a sequential loop, without 19 dependent loads)
+        constexpr int kPer = (kPdhgGrid + 31) / 32;
+        double q[kPer];
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int i = lane + 32 * u;
+            q[u] = i < kPdhgGrid ? p[i] : 0.0;
+        }
         double v = 0.0;
-        for (int i = lane; i < kPdhgGrid; i += 32) v += p[i];
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) v += q[u];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) red[warp] = v;
     }
