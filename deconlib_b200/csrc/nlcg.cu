@@ -71,9 +71,20 @@ __device__ bool fold_last(double (&v)[NS], double* __restrict__ part, unsigned* 
     if (!last) return false;
     __threadfence();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int G = (int)gridDim.x;
     for (int s = warp; s < NS; s += blockDim.x >> 5) {
+        // eight of the lane's partials in flight at a time, summed in block order
         double acc = 0.0;
-        for (int b = lane; b < (int)gridDim.x; b += 32) acc += __ldcg(&part[s * gridDim.x + b]);
+        for (int b0 = lane; b0 < G; b0 += 32 * 8) {
+            double q[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int b = b0 + 32 * u;
+                q[u] = b < G ? __ldcg(&part[s * G + b]) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) acc += q[u];
+        }
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
         if (lane == 0) out[s] = acc;
     }
