@@ -561,13 +561,37 @@ def run_nlcg(D, iters=50):
     return out
 
 
-def zpass_bytes(n_shape, f_shape):
-    nz = n_shape[0]
+def zpass_bytes(n_shape, f_shape, fused):
+    """Algorithmic bytes of one launch of the axial pass: the fused Y / axial
+    pass reads and writes the kx-major spectrum S1 (Nz x Ny x Hx) and reads the
+    OTF; the unfused axial pass reads and writes S2 (Nz x Fy x Hx) and reads
+    the OTF.  Complex values are 8 bytes."""
+    nz, ny = n_shape[0], n_shape[1]
     fz, fy, fx = f_shape
     hx = fx // 2 + 1
-    hs = nz * fy * hx
     hf = fz * fy * hx
-    return 8 * (2 * hs + hf)  # read S2, read OTF, write S2
+    if fused:
+        return 8 * (2 * nz * ny * hx + hf)
+    return 8 * (2 * nz * fy * hx + hf)
+
+
+def conv_fused(lib, conv):
+    import ctypes as C
+
+    f = C.c_int()
+    lib.decon_conv_fused_yz(conv.plan, C.byref(f))
+    return bool(f.value)
+
+
+def pdhg_model_bytes(n_shape, m_shape, f_shape, c=8):
+    """Minimal bytes of one Hessian-PDHG iteration (linearity-cached, one
+    forward and one adjoint convolution, fused stencil): 32 M + 72 N +
+    8 c Hs + 2 c Hf, Hs = Nz Fy Hx, Hf = Fz Fy Hx."""
+    n = int(np.prod(n_shape))
+    m = int(np.prod(m_shape))
+    fz, fy, fx = f_shape
+    hx = fx // 2 + 1
+    return 32 * m + 72 * n + 8 * c * n_shape[0] * fy * hx + 2 * c * fz * fy * hx
 
 
 def profile_traffic(name):
@@ -660,12 +684,13 @@ def run_ours(args, ws, rank, local):
     info = runner.result()
     value = units / (ms / 1e3)
 
-    # roofline of the axial pass
-    z_bytes = zpass_bytes(OBJ, conv.fft_shape)
+    # roofline of the axial pass (fused Y / axial pass where the canvas allows)
+    fused = conv_fused(lib, conv)
+    z_bytes = zpass_bytes(OBJ, conv.fft_shape, fused)
     z_ms = ms_z.value / max(nz_launch.value, 1)
     hbm, src = peaks()
     achieved = z_bytes / (z_ms / 1e3) / 1e9
-    traffic = profile_traffic("zotf_pdhg_128x256x256")
+    traffic = profile_traffic("yz_pdhg_128x256x256" if fused else "zotf_pdhg_128x256x256")
 
     torch.cuda.synchronize()
     if ws > 1:
@@ -725,8 +750,15 @@ def run_ours(args, ws, rank, local):
             "l2": "inputs larger than L2 (OTF 285 MB, Hessian dual 201 MB per iteration)",
             "parallelism": f"replicas x{ws}",
         },
+        "iteration_model": {
+            "bytes": pdhg_model_bytes(OBJ, DATA, conv.fft_shape),
+            "hbm_frac": pdhg_model_bytes(OBJ, DATA, conv.fft_shape) / (ms / K / 1e3) / 1e9 / hbm,
+            "note": "SURVEY minimal-byte model of one PDHG iteration (FP32 spectra) / ms_per_step"},
         "roofline": {
-            "bound": "hbm", "kernel": "k_col_pipe<16,1,OTF> axial FFT x OTF x IFFT (lean, 2 CTAs/SM)",
+            "bound": "hbm",
+            "kernel": ("k_yz<512,256> fused Y FFT / axial FFT x OTF x IFFT / Y IFFT, one 8-CTA "
+                       "cluster per kx column" if fused else
+                       "k_col_pipe<16,1,OTF> axial FFT x OTF x IFFT (lean, 2 CTAs/SM)"),
             "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
             "peak_source": src, "traffic": traffic, "algorithmic_bytes_per_launch": z_bytes,
             "launch_ms": z_ms, "launches": nz_launch.value,
@@ -740,6 +772,7 @@ def run_ours(args, ws, rank, local):
         "gpu_launches": int(launches),
         "clocks": clk,
         "rl": {"value": rl_value, "unit": "voxel-iter/s", "ms_per_iter": ms_rl / K,
+               "fused_yz": conv_fused(lib, c_rl),
                "model_bytes_per_iter": rl_model_bytes,
                "hbm_frac_model": rl_model_bytes / (ms_rl / K / 1e3) / 1e9 / hbm,
                "zpass_ms": ms_rz.value / max(n_rz.value, 1),
@@ -802,23 +835,35 @@ def cpu_baseline_pdhg(psf, obs, iters=1):
                       f"{workers} threads; set-up excluded", "seconds_per_iter": dt}
 
 
+def _synth_standalone():
+    """deconlib_b200/synth.py loaded as a plain module (NumPy only), without
+    importing the package, so the reference arm's process maps none of this
+    repository's native libraries."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location(
+        "_bench_synth", os.path.join(ROOT, "deconlib_b200", "synth.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def run_reference(args, ws, rank, local):
+    """The reference's CPU path on this host: the NumPy restatement of
+    deconlib's PDHG loop (oracle/), inputs made by the same oracle.  No torch,
+    no CUDA, nothing of deconlib_b200 but its NumPy input generators."""
     if rank != 0:
         return
-    import torch
-    import deconlib_b200.deconvolution as D
+    from oracle import ops
 
-    if torch.cuda.is_available():
-        psf, obs = pdhg_inputs(D)
-    else:  # inputs only; the reference arm itself is CPU
-        from deconlib_b200 import synth
-        from oracle import ops
-
-        psf, truth = synth.pdhg_workload(OBJ, SPACING_PD, seed=2)
-        fwd = ops.compose(ops.FractionalAreaDownsample(2.0, in_shape=OBJ),
-                          ops.LinearFFTConvolver(psf, OBJ))
-        obs = synth.poisson_observation(fwd.forward(truth), 500.0, 5.0, np.random.default_rng(3))
+    synth = _synth_standalone()
+    psf, truth = synth.pdhg_workload(OBJ, SPACING_PD, seed=2)
+    fwd = ops.compose(ops.FractionalAreaDownsample(2.0, in_shape=OBJ, dtype=np.float64),
+                      ops.LinearFFTConvolver(psf, OBJ, dtype=np.float64))
     workers = len(os.sched_getaffinity(0))
+    ops.set_fft_workers(workers)
+    obs = synth.poisson_observation(fwd.forward(truth.astype(np.float64)), 500.0, 5.0,
+                                    np.random.default_rng(3))
     solvers, y, A, reg, x0 = _oracle_pdhg_setup(psf, obs, workers)
     W = min(args.warmup, 1)
     K = max(1, min(args.steps, 3))
@@ -830,9 +875,12 @@ def run_reference(args, ws, rank, local):
     dt = time.perf_counter() - t0
     value = int(np.prod(OBJ)) * K / dt
     sample = (f"{K} timed PDHG iteration(s) (+{W} warm-up) of the NumPy restatement of the "
-              f"reference at 128x256x256, scipy.fft with {workers} threads")
+              f"reference at 128x256x256, scipy.fft with {workers} threads; the CPU arm times "
+              f"min(steps, 3) iterations and min(warmup, 1) warm-up (asked: {args.steps} / "
+              f"{args.warmup}), so that it ends within minutes")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "voxel-iter/s",
-            "n_gpus": ws, "steps": K, "warmup": W, "ms_per_step": dt / K * 1e3,
+            "n_gpus": ws, "steps": K, "warmup": W, "steps_requested": args.steps,
+            "warmup_requested": args.warmup, "ms_per_step": dt / K * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": {"workload": "hessian_pdhg_sampling2_object128x256x256_data64x128x128"},
             "cpu_baseline": {"value": value, "unit": "voxel-iter/s", "cores": workers,

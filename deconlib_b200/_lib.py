@@ -31,6 +31,15 @@ _SIGS = {
     "decon_version": (C.c_int, []),
     "decon_launch_count": (_i64, []),
     "decon_device_status": (C.c_int, [_p]),
+    "decon_device_status_clear": (C.c_int, [_p]),
+    "decon_pdhg_solver_create": (C.c_int, [_p, _p, _i64p, _dp, C.c_float, C.c_int, _p, C.c_float,
+                                           C.c_float, C.c_int, C.c_int, C.c_double, C.c_double,
+                                           C.c_double, C.c_int, C.c_int, C.c_int, _p, C.POINTER(_p)]),
+    "decon_pdhg_run": (C.c_int, [_p, C.c_int, _p]),
+    "decon_pdhg_solver_x": (C.c_int, [_p, _p, _p]),
+    "decon_pdhg_solver_state": (C.c_int, [_p, C.POINTER(_p), C.POINTER(C.c_int)]),
+    "decon_pdhg_solver_destroy": (C.c_int, [_p]),
+    "decon_test_wait_timeout": (C.c_int, [C.c_uint, _p]),
     "decon_next_smooth": (_i64, [_i64]),
     "decon_fast_padded_shape": (C.c_int, [C.c_int, _i64p, _i64p, _i64p, _i64p]),
     "decon_conv_create": (C.c_int, [_p, _i64p, _i64p, _i64p, C.c_int, _p, C.POINTER(_p)]),
@@ -38,6 +47,7 @@ _SIGS = {
     "decon_conv_set_kernel": (C.c_int, [_p, _p, C.c_int, _p]),
     "decon_conv_set_precision": (C.c_int, [_p, C.c_int, _p]),
     "decon_conv_norm_sq": (C.c_int, [_p, _dp]),
+    "decon_conv_fused_yz": (C.c_int, [_p, C.POINTER(C.c_int)]),
     "decon_conv_shape": (C.c_int, [_p, _i64p, _i64p]),
     "decon_conv_get_otf": (C.c_int, [_p, _p, _p]),
     "decon_conv_forward": (C.c_int, [_p, _p, _p, _p]),
@@ -108,6 +118,8 @@ _SIGS = {
     "decon_pdhg_set_stop": (C.c_int, [_p, C.c_int, _p]),
     "decon_pdhg_hess_dual": (C.c_int, [_p, _p, _p, _p, _i64p, C.c_float, C.c_float, C.c_int, _p]),
     "decon_pdhg_hess_primal": (C.c_int, [_p, _p, _p, _p, _p, _i64p, C.c_float, _p]),
+    "decon_pdhg_hess_dual_primal": (C.c_int, [_p, _p, _p, _p, _p, _p, _p, _i64p, C.c_float,
+                                              C.c_float, C.c_int, _p]),
     "decon_pdhg_hess_dk": (C.c_int, [_p, _p, _p, _i64, _p, _p, _i64p, C.c_float, _p]),
     "decon_pdhg_hess_loss": (C.c_int, [_p, _p, _p, C.c_float, C.c_int, _i64, _p, _i64p, C.c_float,
                                        C.c_int, C.c_double, C.c_int, _p]),

@@ -102,6 +102,7 @@ static int make_twiddles(int L, float2** out) {
 
 static void free_plan(ConvPlan* p) {
     if (!p) return;
+    cudaFree(p->otft);
     cudaFree(p->otf16);
     cudaFree(p->otf_inv);
     cudaFree(p->otf);
@@ -255,6 +256,7 @@ static int build_otf(decon_conv* p, const float* kernel, int normalize, cudaStre
     if (e != cudaSuccess) return fail(DECON_ERR_CUDA, "OTF build failed: %s", cudaGetErrorString(e));
     p->norm_sq = nrm;
     if (p->precision == 1) DK_TRY(quantize_otf(*p, s));
+    DK_TRY(build_otf_kmajor(*p, s));
     return DECON_OK;
 }
 
@@ -339,6 +341,13 @@ static int conv_create_impl(const float* kernel, const int64_t kshape[3],
         delete p;
         return st;
     }
+    // fused Y / axial pass: the kx-major OTF copy (linear convolutions only)
+    if (!circular && yz_supported(p->N, p->F) && getenv("DECON_NO_YZ") == nullptr &&
+        (st = dev_alloc((void**)&p->otft, (size_t)p->Hx * Fy * Fz * sizeof(float2), "kx-major OTF"))) {
+        free_plan(p);
+        delete p;
+        return st;
+    }
     // TMA tensor maps for the strided column passes (power-of-two lengths
     // <= 512, 16-column tiles).  DECON_NO_TMA=1 selects the plain-load kernels.
     {
@@ -415,6 +424,12 @@ int decon_conv_destroy(decon_conv* p) {
     free_plan(p);
     if (cur != p->device) cudaSetDevice(cur);
     delete p;
+    return DECON_OK;
+}
+
+int decon_conv_fused_yz(const decon_conv* p, int* out) {
+    if (!p || !out) return fail(DECON_ERR_NULL, "null pointer");
+    *out = use_yz(*p) ? 1 : 0;
     return DECON_OK;
 }
 

@@ -29,6 +29,7 @@
 #include "tma.cuh"
 #include "colpipe.cuh"
 #include "xpass.cuh"
+#include "yzpass.cuh"
 
 namespace dk {
 
@@ -292,6 +293,41 @@ extern "C" int decon_device_status(void* stream) {
     return DECON_OK;
 }
 
+extern "C" int decon_device_status_clear(void* stream) {
+    using namespace dk;
+    DK_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    const int zero = 0;
+    DK_CUDA(cudaMemcpyToSymbol(g_wait_timeout, &zero, sizeof(int)));
+    return DECON_OK;
+}
+
+namespace dk {
+
+// One CTA waits, through the kernels' own bounded wait, on an mbarrier that
+// no thread arrives at and no copy completes: every poll fails, the wait
+// gives up after `polls` polls, raises g_wait_timeout and the CTA returns.
+// Nothing is in flight and nothing is written but the flag.
+__global__ void k_wait_probe(unsigned polls) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_proxy_async_smem();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) (void)mbar_wait_bounded(&bar, 0, polls);
+}
+
+}  // namespace dk
+
+extern "C" int decon_test_wait_timeout(unsigned polls, void* stream) {
+    using namespace dk;
+    if (polls == 0 || polls > (1u << 16))
+        return fail(DECON_ERR_VALUE, "decon_test_wait_timeout: polls must be in [1, 65536]");
+    k_wait_probe<<<1, 32, 0, as_stream(stream)>>>(polls);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
 extern "C" int decon_profile_start(int class_mask) {
     dk::g_prof.mask = class_mask;
     dk::g_prof.used = 0;
@@ -317,8 +353,9 @@ extern "C" int decon_profile_stop(double* ms_total, int64_t* launches) {
 namespace dk {
 
 int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cval, float bg,
-                int64_t nz_rows, float2* out, cudaStream_t st) {
+                int64_t nz_rows, float2* out, cudaStream_t st, int64_t kstride) {
     XR2CArgs a{};
+    a.kstride = kstride;
     a.in = in;
     a.cval = cval;
     a.bg = bg;
@@ -424,6 +461,7 @@ int launch_xc2r(const ConvPlan& p, int epi, const float2* in, Win3 win, float* o
     a.aux1 = aux1;
     a.bg = bg;
     a.partials = partials;
+    a.kstride = use_yz(p) ? p.N[0] * p.N[1] : 0;
     {
         const int L = a.ax.L;
         a.fd_L = make_fastdiv(L);
@@ -613,10 +651,105 @@ static int launch_col_tma(const ConvPlan& p, const Axis& ax, int mode, const CUt
                   otf ? PROF_ZOTF : PROF_COL);
 }
 
-// Forward spectrum: x (window in N-space) -> S2 (after the Y pass).
+// ---------------------------------------------------------------------------
+// fused Y / axial pass (yzpass.cuh)
+// ---------------------------------------------------------------------------
+
+bool yz_supported(const int64_t N[3], const int64_t F[3]) {
+    const bool fy = F[1] == 256 || F[1] == 512, fz = F[0] == 128 || F[0] == 256;
+    return fy && fz && N[1] <= F[1] / 2 && N[0] <= F[0] / 2 && N[1] % 2 == 0 && N[0] >= 1 &&
+           N[1] >= 2;
+}
+
+bool use_yz(const ConvPlan& p) {
+    return p.otft != nullptr && p.precision == 0 && getenv("DECON_NO_YZ") == nullptr;
+}
+
+// out[(kx * Fy + ky) * Fz + kz] = otf[(kz * Fy + ky) * P + kx]: 32 x 32 tiles
+// of (kz, kx) per ky through shared memory.
+__global__ void k_otf_kmajor(const float2* __restrict__ otf, int Fz, int Fy, int64_t P, int Hx,
+                             float2* __restrict__ out) {
+    __shared__ float2 t[32][33];
+    const int ky = blockIdx.z;
+    const int kx0 = blockIdx.x * 32, kz0 = blockIdx.y * 32;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int kz = kz0 + i, kx = kx0 + threadIdx.x;
+        if (kz < Fz && kx < Hx) t[i][threadIdx.x] = otf[((int64_t)kz * Fy + ky) * P + kx];
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int kx = kx0 + i, kz = kz0 + threadIdx.x;
+        if (kz < Fz && kx < Hx) out[((int64_t)kx * Fy + ky) * Fz + kz] = t[threadIdx.x][i];
+    }
+}
+
+int build_otf_kmajor(const ConvPlan& p, cudaStream_t st) {
+    if (!p.otft) return DECON_OK;
+    const dim3 grid((unsigned)cdiv(p.Hx, 32), (unsigned)cdiv(p.F[0], 32), (unsigned)p.F[1]);
+    k_otf_kmajor<<<grid, dim3(32, 8), 0, st>>>(p.otf, (int)p.F[0], (int)p.F[1], p.P, (int)p.Hx, p.otft);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
+template <int FY, int FZ>
+static void* pick_yz_fz(bool adjoint) {
+    return adjoint ? (void*)k_yz<FY, FZ, COL_OTF_CONJ> : (void*)k_yz<FY, FZ, COL_OTF>;
+}
+
+static void* pick_yz(int64_t Fy, int64_t Fz, bool adjoint) {
+    if (Fy == 512 && Fz == 256) return pick_yz_fz<512, 256>(adjoint);
+    if (Fy == 512 && Fz == 128) return pick_yz_fz<512, 128>(adjoint);
+    if (Fy == 256 && Fz == 256) return pick_yz_fz<256, 256>(adjoint);
+    if (Fy == 256 && Fz == 128) return pick_yz_fz<256, 128>(adjoint);
+    return nullptr;
+}
+
+// Clusters of k_yz resident at once on this device (cached per kernel).
+static int yz_clusters(void* fn, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::pair<int, void*>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_pair(dev, fn);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kYZCluster * 64);
+    cfg.blockDim = dim3(kYZThreads);
+    cfg.dynamicSmemBytes = smem;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, fn, &cfg) != cudaSuccess || n < 1) {
+        cudaGetLastError();
+        n = std::max(1, sm_count() / kYZCluster);
+    }
+    cache[key] = n;
+    return n;
+}
+
+static int launch_yz(const ConvPlan& p, bool adjoint, cudaStream_t st) {
+    void* fn = pick_yz(p.F[1], p.F[0], adjoint);
+    if (!fn) return fail(DECON_ERR_UNSUPPORTED, "fused Y / axial pass: unsupported canvas");
+    YZArgs a;
+    a.s1t = p.s1;
+    a.otft = p.otft;
+    a.twy = p.twy;
+    a.twz = p.twz;
+    a.Nz = (int)p.N[0];
+    a.Ny = (int)p.N[1];
+    a.Hx = (int)p.Hx;
+    const size_t smem = yz_smem_bytes((int)p.F[1], (int)p.F[0]);
+    DK_TRY(kernel_prepare(fn, smem, kYZThreads, nullptr));
+    const int ncl = (int)std::min<int64_t>(p.Hx, yz_clusters(fn, smem));
+    return launch(fn, (int64_t)ncl * kYZCluster, kYZThreads, smem, st, &a, PROF_ZOTF);
+}
+
+// Forward spectrum: x (window in N-space) -> S2 (after the Y pass), or, with
+// the fused Y / axial pass, -> the kx-major S1 (X pass only).
 int spectrum_forward(const ConvPlan& p, int pro, const float* in, Win3 win, float cval, float bg,
                      cudaStream_t st) {
     const int64_t Nz = p.N[0], Ny = p.N[1], Fy = p.F[1], P = p.P;
+    if (use_yz(p)) return launch_xr2c(p, pro, in, win, cval, bg, Nz, p.s1, st, Nz * Ny);
     DK_TRY(launch_xr2c(p, pro, in, win, cval, bg, Nz, p.s1, st));
     if (p.tma_y) {
         DK_TRY(launch_col_tma(p, p.ax_y, COL_FWD, p.tm_s1_j1, 1, p.s1_box, (int)Ny, p.tm_s2_j1, 1,
@@ -630,6 +763,7 @@ int spectrum_forward(const ConvPlan& p, int pro, const float* in, Win3 win, floa
 
 // Z pass (x OTF or conj OTF) and the inverse Y pass: S2 -> S1.
 int spectrum_filter_back(const ConvPlan& p, bool adjoint, cudaStream_t st) {
+    if (use_yz(p)) return launch_yz(p, adjoint, st);
     const int64_t Nz = p.N[0], Ny = p.N[1], Fy = p.F[1], P = p.P;
     const int mode = adjoint ? COL_OTF_CONJ : COL_OTF;
     if (p.tma_z) {

@@ -42,6 +42,10 @@ struct XR2CArgs {
     Axis ax;            // length Fx/2 (even Fx) or Fx (odd)
     const float2* twx;  // W_Fx table
     FastDiv fd_q4, fd_H, fd_nin, fd_np;  // Nx / 4, Hx, packed non-zero points, L / 2 + 1
+    // 0: spectrum rows of pitch P (element (row, kx) at row * P + kx); > 0:
+    // kx-major spectrum, element (row, kx) at kx * kstride + row (kstride =
+    // Nz * Ny), the layout of the fused Y / axial pass
+    int64_t kstride;
 };
 
 struct ColArgs {
@@ -91,6 +95,7 @@ struct XC2RArgs {
     float bg;
     double* partials;
     FastDiv fd_L, fd_h2, fd_npair, fd_q4, fd_Nx;  // L, L / 2, L / 2 + 1, Nx / 4, Nx
+    int64_t kstride;  // as XR2CArgs::kstride
 };
 
 // Device-resident state of one LinearFFTConvolver.
@@ -118,7 +123,19 @@ struct ConvPlan {
     int precision = 0;
     __half2* otf16 = nullptr;
     float* otf_inv = nullptr;
+    // Fused Y / axial pass (yzpass.cuh): the OTF also stored kx-major
+    // [Hx][Fy][Fz]; the spectrum between the X passes is then kx-major too
+    // ([Hx][Nz][Ny] in s1).  nullptr: the canvas takes the unfused passes.
+    float2* otft = nullptr;
 };
+
+// Canvas and signal extents the fused Y / axial pass implements (Fy in {256,
+// 512}, Fz in {128, 256}, the signal in the first half of both axes, Ny even).
+bool yz_supported(const int64_t N[3], const int64_t F[3]);
+// True when this plan's convolutions run the fused Y / axial pass.
+bool use_yz(const ConvPlan& p);
+// Fill p.otft from p.otf (after every OTF build).
+int build_otf_kmajor(const ConvPlan& p, cudaStream_t st);
 
 // Quantise p.otf into p.otf16 / p.otf_inv (capi.cu).
 int quantize_otf(const ConvPlan& p, cudaStream_t st);
@@ -134,7 +151,7 @@ bool encode_spectrum_map(CUtensorMap* map, const float2* base, int64_t pitch, in
                          int b1, int b2);
 
 int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cval, float bg,
-                int64_t nz_rows, float2* out, cudaStream_t st);
+                int64_t nz_rows, float2* out, cudaStream_t st, int64_t kstride = 0);
 int launch_col(const ConvPlan& p, const Axis& ax, int T, int mode, const float2* src,
                int64_t src_os, int64_t src_js, int nin, float2* dst, int64_t dst_os,
                int64_t dst_js, int nout, int64_t nouter, cudaStream_t st);

@@ -14,8 +14,11 @@
 // kNoAllocChunk elements, so n is limited to kNoAllocSlots * kNoAllocChunk
 // elements; pass 2 folds the partials in fixed order (deterministic).  Host
 // code cannot pass the array's name to a kernel (it is a host-side stand-in,
-// not a device address): the first call on each device, with that device
-// current, looks the address up with cudaGetSymbolAddress and keeps it.
+// not a device address): the first call on each device (in each CUDA context
+// of that device), with that device current, looks the address up with
+// cudaGetSymbolAddress and keeps it.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "conv_impl.cuh"
@@ -89,23 +92,65 @@ __global__ void __launch_bounds__(kNoAllocThreads) k_na_pass2(const double* part
     }
 }
 
-// Device address of g_noalloc_partials, looked up once per device.
+// Device address of g_noalloc_partials.  The address belongs to the module
+// as loaded into one CUDA context, so it is cached per device together with
+// the id of the context it was looked up in (cuCtxGetId, unique for the life
+// of the process) and looked up again when the device's current context is
+// another one (after cudaDeviceReset, or a primary context released and
+// created again).  Without the driver's context queries it is looked up on
+// every call.
+using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
+
+static bool current_context_id(unsigned long long* id) {
+    static PfnCtxGetCurrent get_current = nullptr;
+    static PfnCtxGetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<PfnCtxGetCurrent>(fn);
+        else
+            cudaGetLastError();
+        fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PfnCtxGetId>(fn);
+        else
+            cudaGetLastError();
+    });
+    if (!get_current || !get_id) return false;
+    CUcontext c = nullptr;
+    if (get_current(&c) != CUDA_SUCCESS || c == nullptr) return false;
+    return get_id(c, id) == CUDA_SUCCESS;
+}
+
 static int noalloc_scratch(double** out) {
     static std::mutex mu;
     static double* addr[64] = {nullptr};
+    static unsigned long long ctx[64] = {0};
     int dev = 0;
     DK_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return fail(DECON_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-        if (e != cudaSuccess || p == nullptr)
-            return fail(DECON_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch failed: %s",
-                        cudaGetErrorString(e));
-        addr[dev] = static_cast<double*>(p);
+    unsigned long long id = 0;
+    bool have_id = current_context_id(&id);
+    if (have_id && addr[dev] && ctx[dev] == id) {
+        *out = addr[dev];
+        return DECON_OK;
     }
-    *out = addr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (e != cudaSuccess || p == nullptr)
+        return fail(DECON_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch failed: %s",
+                    cudaGetErrorString(e));
+    // the lookup makes the device's primary context current if none was
+    if (!have_id) have_id = current_context_id(&id);
+    addr[dev] = have_id ? static_cast<double*>(p) : nullptr;  // no id: look up on every call
+    ctx[dev] = have_id ? id : 0;
+    *out = static_cast<double*>(p);
     return DECON_OK;
 }
 

@@ -487,4 +487,184 @@ __global__ void __launch_bounds__(256) k_hessian_adj_t(const float* __restrict__
     hess_adj_walk(hw, d, w, [&](int64_t i, float lt) { out[i] = lt; });
 }
 
+
+// ---- dual and primal update in one z-walk -----------------------------------
+//
+// y2_out = proj(y2_in + sigma H x_bar) and x_new = max(0, x - tau (A^T y1 +
+// H^T y2_out)) for one iteration, without y2_out making a round trip through
+// global memory between the two: per tile the CTA walks z, staging x_bar with
+// a two-voxel halo (36 x 12), evaluating y2_out on the one-voxel halo (34 x
+// 10) of each plane from it, and H^T y2_out of the tile's interior from the
+// last three y2_out planes.  Halo values of y2_out are recomputed by every
+// tile that needs them (at the clamped coordinate, which is the value the
+// staged adjoint reads there), so y2 is double-buffered: y2_in is read, never
+// written, and tiles never see a neighbour's new values.  The float
+// operations are those of k_hess_dual_p and k_hess_primal_t (bit-identical
+// results), and y2_out is written once, by the tile that owns each voxel.
+constexpr int kH2X = kTX + 4, kH2Y = kTY + 4, kPL2 = kH2X * kH2Y;
+
+// hess6_smem on a plane of row stride S.
+template <int S>
+__device__ __forceinline__ void hess6_at(const float* pm, const float* p0, const float* pp, int c,
+                                         const float w[6], float h[6]) {
+    const int n = c - S, s = c + S, wv = c - 1, e = c + 1;
+    const float cv = p0[c];
+    const float hzz = d2v(pm[c], cv, pp[c]);
+    const float hyy = d2v(p0[n], cv, p0[s]);
+    const float hxx = d2v(p0[wv], cv, p0[e]);
+    const float dz_yp = (pp[s] - pm[s]) / 2.f;
+    const float dz_ym = (pp[n] - pm[n]) / 2.f;
+    const float hyz = (dz_yp - dz_ym) / 2.f;
+    const float dz_xp = (pp[e] - pm[e]) / 2.f;
+    const float dz_xm = (pp[wv] - pm[wv]) / 2.f;
+    const float hxz = (dz_xp - dz_xm) / 2.f;
+    const float dy_xp = (p0[s + 1] - p0[n + 1]) / 2.f;
+    const float dy_xm = (p0[s - 1] - p0[n - 1]) / 2.f;
+    const float hxy = (dy_xp - dy_xm) / 2.f;
+    h[0] = hzz * w[0];
+    h[1] = hyy * w[1];
+    h[2] = hxx * w[2];
+    h[3] = hyz * w[3];
+    h[4] = hxz * w[4];
+    h[5] = hxy * w[5];
+}
+
+template <int NORM>
+__global__ void __launch_bounds__(256) k_hess_dual_primal(
+    PdhgDev* s, const float* __restrict__ y2_in, float* __restrict__ y2_out,
+    const float* __restrict__ xc, const float* __restrict__ xp, const float* __restrict__ aty,
+    float* __restrict__ xn, Dims d, W6 w, float alpha, int s_dx2, int s_xc2, int s_xn2) {
+    if (s->stop) return;
+    __shared__ float xb[4][kPL2];     // x_bar planes, ring slot = plane & 3
+    __shared__ float yn[6][4][kPL];   // y2_out planes, ring slot = plane & 3
+    const float sg = (float)s->sigma, th = (float)s->theta, tau = (float)s->tau;
+    const int64_t n = d.nz * d.ny * d.nx, plane = d.ny * d.nx;
+    const TileGeo g(d);
+    const int tid = threadIdx.x, tx = tid % kTX, ty = tid / kTX;
+    double dx2 = 0.0, xc2 = 0.0, xn2 = 0.0;
+    for (int64_t tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
+        const int64_t bx = tile % g.ntx, rr = tile / g.ntx, by = rr % g.nty, bz = rr / g.nty;
+        const int64_t x0 = bx * kTX, y0 = by * kTY, z0 = bz * kZChunk;
+        const int64_t z1 = min(z0 + kZChunk, d.nz);
+        // this thread's x_bar staging slots (two-voxel halo, clamped coordinates)
+        int64_t o2[2];
+        bool k2[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int q = tid + u * 256;
+            k2[u] = q < kPL2;
+            const int sy = q / kH2X, sx = q - sy * kH2X;
+            o2[u] = clampi(y0 - 2 + sy, d.ny) * d.nx + clampi(x0 - 2 + sx, d.nx);
+        }
+        // this thread's y2_out positions (one-voxel halo): the clamped voxel,
+        // its stencil centre in the x_bar plane, and whether it owns the voxel
+        int64_t o1[2];
+        int c2[2];
+        bool k1[2], own[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int q = tid + u * 256;
+            k1[u] = q < kPL;
+            const int ly = q / kHX, lx = q - ly * kHX;
+            const int64_t yy = y0 - 1 + ly, xx = x0 - 1 + lx;
+            const int64_t gy = clampi(yy, d.ny), gx = clampi(xx, d.nx);
+            o1[u] = gy * d.nx + gx;
+            c2[u] = (int)((gy - (y0 - 2)) * kH2X + (gx - (x0 - 2)));
+            own[u] = ly >= 1 && ly <= kTY && lx >= 1 && lx <= kTX && yy < d.ny && xx < d.nx;
+        }
+        const int64_t x = x0 + tx, y = y0 + ty;
+        const bool in = x < d.nx && y < d.ny;
+        const int64_t ipl = y * d.nx + x;
+        Edge e;
+        e.ylo = y == 0 ? -1.f : 1.f;
+        e.yhi = y == d.ny - 1 ? -1.f : 1.f;
+        e.xlo = x == 0 ? -1.f : 1.f;
+        e.xhi = x == d.nx - 1 ? -1.f : 1.f;
+        const int64_t qa = max(z0 - 1, (int64_t)0), qb = min(z1, d.nz - 1);  // y2_out planes
+        const int64_t pa = max(qa - 1, (int64_t)0), pb = min(qb + 1, d.nz - 1);  // x_bar planes
+        auto dual_plane = [&](int64_t q) {
+            const int64_t qm = clampi(q - 1, d.nz), qp = clampi(q + 1, d.nz);
+            const float* pm = xb[qm & 3];
+            const float* p0 = xb[q & 3];
+            const float* pp = xb[qp & 3];
+            const bool owned_plane = q >= z0 && q < z1;
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                if (!k1[u]) continue;
+                float h[6];
+                hess6_at<kH2X>(pm, p0, pp, c2[u], w.w, h);
+                const int64_t i = q * plane + o1[u];
+                float v[6];
+                if constexpr (NORM == 0) {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) v[c] = fminf(fmaxf(__ldg(y2_in + c * n + i) + sg * h[c], -alpha), alpha);
+                } else {
+                    float ss = 0.f;
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) {
+                        v[c] = __ldg(y2_in + c * n + i) + sg * h[c];
+                        ss += v[c] * v[c];
+                    }
+                    const float sc = fmaxf(sqrtf(ss + 1e-12f) / alpha, 1.f);
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) v[c] = v[c] / sc;
+                }
+                const int q1 = tid + u * 256;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) yn[c][q & 3][q1] = v[c];
+                if (own[u] && owned_plane) {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) y2_out[c * n + i] = v[c];
+                }
+            }
+        };
+        auto primal_plane = [&](int64_t z) {
+            if (!in || z < z0 || z >= z1) return;
+            const int sm_ = (int)(clampi(z - 1, d.nz) & 3), sc_ = (int)(z & 3),
+                      sp_ = (int)(clampi(z + 1, d.nz) & 3);
+            e.zlo = z == 0 ? -1.f : 1.f;
+            e.zhi = z == d.nz - 1 ? -1.f : 1.f;
+            const float lt = hess_adj_smem(yn[0][sm_], yn[0][sc_], yn[0][sp_], yn[1][sc_], yn[2][sc_],
+                                           yn[3][sm_], yn[3][sp_], yn[4][sm_], yn[4][sp_], yn[5][sc_],
+                                           ty + 1, tx + 1, e, w.w);
+            const int64_t i = z * plane + ipl;
+            const float a = xc[i];
+            const float gr = aty[i] + lt;
+            const float v = fmaxf(a - tau * gr, 0.f);
+            xn[i] = v;
+            const float dd = v - a;
+            dx2 += (double)dd * dd;
+            xc2 += (double)a * a;
+            xn2 += (double)v * v;
+        };
+        for (int64_t p = pa; p <= pb; ++p) {
+            // stage x_bar plane p (two-voxel halo)
+            float* dst = xb[p & 3];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                if (!k2[u]) continue;
+                const int64_t i = p * plane + o2[u];
+                const float a = __ldg(xc + i);
+                dst[tid + u * 256] = a + th * (a - __ldg(xp + i));
+            }
+            __syncthreads();
+            // y2_out planes whose x_bar neighbourhood is complete
+            const int64_t q = p - 1;
+            if (q >= qa && q <= qb) dual_plane(q);
+            if (p == d.nz - 1 && p >= qa && p <= qb) dual_plane(p);
+            __syncthreads();
+            // x_new planes whose y2_out neighbourhood is complete
+            if (q >= qa && q <= qb) primal_plane(q - 1);
+            if (p == d.nz - 1 && p >= qa && p <= qb) {
+                if (q >= qa) primal_plane(q);
+                primal_plane(p);
+            }
+        }
+        __syncthreads();  // the rings are reused by the next tile
+    }
+    put_slot(s, s_dx2, dx2);
+    put_slot(s, s_xc2, xc2);
+    put_slot(s, s_xn2, xn2);
+}
+
 }  // namespace dk

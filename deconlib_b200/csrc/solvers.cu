@@ -751,6 +751,28 @@ int decon_pdhg_hess_primal(decon_pdhg* h, const float* xc, const float* aty, con
     return DECON_OK;
 }
 
+int decon_pdhg_hess_dual_primal(decon_pdhg* h, const float* y2_in, float* y2_out, const float* xc,
+                                const float* xp, const float* aty, float* xn,
+                                const int64_t shape[3], float r, float alpha, int norm,
+                                void* stream) {
+    if (!h || !y2_in || !y2_out || !xc || !xp || !aty || !xn || !shape)
+        return fail(DECON_ERR_NULL, "null pointer");
+    if (y2_in == y2_out) return fail(DECON_ERR_VALUE, "y2_in and y2_out must be different buffers");
+    W6 w;
+    hessian_weights(r, w.w);
+    const Dims d{shape[0], shape[1], shape[2]};
+    const int grid = (int)std::min<int64_t>(kPdhgGrid, std::max<int64_t>(TileGeo(d).ntiles, 1));
+    const cudaStream_t s = as_stream(stream);
+    if (norm == 0)
+        k_hess_dual_primal<0><<<grid, 256, 0, s>>>(h->dev, y2_in, y2_out, xc, xp, aty, xn, d, w, alpha,
+                                                   kSlotDx2, kSlotXc2, kSlotXn2);
+    else
+        k_hess_dual_primal<1><<<grid, 256, 0, s>>>(h->dev, y2_in, y2_out, xc, xp, aty, xn, d, w, alpha,
+                                                   kSlotDx2, kSlotXc2, kSlotXn2);
+    DK_LAUNCHED();
+    return DECON_OK;
+}
+
 int decon_pdhg_hess_dk(decon_pdhg* h, const float* ax_new, const float* ax_cur, int64_t m,
                        const float* xn, const float* xc, const int64_t shape[3], float r,
                        void* stream) {

@@ -11,8 +11,9 @@
 namespace dk {
 
 // Device-side flag set when a bounded mbarrier wait gives up (read by
-// decon_device_status); such a CTA skips its compute and store.  Only the
-// translation unit with the TMA kernels (conv.cu) includes this header.
+// decon_device_status, cleared by decon_device_status_clear); such a CTA
+// skips its compute and store.  Only the translation unit with the TMA
+// kernels (conv.cu) includes this header.
 static __device__ int g_wait_timeout = 0;
 
 constexpr unsigned kWaitLimit = 1u << 22;
@@ -47,9 +48,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait: gives up after kWaitLimit polls and raises g_wait_timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (unsigned i = 0; i < kWaitLimit; ++i)
+// Bounded wait: gives up after `limit` polls (kWaitLimit in the kernels) and
+// raises g_wait_timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  unsigned limit = kWaitLimit) {
+    for (unsigned i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     atomicExch(&g_wait_timeout, 1);
     return false;

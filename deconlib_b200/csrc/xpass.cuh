@@ -161,12 +161,37 @@ __global__ void __launch_bounds__(kFftThreads, 3) k_xr2c(XR2CArgs a) {
     if constexpr (LS > 0) fft_lines_pow2<LS, -1, 1, TC>(sm, T, tid % T, tid / T, a.ax.tw, a.ax.tws, nin);
     else fft_lines<-1, LS>(sm, T, tid % T, tid / T, a.ax, nin);
     const int H = a.Hx;
+    const int lgT = 31 - __clz(T);  // T is a power of two
     if (a.odd) {
         #pragma unroll 1
         for (int q = tid; q < T * H; q += blockDim.x) {
-            const int t = fdiv(q, a.fd_H), k = q - t * H;
+            int t, k;
+            if (a.kstride) {
+                k = q >> lgT;
+                t = q & (T - 1);
+            } else {
+                t = fdiv(q, a.fd_H);
+                k = q - t * H;
+            }
             const int64_t row = row0 + t;
-            if (row < a.nrows) a.out[row * a.P + k] = sm[phys(k, t, T)];
+            if (row < a.nrows) a.out[a.kstride ? k * a.kstride + row : row * a.P + k] = sm[phys(k, t, T)];
+        }
+    } else if (a.kstride) {
+        // kx-major spectrum: consecutive threads take consecutive rows at one
+        // frequency pair, so every warp stores two 256-byte runs
+        const int M = L, np = (M >> 1) + 1;
+        #pragma unroll 1
+        for (int q = tid; q < T * np; q += blockDim.x) {
+            const int k = q >> lgT, t = q & (T - 1);
+            const int64_t row = row0 + t;
+            if (row >= a.nrows) continue;
+            const int km = M - k;
+            const float2 zk = sm[phys(k, t, T)];
+            const float2 zm = cconj(sm[phys(k == 0 ? 0 : km, t, T)]);
+            const float2 e = cscale(cadd(zk, zm), 0.5f);
+            const float2 o = rot90<-1>(cscale(csub(zk, zm), 0.5f));
+            if (k < H) a.out[k * a.kstride + row] = cadd(e, cmul(__ldg(&a.twx[k]), o));
+            if (km != k && km < H) a.out[km * a.kstride + row] = cadd(cconj(e), cmul(__ldg(&a.twx[km]), cconj(o)));
         }
     } else {
         // X[k] = e + W^k o and X[M-k] = conj(e) + W^(M-k) conj(o) with
@@ -234,16 +259,28 @@ __global__ void __launch_bounds__(kFftThreads, 2) k_xc2r(XC2RArgs a) {
     const int T = TC > 0 ? TC : a.T, L = LS > 0 ? LS : a.ax.L, tid = threadIdx.x;
     auto phys = [&](int j, int t, int) { return physw<TC>(j, t, T); };
     const int64_t row0 = (int64_t)blockIdx.x * T;
+    const int lgT = 31 - __clz(T);  // T is a power of two
     if (a.odd) {
         #pragma unroll 1
         for (int q = tid; q < T * L; q += blockDim.x) {
-            const int t = fdiv(q, a.fd_L), k = q - t * L;
+            int t, k;
+            if (a.kstride) {
+                k = q >> lgT;
+                t = q & (T - 1);
+            } else {
+                t = fdiv(q, a.fd_L);
+                k = q - t * L;
+            }
             const int64_t row = row0 + t;
             float2 Z = make_float2(0.f, 0.f);
             if (row < a.nrows) {
-                const float2* rp = a.in + row * a.P;
                 // full Hermitian spectrum from the half: X[k] = conj(X[Fx - k])
-                Z = k < a.Hx ? rp[k] : cconj(rp[L - k]);
+                if (a.kstride) {
+                    Z = k < a.Hx ? a.in[k * a.kstride + row] : cconj(a.in[(L - k) * a.kstride + row]);
+                } else {
+                    const float2* rp = a.in + row * a.P;
+                    Z = k < a.Hx ? rp[k] : cconj(rp[L - k]);
+                }
                 if (k == 0) Z.y = 0.f;
             }
             sm[phys(k, t, T)] = Z;
@@ -251,39 +288,55 @@ __global__ void __launch_bounds__(kFftThreads, 2) k_xc2r(XC2RArgs a) {
         __syncthreads();
     } else {
         const int M = L;
-        // stage the half spectrum: X[0..M) as float4 pairs, X[M] aside
-        const int h2 = M >> 1;  // float4 (two complex) per row
-        const int nq = T * h2;
-        constexpr int U = 4;
-        #pragma unroll 1
-        for (int c0 = tid; c0 < nq; c0 += U * blockDim.x) {
-            float4 v[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int c = c0 + u * blockDim.x;
-                const int t = fdiv(c, a.fd_h2);
+        if (a.kstride) {
+            // kx-major spectrum: a warp reads 32 consecutive rows of one
+            // frequency (256 bytes) per load
+            #pragma unroll 1
+            for (int q = tid; q < T * M; q += blockDim.x) {
+                const int k = q >> lgT, t = q & (T - 1);
                 const int64_t row = row0 + t;
-                v[u] = (c < nq && row < a.nrows)
-                           ? __ldg(reinterpret_cast<const float4*>(a.in + row * a.P) + (c - t * h2))
-                           : make_float4(0.f, 0.f, 0.f, 0.f);
+                sm[phys(k, t, T)] = row < a.nrows ? a.in[k * a.kstride + row] : make_float2(0.f, 0.f);
             }
+            #pragma unroll 1
+            for (int t = tid; t < T; t += blockDim.x) {
+                const int64_t row = row0 + t;
+                nyq[t] = row < a.nrows ? a.in[M * a.kstride + row] : make_float2(0.f, 0.f);
+            }
+        } else {
+            // stage the half spectrum: X[0..M) as float4 pairs, X[M] aside
+            const int h2 = M >> 1;  // float4 (two complex) per row
+            const int nq = T * h2;
+            constexpr int U = 4;
+            #pragma unroll 1
+            for (int c0 = tid; c0 < nq; c0 += U * blockDim.x) {
+                float4 v[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int c = c0 + u * blockDim.x;
-                if (c < nq) {
-                    const int t = fdiv(c, a.fd_h2), q2 = c - t * h2;
-                    sm[phys(2 * q2, t, T)] = make_float2(v[u].x, v[u].y);
-                    sm[phys(2 * q2 + 1, t, T)] = make_float2(v[u].z, v[u].w);
+                for (int u = 0; u < U; ++u) {
+                    const int c = c0 + u * blockDim.x;
+                    const int t = fdiv(c, a.fd_h2);
+                    const int64_t row = row0 + t;
+                    v[u] = (c < nq && row < a.nrows)
+                               ? __ldg(reinterpret_cast<const float4*>(a.in + row * a.P) + (c - t * h2))
+                               : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int c = c0 + u * blockDim.x;
+                    if (c < nq) {
+                        const int t = fdiv(c, a.fd_h2), q2 = c - t * h2;
+                        sm[phys(2 * q2, t, T)] = make_float2(v[u].x, v[u].y);
+                        sm[phys(2 * q2 + 1, t, T)] = make_float2(v[u].z, v[u].w);
+                    }
                 }
             }
-        }
-        #pragma unroll 1
-        for (int t = tid; t < T; t += blockDim.x) {
-            const int64_t row = row0 + t;
-            const bool ok = row < a.nrows;
-            nyq[t] = ok ? a.in[row * a.P + M] : make_float2(0.f, 0.f);
-            // odd M: the last packed point is not covered by the float4 pairs
-            if (M & 1) sm[phys(M - 1, t, T)] = ok ? a.in[row * a.P + M - 1] : make_float2(0.f, 0.f);
+            #pragma unroll 1
+            for (int t = tid; t < T; t += blockDim.x) {
+                const int64_t row = row0 + t;
+                const bool ok = row < a.nrows;
+                nyq[t] = ok ? a.in[row * a.P + M] : make_float2(0.f, 0.f);
+                // odd M: the last packed point is not covered by the float4 pairs
+                if (M & 1) sm[phys(M - 1, t, T)] = ok ? a.in[row * a.P + M - 1] : make_float2(0.f, 0.f);
+            }
         }
         __syncthreads();
         // Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) W_Fx^-k, one

@@ -10,6 +10,7 @@ from __future__ import annotations
 from typing import Any, Callable, Protocol, Tuple, runtime_checkable
 
 import numpy as np
+import torch
 
 __all__ = ["LinearOperator", "Compose", "compose", "as_numpy_op"]
 
@@ -87,10 +88,21 @@ def flatten(op) -> list:
 
 
 def _call_numpy(fn: Callable, x: np.ndarray) -> np.ndarray:
-    from ._device import to_device
+    """Call an operator method with a NumPy array and return a NumPy array
+    (composition.py:125-137): the array itself first, so pure NumPy operators
+    take part too; this package's operators copy it to the device and return
+    a CUDA tensor, which is read back.  A ``TypeError`` retries with the
+    array on the device."""
+    x_np = np.ascontiguousarray(x)
+    try:
+        out = fn(x_np)
+    except TypeError:
+        from ._device import to_device
 
-    out = fn(to_device(np.ascontiguousarray(x)))
-    return out.detach().cpu().numpy()
+        out = fn(to_device(x_np))
+    if isinstance(out, torch.Tensor):
+        return out.detach().cpu().numpy()
+    return np.asarray(out)
 
 
 def as_numpy_op(op: LinearOperator) -> Tuple[Callable[[np.ndarray], np.ndarray],

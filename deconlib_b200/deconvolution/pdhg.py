@@ -313,9 +313,11 @@ class PDHGRunner:
     :1066-1221), split into set-up / ``iterate`` / ``result`` so a caller
     (the benchmark, the serving loop) can time or interleave iterations.
 
-    Buffers: x and A x are double-buffered (slot k % 2 holds x_k, the other
-    x_{k-1}); iteration k writes x_{k+1} over x_{k-1}.  x_bar and A x_bar are
-    never stored: they are formed from the two slots inside the kernels."""
+    Buffers: x is triple-buffered (slot k % 3 holds x_k, slot (k + 2) % 3
+    x_{k-1}; iteration k writes x_{k+1} into slot (k + 1) % 3, so the fused
+    Hessian kernel never writes a buffer it still reads with halos); A x is
+    double-buffered (slot k % 2).  x_bar and A x_bar are never stored: they
+    are formed from the slots inside the kernels."""
 
     def __init__(self, data, A, reg, x0, alpha, loss_type, num_iter, background, delta, eta,
                  eval_interval, tol, min_iter, patience, verbose=False, callback=None,
@@ -337,7 +339,7 @@ class PDHGRunner:
             self.state = _State(num_iter, step_scale, delta, eta, tol, min_iter, patience)
         self.h = self.state.h
         self.ncomp = reg.output_components
-        self.X = [x0.contiguous(), x0.clone()]
+        self.X = [x0.contiguous(), x0.clone(), x0.clone()]
         ax0 = to_device(A.forward(self.X[0])).clone()
         if tuple(ax0.shape) != tuple(data.shape):
             raise ValueError(
@@ -361,6 +363,9 @@ class PDHGRunner:
             self.shp = _lib.i64arr(tuple(x0.shape))
             self.r = float(reg.r)
             self.xbar = self.dxb = None
+            # the fused dual + primal kernel reads y2 of iteration k from one
+            # buffer and writes iteration k + 1's into the other
+            self.y2s = [self.y2, zeros((self.ncomp,) + tuple(x0.shape))]
 
     def iterate(self) -> bool:
         """Queue iteration k; returns False once the solve has stopped."""
@@ -368,7 +373,7 @@ class PDHGRunner:
         if k >= self.num_iter or self.stopped_at is not None:
             return False
         m, n = self.m, self.n
-        xc, xp = self.X[k % 2], self.X[(k + 1) % 2]
+        xc, xp, xo = self.X[k % 3], self.X[(k + 2) % 3], self.X[(k + 1) % 3]
         axc, axp = self.AX[k % 2], self.AX[(k + 1) % 2]
         _lib.call("decon_pdhg_dual_data", h, _lib.ptr(self.y1), _lib.ptr(axc), _lib.ptr(axp),
                   _lib.ptr(self.data), C.c_float(self.bg), self.lcode, m, s)
@@ -377,11 +382,12 @@ class PDHGRunner:
         if self.fused:
             # Hessian3D: L x_bar, L^T y2 and L (x_new - x) evaluated on the fly
             shp, r = self.shp, C.c_float(self.r)
-            _lib.call("decon_pdhg_hess_dual", h, _lib.ptr(self.y2), _lib.ptr(xc), _lib.ptr(xp), shp,
-                      r, C.c_float(self.alpha), self.ncode, s)
-            _lib.call("decon_pdhg_hess_primal", h, _lib.ptr(xc), _lib.ptr(aty), _lib.ptr(self.y2),
-                      _lib.ptr(xp), shp, r, s)
-            xn = xp
+            y2i, y2o = self.y2s[k % 2], self.y2s[(k + 1) % 2]
+            _lib.call("decon_pdhg_hess_dual_primal", h, _lib.ptr(y2i), _lib.ptr(y2o), _lib.ptr(xc),
+                      _lib.ptr(xp), _lib.ptr(aty), _lib.ptr(xo), shp, r, C.c_float(self.alpha),
+                      self.ncode, s)
+            self.y2 = y2o
+            xn = xo
             axn = to_device(A.forward(xn))
             _lib.call("decon_pdhg_hess_dk", h, _lib.ptr(axn), _lib.ptr(axc), m, _lib.ptr(xn),
                       _lib.ptr(xc), shp, r, s)
@@ -397,8 +403,8 @@ class PDHGRunner:
                       C.c_float(self.alpha), self.ncode, self.ncomp, n, s)
             lty = to_device(reg.adjoint(self.y2))
             _lib.call("decon_pdhg_primal", h, _lib.ptr(xc), _lib.ptr(aty), _lib.ptr(lty),
-                      _lib.ptr(xp), n, s)
-            xn = xp
+                      _lib.ptr(xo), n, s)
+            xn = xo
             axn = to_device(A.forward(xn))
             _lib.call("decon_pdhg_sub", h, _lib.ptr(xn), _lib.ptr(xc), _lib.ptr(self.dxb), n, s)
             ldx = to_device(reg.forward(self.dxb))
@@ -449,7 +455,7 @@ class PDHGRunner:
         final_iter = info["final_iter"] if self.stopped_at is None else self.stopped_at
         final_iter = min(final_iter, self.k) if self.num_iter > 0 else 0
         converged = info["converged"]
-        x = self.X[final_iter % 2]
+        x = self.X[final_iter % 3]
         taus = [float(v) for v in info["tau_hist"][:final_iter]]
         sigmas = [float(v) for v in info["sigma_hist"][:final_iter]]
         lh = info["loss_hist"]

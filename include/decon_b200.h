@@ -42,8 +42,19 @@ const char* decon_last_error(void);
 /* Library ABI version (major * 10000 + minor * 100 + patch). */
 int decon_version(void);
 /* Synchronises the stream and reports DECON_ERR_TIMEOUT if any kernel's
- * bounded TMA/mbarrier wait gave up since load (its results are invalid). */
+ * bounded TMA/mbarrier wait gave up since load or since the last
+ * decon_device_status_clear (the results of that kernel are invalid). */
 int decon_device_status(void* stream);
+/* Synchronises the stream and clears the timeout record that
+ * decon_device_status reads, so later checks report only new timeouts. */
+int decon_device_status_clear(void* stream);
+/* Test hook for the bounded waits (no counterpart in the reference): one
+ * CTA waits, through the same bounded mbarrier wait the TMA kernels use, on
+ * a barrier that nothing completes; after `polls` polls (1..65536) the wait
+ * gives up, records the timeout and the kernel returns.  Faults nothing and
+ * leaves the context usable; decon_device_status then reports
+ * DECON_ERR_TIMEOUT until decon_device_status_clear. */
+int decon_test_wait_timeout(unsigned polls, void* stream);
 /* Kernels launched by this library since load (benchmark accounting). */
 int64_t decon_launch_count(void);
 
@@ -95,6 +106,12 @@ int decon_conv_set_precision(decon_conv* plan, int precision, void* stream);
 int decon_conv_destroy(decon_conv* plan);
 /* operator_norm_sq = max |OTF|^2 (linops_mlx.py:415). */
 int decon_conv_norm_sq(const decon_conv* plan, double* out);
+/* 1 when this plan's convolutions run the fused Y / axial pass (one
+ * thread-block cluster per kx column; canvases with Fy in {256, 512}, Fz in
+ * {128, 256}, the signal in the first half of both axes, even Ny, FP32 OTF),
+ * 0 when they run the separate Y and axial passes.  No reference
+ * counterpart (a property of this implementation). */
+int decon_conv_fused_yz(const decon_conv* plan, int* out);
 /* Canvas fft_shape and the spectrum row pitch (complex elements). Host. */
 int decon_conv_shape(const decon_conv* plan, int64_t fft_shape[3], int64_t* pitch);
 /* Copies the OTF (fft_z, fft_y, fft_x/2+1) complex64 into out (device). */
@@ -305,6 +322,16 @@ int decon_pdhg_hess_dual(decon_pdhg* h, float* y2, const float* xc, const float*
                          const int64_t shape[3], float r, float alpha, int norm, void* stream);
 int decon_pdhg_hess_primal(decon_pdhg* h, const float* xc, const float* aty, const float* y2,
                            float* xn, const int64_t shape[3], float r, void* stream);
+/* hess_dual followed by hess_primal in one kernel (pdhg_mlx.py:732-743):
+ * y2_out = proj(y2_in + sigma H x_bar), then x_new = max(0, x - tau (aty +
+ * H^T y2_out)) and its FP64 sums, with y2_out consumed from shared memory
+ * (each tile recomputes the y2_out values of its one-voxel halo).  y2_in and
+ * y2_out are distinct buffers (6, z, y, x): alternate them between
+ * iterations.  Same float32 values as the two separate calls. */
+int decon_pdhg_hess_dual_primal(decon_pdhg* h, const float* y2_in, float* y2_out, const float* xc,
+                                const float* xp, const float* aty, float* xn,
+                                const int64_t shape[3], float r, float alpha, int norm,
+                                void* stream);
 int decon_pdhg_hess_dk(decon_pdhg* h, const float* ax_new, const float* ax_cur, int64_t m,
                        const float* xn, const float* xc, const int64_t shape[3], float r,
                        void* stream);
@@ -319,6 +346,42 @@ int decon_pdhg_read(decon_pdhg* h, int* k, int* final_iter, int* converged, int*
                     double* rel_hist, void* stream);
 /* Host-requested stop (a callback returned truthy). Synchronises. */
 int decon_pdhg_set_stop(decon_pdhg* h, int final_iter, void* stream);
+
+/* ---- resident Hessian-PDHG solve (pdhg_mlx.py:507-900) ------------------ */
+
+typedef struct decon_pdhg_solver decon_pdhg_solver; /* x, A x, duals, tables */
+
+/* solve_pdhg_mlx with regularization="hessian" (pdhg_mlx.py:507-700 set-up)
+ * as one device-resident object: A = FractionalAreaDownsample(scale) o
+ * LinearFFTConvolver(conv) (conv's signal shape N is the object shape;
+ * data_shape M the observation's, M[a] == N[a] on axes that are not
+ * resampled; all scale[a] == 1 is the plain operator A = conv), Hessian3D
+ * with spacing ratio r, norm 0 = L1 / 1 = L1_2, loss 0 = Poisson / 1 =
+ * Gaussian.  data: device, shape M (copied).  x0: device, shape N, clamped
+ * at 0; NULL = the reference's default (max(A^T data, 0) when resampled,
+ * max(data, 0) for the plain operator).  The plan `conv` must outlive the
+ * solver.  Allocates its buffers (x and A x twice, y1, six-component y2,
+ * A^T y1, two resampling intermediates); queues the initial state on
+ * `stream`. */
+int decon_pdhg_solver_create(decon_conv* conv, const float* data, const int64_t data_shape[3],
+                             const double scale[3], float background, int loss_type,
+                             const float* x0, float r, float alpha, int norm, int num_iter,
+                             double delta, double eta, double tol, int min_iter, int patience,
+                             int eval_interval, void* stream, decon_pdhg_solver** out);
+/* Queues up to `iterations` more iterations of the PDHG loop
+ * (pdhg_mlx.py:717-900; at most num_iter in total), each the fused launch
+ * sequence dual / A^T / Hessian dual / primal / A / ||dK x||^2 / FP64 step,
+ * plus the loss every eval_interval iterations.  No host synchronisation and
+ * no allocation: the calls may be captured in a CUDA graph.  Iterations
+ * after convergence are no-ops on the device. */
+int decon_pdhg_run(decon_pdhg_solver* s, int iterations, void* stream);
+/* Copies x of the last completed iteration (the converged iterate if the
+ * solve stopped early) to x_out (device, shape N).  Synchronises. */
+int decon_pdhg_solver_x(decon_pdhg_solver* s, float* x_out, void* stream);
+/* The solver's scalar state (read it with decon_pdhg_read) and the number of
+ * iterations queued so far. */
+int decon_pdhg_solver_state(decon_pdhg_solver* s, decon_pdhg** state, int* queued);
+int decon_pdhg_solver_destroy(decon_pdhg_solver* s);
 
 /* ---- pad / crop (deconvolution/core_operators.py:29-137) ---------------- */
 
@@ -383,9 +446,10 @@ int decon_reduce(const float* a, const float* b, int64_t n, int op, double* out,
  * nothing: its scratch is a fixed 128 KB device array inside the library
  * (held by every GPU that loads it until exit), so n is limited to
  * 67,108,864 elements (DECON_ERR_VALUE beyond).  The first call on a device
- * looks up that array's address with the device current; make that first
- * call before any stream capture.  All calls share the array: calls whose
- * kernels overlap on the GPU race, so order them on one stream. */
+ * looks up that array's address with the device current, and looks it up
+ * again after the device's context changed (cudaDeviceReset); make that
+ * first call before any stream capture.  All calls share the array: calls
+ * whose kernels overlap on the GPU race, so order them on one stream. */
 int decon_reduce_noalloc(const float* a, const float* b, int64_t n, int op, double* out,
                          void* stream);
 

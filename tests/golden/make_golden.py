@@ -2,7 +2,7 @@
 
 Run from the repository root, in the container that holds the reference:
 
-    python tests/golden/make_golden.py [--reference PATH]
+    python tests/golden/make_golden.py --reference PATH
 
 The reference imports ``mlx.core``; ``tests/golden/mlx_standin`` supplies a
 NumPy stand-in for the names it calls.  The script runs itself twice in
@@ -425,7 +425,8 @@ def _run_nlcg(out_path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True,
+                    help="root of the deconlib 0.4.0 source tree (read-only)")
     ap.add_argument("--worker", choices=["fp32", "fp64", "psf", "nlcg32", "nlcg64"], default=None)
     a = ap.parse_args()
     if a.worker == "psf":

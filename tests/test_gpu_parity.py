@@ -257,6 +257,7 @@ def test_column_pass_variants_agree(D, monkeypatch, shape, fft):
     # The pipelined column kernel (R x R Stockham, half-zero split for 128 /
     # 512), the one-tile TMA kernel (DECON_NO_PIPE) and the plain-load kernel
     # (DECON_NO_TMA) compute the same transforms with different factorings;
+    # so does the fused Y / axial pass (the default where it applies);
     # DECON_PIPE_LEAN selects the two-CTA axial kernel (twiddles in shared
     # memory, one ring slot) or the one-CTA kernel (same arithmetic).
     rng = np.random.default_rng(11)
@@ -264,9 +265,13 @@ def test_column_pass_variants_agree(D, monkeypatch, shape, fft):
     k = rng.random(kshape).astype(np.float32)
     x = rng.random(shape).astype(np.float32)
     outs = []
-    keys = ("DECON_NO_PIPE", "DECON_NO_TMA", "DECON_PIPE_LEAN")
-    for env in ({}, {"DECON_NO_PIPE": "1"}, {"DECON_NO_TMA": "1"}, {"DECON_PIPE_LEAN": "0"},
-                {"DECON_PIPE_LEAN": "1"}):
+    # DECON_NO_YZ=1 keeps these canvases on the unfused passes (without it the
+    # 256/512-point ones take the fused Y / axial pass, tests/test_gpu_yz.py)
+    keys = ("DECON_NO_PIPE", "DECON_NO_TMA", "DECON_PIPE_LEAN", "DECON_NO_YZ")
+    for env in ({}, {"DECON_NO_YZ": "1"}, {"DECON_NO_YZ": "1", "DECON_NO_PIPE": "1"},
+                {"DECON_NO_YZ": "1", "DECON_NO_TMA": "1"},
+                {"DECON_NO_YZ": "1", "DECON_PIPE_LEAN": "0"},
+                {"DECON_NO_YZ": "1", "DECON_PIPE_LEAN": "1"}):
         for key in keys:
             monkeypatch.delenv(key, raising=False)
         for key, val in env.items():
@@ -363,3 +368,66 @@ def test_axial_pass_bit_identical_under_concurrent_streams(D):
         for (f0, a0), reps in zip(ref, outs):
             for f, a in reps:
                 assert torch.equal(f, f0) and torch.equal(a, a0)
+
+
+@pytest.mark.parametrize("shape", [(16, 32, 32), (9, 11, 13), (20, 30), (48,)])
+def test_circular_fft_convolver_vs_fp64_oracle(D, shape):
+    # FFTConvolver: circular convolution by the resident OTF of the whole
+    # kernel (deconlib/deconvolution/linops_mlx.py:384-432): OTF, norm,
+    # forward and adjoint (conj OTF) against the FP64 oracle.
+    from oracle import ops
+
+    rng = np.random.default_rng(len(shape) * 100 + shape[-1])
+    k = (rng.random(shape, dtype=np.float32) ** 3).astype(np.float32)
+    x = rng.random(shape, dtype=np.float32)
+    c = D.FFTConvolver(k)
+    o = ops.FFTConvolver(k, dtype=np.float64)
+    assert c.in_shape == c.out_shape == tuple(shape)
+    assert rel(c.forward(x), o.forward(x.astype(np.float64))) < 1e-6
+    assert rel(c.adjoint(x), o.adjoint(x.astype(np.float64))) < 1e-6
+    assert rel(c(x), o.forward(x.astype(np.float64))) < 1e-6
+    def crel(a, b):
+        a = a.detach().cpu().numpy().astype(np.complex128)
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    assert crel(c.otf, o.otf) < 1e-6
+    assert crel(c.otf_conj, np.conj(o.otf)) < 1e-6
+    assert abs(c.operator_norm_sq - o.operator_norm_sq) <= 1e-6 * o.operator_norm_sq
+    cu = D.FFTConvolver(k, normalize=False)
+    ou = ops.FFTConvolver(k, normalize=False, dtype=np.float64)
+    assert rel(cu.forward(x), ou.forward(x.astype(np.float64))) < 1e-6
+
+
+def test_as_numpy_op_pairs(D, g32, g64):
+    # as_numpy_op (deconlib/deconvolution/composition.py:140-159): NumPy in,
+    # NumPy out in native shape, for one of this package's compositions and
+    # for a pure-NumPy operator (tried with the array first, as the reference).
+    c = D.LinearFFTConvolver(g32["psf16"], (16, 32, 32))
+    op = D.compose(D.Crop((16, 32, 32), (12, 26, 28), start=(2, 3, 2)), c)
+    R, Rt = D.as_numpy_op(op)
+    x = g32["conv_x"]
+    fx = R(x)
+    assert isinstance(fx, np.ndarray) and fx.shape == (12, 26, 28) and fx.dtype == np.float32
+    np.testing.assert_array_equal(fx, cpu(op.forward(x)))
+    y = np.random.default_rng(2).random((12, 26, 28), dtype=np.float32)
+    aty = Rt(y)
+    assert isinstance(aty, np.ndarray) and aty.shape == (16, 32, 32)
+    np.testing.assert_array_equal(aty, cpu(op.adjoint(y)))
+    lhs = float(np.sum(fx.astype(np.float64) * y))
+    rhs = float(np.sum(x.astype(np.float64) * aty))
+    assert abs(lhs - rhs) <= 1e-5 * abs(lhs)
+    R2, Rt2 = D.as_numpy_op(c)
+    assert rel(R2(x), g64["conv_fwd"]) < 1e-6
+
+    class NumpyScale:
+        def forward(self, v):
+            assert isinstance(v, np.ndarray)
+            return 2.0 * v
+
+        def adjoint(self, v):
+            assert isinstance(v, np.ndarray)
+            return 2.0 * v
+
+    Rn, Rtn = D.as_numpy_op(NumpyScale())
+    np.testing.assert_array_equal(Rn(x), 2.0 * x)
+    np.testing.assert_array_equal(Rtn(x), 2.0 * x)

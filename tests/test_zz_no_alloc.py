@@ -4,7 +4,9 @@ pipelines that reserve memory up front), called through the C ABI and
 checked against decon_reduce, which takes a caller-allocated workspace.
 
 Both are FP64 sums of the same float32 data in different block orders, so
-they agree to 1e-12 relative (MAX exactly).  Two calls in a row with
+they agree to 1e-12 relative (MAX exactly).  The results are also checked
+against torch's own float64 reductions of the same data (a check that shares
+no code with the library).  Two calls in a row with
 different data show that the shared scratch array keeps nothing stale
 between calls.  This file sorts last so that a run stopping at the first
 failure has already run every other test; it must also pass on its own.
@@ -71,10 +73,15 @@ def test_noalloc_matches_workspace_reduction_twice(lib, n):
             bb = b if op in (DIFFSQ, DOT) else None
             got = _reduce(lib, "noalloc", a, bb, op)
             ref = _reduce(lib, "workspace", a, bb, op)
+            ad, bd = a.double(), b.double()
+            ind = {SUM: ad.sum(), SUMSQ: (ad * ad).sum(), DIFFSQ: ((ad - bd) ** 2).sum(),
+                   DOT: (ad * bd).sum(), MAX: a.max().double()}[op].item()
             if op == MAX:
-                assert got == ref
+                assert got == ref == ind
             else:
-                assert abs(got - ref) <= 1e-12 * max(1.0, abs(ref)), (op, got, ref)
+                scale = max(1.0, abs(ref))
+                assert abs(got - ref) <= 1e-12 * scale, (op, got, ref)
+                assert abs(got - ind) <= 1e-12 * max(1.0, abs(ind)), (op, got, ind)
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(lib):
