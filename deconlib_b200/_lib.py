@@ -52,11 +52,22 @@ _SIGS = {
     "decon_conv_get_otf": (C.c_int, [_p, _p, _p]),
     "decon_conv_forward": (C.c_int, [_p, _p, _p, _p]),
     "decon_conv_adjoint": (C.c_int, [_p, _p, _p, _p]),
+    "decon_conv_forward_down2": (C.c_int, [_p, _p, _p, _p]),
+    "decon_conv_adjoint_up2": (C.c_int, [_p, _p, _p, _p]),
     "decon_rl_setup": (C.c_int, [_p, _p, C.c_float, _p, _p, _p, _p]),
     "decon_rl_iteration": (C.c_int, [_p, _p, C.c_float, _p, _p, _p, _p, _p]),
     "decon_rl_predict": (C.c_int, [_p, _p, C.c_float, _p, _p, _p, _p]),
     "decon_rl_run": (C.c_int, [_p, _p, C.c_float, _p, _p, _p, C.c_int, _p]),
     "decon_pupil_to_psf": (C.c_int, [_p, _p, _p, _i64, _i64, _i64, C.c_int, _p, _p]),
+    "decon_psf_geometry": (C.c_int, [_i64, _i64, C.c_double, C.c_double, C.c_double, C.c_double,
+                                     C.c_double, C.c_int, C.c_double, _p, _p, _p, _p, _p, _p, _p,
+                                     _p, _p, _p, _p]),
+    "decon_psf_pupil": (C.c_int, [_p, _p, _p, _i64, C.c_int, _p, _p]),
+    "decon_psf_defocus": (C.c_int, [_p, _i64, C.c_double, _p, _p]),
+    "decon_psf_index_mismatch": (C.c_int, [_p, _p, _i64, C.c_double, C.c_double, C.c_double,
+                                           C.c_double, _p, _p]),
+    "decon_psf_zernike": (C.c_int, [_p, _p, _p, _i64, C.c_int, C.POINTER(C.c_int),
+                                    C.POINTER(C.c_double), _p, _p]),
     "decon_nlcg_create": (C.c_int, [_p]),
     "decon_nlcg_destroy": (C.c_int, [_p]),
     "decon_nlcg_init": (C.c_int, [_p, _p, _p, _i64, C.c_int, _p]),

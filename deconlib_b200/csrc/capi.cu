@@ -465,6 +465,37 @@ int decon_conv_forward(decon_conv* p, const float* x, float* y, void* stream) {
     return DECON_OK;
 }
 
+// compose(FractionalAreaDownsample(2), LinearFFTConvolver) in one pass
+// sequence: the 2x area sum of the convolution is the X C2R epilogue, its
+// adjoint the X R2C prologue (core_operators.py:222-352 with unit weights).
+static bool down2_ok(const decon_conv* p) {
+    return !p->odd && !((p->N[0] | p->N[1] | p->N[2]) & 1);
+}
+
+int decon_conv_forward_down2(decon_conv* p, const float* x, float* y, void* stream) {
+    if (!p || !x || !y) return fail(DECON_ERR_NULL, "null pointer");
+    if (!down2_ok(p))
+        return fail(DECON_ERR_UNSUPPORTED, "decon_conv_forward_down2: extents must be even (and Fx)");
+    const cudaStream_t s = as_stream(stream);
+    const Win3 w = full_window(p->N);
+    DK_TRY(spectrum_forward(*p, PRO_ARRAY, x, w, 0.f, 0.f, s));
+    DK_TRY(spectrum_filter_back(*p, false, s));
+    DK_TRY(launch_xc2r(*p, EPI_DOWN2, p->s1, w, y, nullptr, nullptr, 0.f, nullptr, nullptr, s));
+    return DECON_OK;
+}
+
+int decon_conv_adjoint_up2(decon_conv* p, const float* y, float* x, void* stream) {
+    if (!p || !x || !y) return fail(DECON_ERR_NULL, "null pointer");
+    if (!down2_ok(p))
+        return fail(DECON_ERR_UNSUPPORTED, "decon_conv_adjoint_up2: extents must be even (and Fx)");
+    const cudaStream_t s = as_stream(stream);
+    const Win3 w = full_window(p->N);
+    DK_TRY(spectrum_forward(*p, PRO_UP2, y, w, 0.f, 0.f, s));
+    DK_TRY(spectrum_filter_back(*p, true, s));
+    DK_TRY(launch_xc2r(*p, EPI_STORE, p->s1, w, x, nullptr, nullptr, 0.f, nullptr, nullptr, s));
+    return DECON_OK;
+}
+
 int decon_conv_adjoint(decon_conv* p, const float* y, float* x, void* stream) {
     if (!p || !x || !y) return fail(DECON_ERR_NULL, "null pointer");
     const cudaStream_t s = as_stream(stream);

@@ -400,6 +400,7 @@ int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cva
         case PRO_CONST: fn = pick_xr2c<PRO_CONST>(a.ax.L); break;
         case PRO_KERNEL: fn = pick_xr2c<PRO_KERNEL>(a.ax.L); break;
         case PRO_RLINIT: fn = pick_xr2c<PRO_RLINIT>(a.ax.L); break;
+        case PRO_UP2: fn = pick_xr2c<PRO_UP2>(a.ax.L); break;
         default: return fail(DECON_ERR_VALUE, "bad prologue %d", pro);
     }
     return launch(fn, nblk, nthr, smem, st, &a, PROF_XR2C);
@@ -467,8 +468,15 @@ int launch_xc2r(const ConvPlan& p, int epi, const float2* in, Win3 win, float* o
         a.fd_L = make_fastdiv(L);
         a.fd_h2 = make_fastdiv(std::max(1, L / 2));
         a.fd_npair = make_fastdiv(L / 2 + 1);
-        a.fd_q4 = make_fastdiv(std::max<int64_t>(1, a.Nx / 4));
+        a.fd_q4 = make_fastdiv(std::max<int64_t>(1, epi == EPI_DOWN2 ? a.Nx / 2 : a.Nx / 4));
         a.fd_Nx = make_fastdiv(a.Nx);
+    }
+    if (epi == EPI_DOWN2) {
+        // whole 2 x 2 x 2 blocks per CTA: T / 2 lines from each of two planes
+        a.vec4 = 0;
+        if (p.odd || (p.N[0] | p.N[1] | p.N[2]) & 1 || a.T < 4 || p.N[1] % (a.T / 2) != 0)
+            return fail(DECON_ERR_UNSUPPORTED, "2x area-sum epilogue: extents must be even and Ny a "
+                                               "multiple of %d", a.T / 2);
     }
     const int nthr = threads_for(a.T, a.ax);
     const int64_t nblk = cdiv(a.nrows, a.T);
@@ -480,6 +488,7 @@ int launch_xc2r(const ConvPlan& p, int epi, const float2* in, Win3 win, float* o
         case EPI_RL_RATIO: fn = pick_xc2r<EPI_RL_RATIO>(a.ax.L); break;
         case EPI_RL_UPDATE: fn = pick_xc2r<EPI_RL_UPDATE>(a.ax.L); break;
         case EPI_PRED: fn = pick_xc2r<EPI_PRED>(a.ax.L); break;
+        case EPI_DOWN2: fn = pick_xc2r<EPI_DOWN2>(a.ax.L); break;
         default: return fail(DECON_ERR_VALUE, "bad epilogue %d", epi);
     }
     return launch(fn, nblk, nthr, smem, st, &a, PROF_XC2R);

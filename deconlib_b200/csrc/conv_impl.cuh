@@ -24,8 +24,12 @@ struct Win3 {
 
 inline Win3 full_window(const int64_t* N) { return Win3{N[0], N[1], N[2], 0, 0, 0}; }
 
-enum Prologue { PRO_ARRAY = 0, PRO_CONST = 1, PRO_KERNEL = 2, PRO_RLINIT = 3 };
-enum Epilogue { EPI_STORE = 0, EPI_RL_RATIO = 1, EPI_RL_UPDATE = 2, EPI_PRED = 3 };
+// PRO_UP2: the input is the coarse (Nz/2, Ny/2, Nx/2) array of a 2x fractional-area
+// downsample and the X pass reads its adjoint (every fine voxel takes its
+// coarse voxel's value).  EPI_DOWN2: the output is the 2x area sum of the
+// convolved volume, written at the coarse shape.
+enum Prologue { PRO_ARRAY = 0, PRO_CONST = 1, PRO_KERNEL = 2, PRO_RLINIT = 3, PRO_UP2 = 4 };
+enum Epilogue { EPI_STORE = 0, EPI_RL_RATIO = 1, EPI_RL_UPDATE = 2, EPI_PRED = 3, EPI_DOWN2 = 4 };
 enum ColMode { COL_FWD = 0, COL_INV = 1, COL_OTF = 2, COL_OTF_CONJ = 3 };
 // kernel classes for decon_profile_start (bit mask)
 enum ProfClass { PROF_XR2C = 1, PROF_COL = 2, PROF_ZOTF = 4, PROF_XC2R = 8 };

@@ -50,6 +50,8 @@ struct decon_pdhg_solver {
         float *w_f, *w_a;
     };
     std::vector<Band> bands;
+    // every axis halved exactly: A and A^T as the fused 2x area-sum passes
+    bool down2 = false;
     std::vector<void*> allocs;
 };
 
@@ -87,6 +89,11 @@ static int pr_band(const decon_pdhg_solver::Band& b, bool adjoint, const float* 
 // axis order (FractionalAreaDownsample.forward, core_operators.py:301-320).
 static int pr_forward(decon_pdhg_solver* s, const float* x, float* out, cudaStream_t st) {
     if (s->bands.empty()) return decon_conv_forward(s->conv, x, out, st);
+    if (s->down2) {
+        const int e = decon_conv_forward_down2(s->conv, x, out, st);
+        if (e != DECON_ERR_UNSUPPORTED) return e;
+        s->down2 = false;
+    }
     DK_TRY(decon_conv_forward(s->conv, x, s->t0, st));
     int64_t shp[3] = {s->N[0], s->N[1], s->N[2]};
     const float* cur = s->t0;
@@ -102,6 +109,11 @@ static int pr_forward(decon_pdhg_solver* s, const float* x, float* out, cudaStre
 // (core_operators.py:322-336), then the convolution adjoint.
 static int pr_adjoint(decon_pdhg_solver* s, const float* y, float* out, cudaStream_t st) {
     if (s->bands.empty()) return decon_conv_adjoint(s->conv, y, out, st);
+    if (s->down2) {
+        const int e = decon_conv_adjoint_up2(s->conv, y, out, st);
+        if (e != DECON_ERR_UNSUPPORTED) return e;
+        s->down2 = false;
+    }
     int64_t shp[3] = {s->M[0], s->M[1], s->M[2]};
     const float* cur = y;
     for (size_t i = 0; i < s->bands.size(); ++i) {
@@ -184,6 +196,8 @@ int decon_pdhg_solver_create(decon_conv* conv, const float* data, const int64_t 
         if (int e = upload_blocking(b.w_a, w_a.data(), w_a.size() * 4)) return bail(e);
         s->bands.push_back(b);
     }
+    s->down2 = s->bands.size() == 3;
+    for (const auto& b : s->bands) s->down2 = s->down2 && b.nl == 2 * b.ns;
     if (s->bands.empty() && (s->M[0] != s->N[0] || s->M[1] != s->N[1] || s->M[2] != s->N[2]))
         return bail(fail(DECON_ERR_VALUE, "decon_pdhg_solver_create: shape mismatch"));
     // buffers

@@ -96,7 +96,23 @@ __global__ void __launch_bounds__(kFftThreads, 3) k_xr2c(XR2CArgs a) {
     const int64_t row0 = (int64_t)blockIdx.x * T;
     // packed points that can be non-zero
     const int nin = a.odd ? (int)(a.Nx < L ? a.Nx : L) : (int)(((a.Nx + 1) >> 1) < L ? ((a.Nx + 1) >> 1) : L);
-    if (PRO == PRO_ARRAY && a.vec4) {
+    if constexpr (PRO == PRO_UP2) {
+        // fine row (z, y) of the adjoint of the 2x area sum: fine x = 2n and
+        // 2n + 1 both take coarse value n of coarse row (z / 2, y / 2), so the
+        // packed point n is (c[n], c[n]) (even Fx, even extents)
+        const int64_t mx = a.Nx >> 1, my = a.Ny >> 1;
+        #pragma unroll 1
+        for (int q = tid; q < T * nin; q += blockDim.x) {
+            const int t = fdiv(q, a.fd_nin), n = q - t * nin;
+            const int64_t row = row0 + t;
+            float v = 0.f;
+            if (row < a.nrows) {
+                const int64_t z = row / a.Ny, y = row - z * a.Ny;
+                v = __ldg(a.in + ((z >> 1) * my + (y >> 1)) * mx + n);
+            }
+            sm[phys(n, t, T)] = make_float2(v, v);
+        }
+    } else if (PRO == PRO_ARRAY && a.vec4) {
         const int q4 = (int)(a.Nx >> 2);  // float4 per row
         const int nq = T * q4;
         constexpr int U = 4;
@@ -220,6 +236,22 @@ __global__ void __launch_bounds__(kFftThreads, 3) k_xr2c(XR2CArgs a) {
 // pass 5: X C2R with fused epilogues
 // ---------------------------------------------------------------------------
 
+// Spectrum row of the CTA's line t: rows blockIdx.x * T + t, or, for the 2x
+// area-sum epilogue, lines t < T / 2 from plane 2k and lines t >= T / 2 from
+// plane 2k + 1 over the same T / 2 y values, so that each CTA holds whole
+// 2 x 2 x 2 blocks.
+template <int EPI>
+__device__ __forceinline__ int64_t c2r_row(const XC2RArgs& a, int T, int t) {
+    if constexpr (EPI == EPI_DOWN2) {
+        const int h = T >> 1;
+        const int64_t b = blockIdx.x, nyb = a.Ny / h;
+        const int64_t k = b / nyb, yb = b - k * nyb;
+        return (2 * k + (t >= h ? 1 : 0)) * a.Ny + yb * h + (t & (h - 1));
+    } else {
+        return (int64_t)blockIdx.x * T + t;
+    }
+}
+
 // The element-wise epilogue on one output voxel i (v already scaled).
 template <int EPI>
 __device__ __forceinline__ void epilogue(const XC2RArgs& a, int64_t i, float v, double& acc) {
@@ -271,7 +303,7 @@ __global__ void __launch_bounds__(kFftThreads, 2) k_xc2r(XC2RArgs a) {
                 t = fdiv(q, a.fd_L);
                 k = q - t * L;
             }
-            const int64_t row = row0 + t;
+            const int64_t row = c2r_row<EPI>(a, T, t);
             float2 Z = make_float2(0.f, 0.f);
             if (row < a.nrows) {
                 // full Hermitian spectrum from the half: X[k] = conj(X[Fx - k])
@@ -294,12 +326,12 @@ __global__ void __launch_bounds__(kFftThreads, 2) k_xc2r(XC2RArgs a) {
             #pragma unroll 1
             for (int q = tid; q < T * M; q += blockDim.x) {
                 const int k = q >> lgT, t = q & (T - 1);
-                const int64_t row = row0 + t;
+                const int64_t row = c2r_row<EPI>(a, T, t);
                 sm[phys(k, t, T)] = row < a.nrows ? a.in[k * a.kstride + row] : make_float2(0.f, 0.f);
             }
             #pragma unroll 1
             for (int t = tid; t < T; t += blockDim.x) {
-                const int64_t row = row0 + t;
+                const int64_t row = c2r_row<EPI>(a, T, t);
                 nyq[t] = row < a.nrows ? a.in[M * a.kstride + row] : make_float2(0.f, 0.f);
             }
         } else {
@@ -314,7 +346,7 @@ __global__ void __launch_bounds__(kFftThreads, 2) k_xc2r(XC2RArgs a) {
                 for (int u = 0; u < U; ++u) {
                     const int c = c0 + u * blockDim.x;
                     const int t = fdiv(c, a.fd_h2);
-                    const int64_t row = row0 + t;
+                    const int64_t row = c2r_row<EPI>(a, T, t);
                     v[u] = (c < nq && row < a.nrows)
                                ? __ldg(reinterpret_cast<const float4*>(a.in + row * a.P) + (c - t * h2))
                                : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -331,7 +363,7 @@ __global__ void __launch_bounds__(kFftThreads, 2) k_xc2r(XC2RArgs a) {
             }
             #pragma unroll 1
             for (int t = tid; t < T; t += blockDim.x) {
-                const int64_t row = row0 + t;
+                const int64_t row = c2r_row<EPI>(a, T, t);
                 const bool ok = row < a.nrows;
                 nyq[t] = ok ? a.in[row * a.P + M] : make_float2(0.f, 0.f);
                 // odd M: the last packed point is not covered by the float4 pairs
@@ -380,13 +412,36 @@ __global__ void __launch_bounds__(kFftThreads, 2) k_xc2r(XC2RArgs a) {
 
     double acc = 0.0;
     const int64_t Nx = a.Nx;
-    if (a.vec4) {
+    if constexpr (EPI == EPI_DOWN2) {
+        // 2x area sum of the scaled output, in the order of the three banded
+        // passes (z pairs, then y pairs, then x pairs; unit weights): line t
+        // holds plane 2k (t < T/2) or 2k + 1, packed point i holds x = 2i, 2i + 1
+        const int h = T >> 1, hq = h >> 1;
+        const int64_t mx = Nx >> 1, my = a.Ny >> 1;
+        const int64_t nyb = a.Ny / h, k = (int64_t)blockIdx.x / nyb, yb = (int64_t)blockIdx.x - k * nyb;
+        const int nq = hq * (int)mx;
+        const float s = a.scale;
+        #pragma unroll 1
+        for (int q = tid; q < nq; q += blockDim.x) {
+            const int j = fdiv(q, a.fd_q4), i = q - j * (int)mx;  // fd_q4 holds mx here
+            const float2 p0 = sm[phys(i, 2 * j, T)], p1 = sm[phys(i, 2 * j + 1, T)];
+            const float2 q0 = sm[phys(i, h + 2 * j, T)], q1 = sm[phys(i, h + 2 * j + 1, T)];
+            // round-to-nearest intrinsics: every product and sum rounded as
+            // the stored output and the separate passes round it (no fma)
+            const float a0x = __fadd_rn(__fmul_rn(p0.x, s), __fmul_rn(q0.x, s));  // z pairs, y = 2j
+            const float a0y = __fadd_rn(__fmul_rn(p0.y, s), __fmul_rn(q0.y, s));
+            const float a1x = __fadd_rn(__fmul_rn(p1.x, s), __fmul_rn(q1.x, s));  // y = 2j + 1
+            const float a1y = __fadd_rn(__fmul_rn(p1.y, s), __fmul_rn(q1.y, s));
+            const float bx = __fadd_rn(a0x, a1x), by = __fadd_rn(a0y, a1y);       // y pairs
+            a.out[(k * my + yb * hq + j) * mx + i] = __fadd_rn(bx, by);           // x pair
+        }
+    } else if (a.vec4) {
         // plain rows, full window: 4 voxels per thread step
         const int q4 = (int)(Nx >> 2), nq = T * q4;
         #pragma unroll 1
         for (int c = tid; c < nq; c += blockDim.x) {
             const int t = fdiv(c, a.fd_q4), x4 = c - t * q4;
-            const int64_t row = row0 + t;
+            const int64_t row = c2r_row<EPI>(a, T, t);
             if (row >= a.nrows) continue;
             const float2 p0 = sm[phys(2 * x4, t, T)], p1 = sm[phys(2 * x4 + 1, t, T)];
             const int64_t i = row * Nx + 4 * x4;
@@ -426,7 +481,7 @@ __global__ void __launch_bounds__(kFftThreads, 2) k_xc2r(XC2RArgs a) {
     } else {
         // window rows: output index of x = 0 per row, once
         if (tid < T) {
-            const int64_t row = row0 + tid;
+            const int64_t row = c2r_row<EPI>(a, T, tid);
             int64_t b = kOutside;
             if (row < a.nrows) {
                 const int64_t z = row / a.Ny, y = row - z * a.Ny;

@@ -57,15 +57,62 @@ class Compose:
         self.in_shape = getattr(inner, "in_shape", None)
         self.out_shape = getattr(outer, "out_shape", None)
         self.operator_norm_sq = float(outer.operator_norm_sq * inner.operator_norm_sq)
+        self._down2 = _down2_plan(outer, inner)
 
     def forward(self, x):
+        if self._down2 is not None:
+            y = self._fused("decon_conv_forward_down2", x, self._down2[1], self._down2[2])
+            if y is not None:
+                return y
         return self.outer.forward(self.inner.forward(x))
 
     def adjoint(self, y):
+        if self._down2 is not None:
+            x = self._fused("decon_conv_adjoint_up2", y, self._down2[2], self._down2[1])
+            if x is not None:
+                return x
         return self.inner.adjoint(self.outer.adjoint(y))
+
+    def _fused(self, name, x, in_shape, out_shape):
+        """The recognised composition FractionalAreaDownsample(2) o
+        LinearFFTConvolver as one pass sequence (the area sum fused into the
+        convolution's last FFT pass, its adjoint into the first); the same
+        float32 values as applying the two operators in turn.  None if the
+        plan cannot (the caller then applies them in turn)."""
+        from .. import _lib
+        from ._device import empty, stream, to_device
+
+        x = to_device(x)
+        if tuple(x.shape) != in_shape:
+            return None
+        out = empty(out_shape)
+        st = getattr(_lib.load(), name)(self._down2[0].plan, _lib.ptr(x), _lib.ptr(out), stream())
+        if st == _lib.ERR_UNSUPPORTED:
+            self._down2 = None
+            return None
+        _lib.check(st)
+        return out
 
     def __call__(self, x):
         return self.forward(x)
+
+
+def _down2_plan(outer, inner):
+    """(conv, N, N / 2) when ``outer`` is a FractionalAreaDownsample that
+    halves every axis of a 3-D LinearFFTConvolver ``inner`` exactly
+    (n_large = 2 n_small, so the band weights are 1 and 0), else None."""
+    from .core_operators import FractionalAreaDownsample
+    from .linops import LinearFFTConvolver
+
+    if not (isinstance(outer, FractionalAreaDownsample) and isinstance(inner, LinearFFTConvolver)):
+        return None
+    n = tuple(inner.signal_shape)
+    if len(n) != 3 or any(v % 2 for v in n) or inner.fft_shape[2] % 2:
+        return None
+    pairs = outer.axis_pairs(n)
+    if sorted((a % 3, nl, ns) for a, nl, ns in pairs) != [(a, n[a], n[a] // 2) for a in range(3)]:
+        return None
+    return inner, n, tuple(v // 2 for v in n)
 
 
 def compose(*ops: LinearOperator) -> LinearOperator:

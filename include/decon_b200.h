@@ -123,6 +123,17 @@ int decon_conv_forward(decon_conv* plan, const float* x, float* y, void* stream)
 /* LinearFFTConvolver.adjoint: correlation with conj(OTF)
  * (linops_mlx.py:526-530). */
 int decon_conv_adjoint(decon_conv* plan, const float* y, float* x, void* stream);
+/* compose(FractionalAreaDownsample(2), LinearFFTConvolver) (composition.py:92-106
+ * over core_operators.py:222-352 and linops_mlx.py:520-530) when the
+ * downsample halves every axis exactly (n_large = 2 n_small): forward writes
+ * the coarse (Nz/2, Ny/2, Nx/2) 2x area sum of the convolution straight from
+ * the last FFT pass; adjoint takes the coarse array and convolves its
+ * adjoint (each fine voxel = its coarse voxel) read in the first FFT pass.
+ * Same float32 values as the operator-by-operator path (unit weights, the
+ * passes' summation order).  DECON_ERR_UNSUPPORTED unless N and Fx are even
+ * (and Ny a multiple of the X pass's half line count). */
+int decon_conv_forward_down2(decon_conv* plan, const float* x, float* y_coarse, void* stream);
+int decon_conv_adjoint_up2(decon_conv* plan, const float* y_coarse, float* x, void* stream);
 
 /* ---- Richardson-Lucy fused iterations (deconvolution/rl_mlx.py:83-185) - */
 
@@ -221,6 +232,41 @@ int decon_nlcg_read(decon_nlcg* h, double* out, void* stream);
  * The first call for an axis length uploads its twiddle table synchronously. */
 int decon_pupil_to_psf(const float* pupil, const double* kz, const double* z, int64_t nz,
                        int64_t ny, int64_t nx, int normalize, float* psf, void* stream);
+
+/* ---- pupil model (psf/optics.py:96-225, psf/pupil.py:17-97,
+ *      psf/aberrations/geometric.py:38-58, psf/aberrations/zernike.py:92-115)
+ * FP64 device arrays of ny * nx values (row-major, DC at the corner). */
+
+/* make_geometry: kx, ky (fftfreq grids), kz = sqrt(max(0, (ni/lambda)^2 -
+ * kr^2)), rho = kr / (NA/lambda) inside the NA disc else 0, phi = atan2(ky,
+ * kx), mask (uint8, kr <= NA/lambda), support (fraction of an oversample x
+ * oversample sub-grid inside the disc; oversample 1..32), cos_theta /
+ * sin_theta (sin = clip(lambda kr / ni, 0, 1)).  smoothing_sigma > 0 applies
+ * the wrapped Gaussian of scipy.ndimage.gaussian_filter (truncate 4, sigma <=
+ * 32) to the support, then clips it to [0, 1]; it needs `scratch` (ny * nx
+ * doubles).  Errors as the reference: spacing and oversample must be
+ * positive, sigma >= 0 (DECON_ERR_VALUE). */
+int decon_psf_geometry(int64_t ny, int64_t nx, double dy, double dx, double wavelength, double na,
+                       double ni, int oversample, double smoothing_sigma, double* kx, double* ky,
+                       double* kz, double* rho, double* phi, uint8_t* mask, double* support,
+                       double* cos_theta, double* sin_theta, double* scratch, void* stream);
+/* make_pupil: pupil (complex128, interleaved) = support, times the aplanatic
+ * factor 1 / sqrt(max(cos theta, eps)) inside the mask when apodize != 0. */
+int decon_psf_pupil(const double* support, const double* cos_theta, const uint8_t* mask, int64_t n,
+                    int apodize, double* pupil, void* stream);
+/* IndexMismatch(depth): pupil *= exp(i 2 pi depth (ns cos t2 - ni cos t1) /
+ * lambda), sin t2 = clip((ni / ns) sin t1, 0, 1) (Gibson-Lanni). */
+int decon_psf_index_mismatch(const double* sin_theta, const double* cos_theta, int64_t n,
+                             double wavelength, double ni, double ns, double depth, double* pupil,
+                             void* stream);
+/* Defocus(z): pupil *= exp(2 pi i kz z) (psf/aberrations/geometric.py:65-96). */
+int decon_psf_defocus(const double* kz, int64_t n, double z, double* pupil, void* stream);
+/* ZernikeAberration: pupil *= exp(i mask sum_q coef[q] Z_{j[q]}(rho, phi)),
+ * orthonormal OSA/ANSI Zernike polynomials, the sum in the given order (zero
+ * coefficients skipped); at most 32 non-zero terms of radial order <= 18.
+ * j and coef are host arrays. */
+int decon_psf_zernike(const double* rho, const double* phi, const uint8_t* mask, int64_t n,
+                      int nterms, const int* j, const double* coef, double* pupil, void* stream);
 
 /* ---- batched RL: many independent problems in one CUDA graph ------------
  * Problem i has its own plan (distinct plans; a plan's scratch spectra serve

@@ -84,3 +84,39 @@ def test_rl_through_fused_pass_matches_unfused(D, monkeypatch):
     monkeypatch.delenv("DECON_NO_YZ", raising=False)
     assert rel(out[0][0], out[1][0]) < 1e-5
     np.testing.assert_allclose(out[0][1], out[1][1], rtol=1e-6)
+
+
+@pytest.mark.parametrize("shape,fft", [((128, 256, 256), None), ((16, 32, 32), None),
+                                       ((20, 64, 48), (64, 128, 96)), ((40, 32, 64), None)])
+def test_fused_area_sum_composition_equals_operators(D, shape, fft):
+    # compose(FractionalAreaDownsample(2), LinearFFTConvolver): the 2x area sum
+    # fused into the last FFT pass and its adjoint into the first give the
+    # float32 values of the two operators applied in turn (unit weights, the
+    # passes' summation order), on fused and unfused column passes alike.
+    rng = np.random.default_rng(sum(shape))
+    k = (rng.random(shape if fft is None else tuple(f - n + 1 for n, f in zip(shape, fft)),
+                    dtype=np.float32) ** 4).astype(np.float32)
+    conv = D.LinearFFTConvolver(k, shape, fft_shape=fft)
+    down = D.FractionalAreaDownsample(2.0)
+    A = D.compose(down, conv)
+    assert A._down2 is not None
+    x = torch.from_numpy(rng.random(shape, dtype=np.float32)).cuda()
+    y = torch.from_numpy(rng.random(tuple(s // 2 for s in shape), dtype=np.float32)).cuda()
+    f1, a1 = A.forward(x), A.adjoint(y)
+    assert A._down2 is not None  # the fused path ran
+    f0 = down.forward(conv.forward(x))
+    a0 = conv.adjoint(down.adjoint(y))
+    assert torch.equal(f1, f0)
+    assert torch.equal(a1, a0)
+
+
+def test_area_sum_composition_falls_back_for_odd_extents(D):
+    rng = np.random.default_rng(1)
+    shape = (10, 33, 40)
+    k = rng.random((5, 7, 9)).astype(np.float32)
+    conv = D.LinearFFTConvolver(k, shape)
+    A = D.compose(D.FractionalAreaDownsample(2.0), conv)
+    assert A._down2 is None
+    x = rng.random(shape, dtype=np.float32)
+    ref = D.FractionalAreaDownsample(2.0).forward(conv.forward(x))
+    assert torch.equal(A.forward(x), ref)

@@ -85,3 +85,25 @@ def test_nlcg_objective_decreases_monotonically():
                             callback=lambda k, f: phis.append(
                                 nlcg.nlcg_objective(np.sqrt(f), conv, obs, 5.0, dtype=np.float64)))
     assert len(phis) == 8 and all(b < a for a, b in zip(phis, phis[1:]))
+
+
+def test_pupil_restatement_matches_reference_pupils():
+    """The oracle's make_geometry / make_pupil / IndexMismatch / Zernike
+    rebuild the four pupils and kz grids the reference wrote into
+    golden_psf.npz (tests/golden/make_golden.py::_run_psf: 525 nm, NA 1.4,
+    ni 1.515, ns 1.334; aberrated cases IndexMismatch(6) then Zernike
+    {SPHERICAL: 0.4, COMA_X: 0.3})."""
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_psf.npz"))
+    cases = [((64, 64), 0.085, False, False), ((36, 50), 0.1, False, True),
+             ((120, 256), 0.065, True, True), ((48, 63), 0.09, True, False)]
+    for i, (shape, dxy, apod, aberr) in enumerate(cases):
+        geom = opsf.make_geometry(shape, dxy, 0.525, 1.4, 1.515)
+        pupil = opsf.make_pupil(geom, apodize=apod)
+        if aberr:
+            pupil = pupil * opsf.index_mismatch(geom, 6.0, 0.525, 1.515, 1.334)
+            pupil = pupil * opsf.zernike_phase_factor(geom, {12: 0.4, 8: 0.3})
+        ref = g[f"psf{i}_pupil"]
+        np.testing.assert_array_equal(geom["kz"], g[f"psf{i}_kz"])
+        assert np.abs(pupil - ref).max() <= 1e-12
