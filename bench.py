@@ -269,6 +269,21 @@ def batch_inputs(D, seed=20):
     return data, psf, tiles, vols
 
 
+def _schedule_table(b):
+    """The autotuner's choice per distinct problem shape: canvas and schedule."""
+    from deconlib_b200.batch import SCHEDULES
+
+    names = {v: k for k, v in SCHEDULES.items()}
+    seen = {}
+    for o, c in zip(b.obs, b.convs):
+        key = "x".join(str(s) for s in o.shape)
+        if key not in seen:
+            seen[key] = {"fft_shape": list(c.fft_shape), "schedule": c.schedule,
+                         "schedule_name": names.get(c.schedule, str(c.schedule)),
+                         "fused_yz": c.fused_yz}
+    return seen
+
+
 def run_batched(D, iters=100):
     """All tiles + volumes in one batch (autotuned canvases, one CUDA graph of
     all iterations) vs the same problems solved one at a time through
@@ -337,6 +352,7 @@ def run_batched(D, iters=100):
            "setup_s": {"inputs": t_inputs, "autotune_plans_otf_init": t_setup,
                        "first_run_with_capture": t_first},
            "fft_shapes_distinct": len(set(b.fft_shapes)),
+           "schedule_per_shape": _schedule_table(b),
            "note": "ms = device time of one replay of the captured graph (every problem, every "
                    "iteration); useful voxels = the stitched volume + the 16 volumes; plain = each "
                    "problem through richardson_lucy_with_operator one after another (wall clock, "

@@ -32,8 +32,8 @@ _SIGS = {
     "decon_launch_count": (_i64, []),
     "decon_device_status": (C.c_int, [_p]),
     "decon_device_status_clear": (C.c_int, [_p]),
-    "decon_pdhg_solver_create": (C.c_int, [_p, _p, _i64p, _dp, C.c_float, C.c_int, _p, C.c_float,
-                                           C.c_float, C.c_int, C.c_int, C.c_double, C.c_double,
+    "decon_pdhg_solver_create": (C.c_int, [_p, _p, _i64p, _dp, C.c_float, C.c_int, _p, C.c_double,
+                                           C.c_double, C.c_int, C.c_int, C.c_double, C.c_double,
                                            C.c_double, C.c_int, C.c_int, C.c_int, _p, C.POINTER(_p)]),
     "decon_pdhg_run": (C.c_int, [_p, C.c_int, _p]),
     "decon_pdhg_solver_x": (C.c_int, [_p, _p, _p]),
@@ -48,6 +48,8 @@ _SIGS = {
     "decon_conv_set_precision": (C.c_int, [_p, C.c_int, _p]),
     "decon_conv_norm_sq": (C.c_int, [_p, _dp]),
     "decon_conv_fused_yz": (C.c_int, [_p, C.POINTER(C.c_int)]),
+    "decon_conv_set_schedule": (C.c_int, [_p, C.c_int]),
+    "decon_conv_get_schedule": (C.c_int, [_p, C.POINTER(C.c_int)]),
     "decon_conv_shape": (C.c_int, [_p, _i64p, _i64p]),
     "decon_conv_get_otf": (C.c_int, [_p, _p, _p]),
     "decon_conv_forward": (C.c_int, [_p, _p, _p, _p]),

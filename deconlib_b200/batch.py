@@ -3,9 +3,13 @@
 A large volume is split into overlapping tiles of uneven shape (a seeded
 core size per tile and axis plus a halo), and independent volumes with their
 own PSFs join the same batch.  Every problem gets its own convolution plan,
-with an FFT canvas chosen by ``autotune_fft_shape`` (each candidate canvas
-is a different radix factorisation of the axes; the fastest measured
-forward + adjoint convolution wins, cached per shape), and K iterations of
+with an FFT canvas and a pass schedule chosen by ``autotune_schedule`` (each
+candidate canvas is a different radix factorisation of the axes, each
+schedule a different family of equivalent FFT kernels: fused or separate
+Y / axial passes, pipelined / one-tile / plain-load column kernels, one- or
+two-CTA axial kernel, radix order, lines per CTA; the fastest measured
+forward + adjoint convolution wins, cached per shape in memory and in a JSON
+file), and K iterations of
 all problems are recorded into one CUDA graph by the native batch runtime
 (``decon_batch_rl_*``): the graph forks the problems over internal streams,
 so one replay advances every tile and volume together.  The stitched result
@@ -20,6 +24,8 @@ different FFT canvas, which the tests bound.
 from __future__ import annotations
 
 import ctypes as C
+import json
+import os
 from dataclasses import dataclass
 from typing import Dict, List, Optional, Sequence, Tuple
 
@@ -31,7 +37,7 @@ from .deconvolution._device import empty, stream, to_device
 from .deconvolution.linops import LinearFFTConvolver, _next_smooth_number
 
 __all__ = ["BatchTile", "plan_uneven_tiles", "fft_shape_candidates", "autotune_fft_shape",
-           "BatchedRL", "batched_tiled_rl"]
+           "autotune_schedule", "SCHEDULES", "tune_cache_path", "BatchedRL", "batched_tiled_rl"]
 
 
 # ---------------------------------------------------------------------------
@@ -144,43 +150,128 @@ def fft_shape_candidates(signal_shape, kernel_shape, max_growth: float = 1.35) -
     return sorted(cands, key=lambda t: (int(np.prod(t)), t))
 
 
-_TUNED: Dict[tuple, tuple] = {}
+# Schedules the autotuner tries per canvas (decon_conv_set_schedule bits):
+# each names an equivalent family of FFT passes, so the winner changes the
+# speed, not the result (beyond FP32 rounding).
+SCHED_NO_FUSED, SCHED_NO_PIPE, SCHED_NO_TMA, SCHED_LEAN_OFF, SCHED_ODD_RADIX, SCHED_HALF_LINES = (
+    1, 2, 4, 8, 16, 32)
+SCHEDULES = {
+    "default": 0,
+    "unfused": SCHED_NO_FUSED,
+    "unfused-one-tile": SCHED_NO_FUSED | SCHED_NO_PIPE,
+    "unfused-plain-loads": SCHED_NO_FUSED | SCHED_NO_TMA,
+    "unfused-one-cta-axial": SCHED_NO_FUSED | SCHED_LEAN_OFF,
+    "odd-radix-first": SCHED_ODD_RADIX,
+    "half-lines": SCHED_HALF_LINES,
+}
+
+_TUNED: Dict[str, tuple] = {}
+_CACHE_LOADED = False
+
+
+def tune_cache_path() -> str:
+    """JSON file the autotuner persists its choices to: $DECON_AUTOTUNE_CACHE,
+    else ~/.cache/deconlib_b200/autotune.json."""
+    return os.environ.get("DECON_AUTOTUNE_CACHE") or os.path.join(
+        os.path.expanduser("~"), ".cache", "deconlib_b200", "autotune.json")
+
+
+def _device_tag() -> str:
+    p = torch.cuda.get_device_properties(torch.cuda.current_device())
+    return f"{p.name}|sm{p.major}{p.minor}|{p.multi_processor_count}"
+
+
+def _load_cache() -> None:
+    global _CACHE_LOADED
+    if _CACHE_LOADED:
+        return
+    _CACHE_LOADED = True
+    try:
+        with open(tune_cache_path()) as f:
+            for k, v in json.load(f).items():
+                _TUNED[k] = (tuple(v["fft_shape"]), int(v["schedule"]), float(v.get("ms", -1.0)))
+    except (OSError, ValueError, KeyError):
+        pass
+
+
+def _save_cache() -> None:
+    path = tune_cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        out = {k: {"fft_shape": list(v[0]), "schedule": v[1], "ms": v[2]} for k, v in _TUNED.items()}
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(out, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass
+
+
+def _time_pair(conv, x, reps) -> float:
+    conv.adjoint(conv.forward(x))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        conv.adjoint(conv.forward(x))
+    e1.record()
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def autotune_schedule(signal_shape, psf, candidates: Optional[List[tuple]] = None,
+                      max_candidates: int = 6, reps: int = 3, schedules=None) -> Tuple[tuple, int]:
+    """Fastest (canvas, schedule) for a LinearFFTConvolver of ``psf`` on
+    ``signal_shape``: every candidate canvas (a different radix factorisation)
+    is timed under every applicable schedule (fused or separate Y / axial
+    passes, pipelined / one-tile / plain-load column kernels, one- or two-CTA
+    axial kernel, radix order, lines per CTA), forward + adjoint with CUDA
+    events after a warm-up.  The winner is cached per (device, signal shape,
+    kernel shape) in memory and in the JSON file of ``tune_cache_path()``;
+    shapes with the same candidate canvases share one timing."""
+    _load_cache()
+    kshape = tuple(int(s) for s in psf.shape)
+    sig = tuple(int(s) for s in signal_shape)
+    dev = _device_tag()
+    key = f"{dev}|{sig}|{kshape}"
+    if key in _TUNED:
+        return _TUNED[key][0], _TUNED[key][1]
+    cands = (candidates or fft_shape_candidates(sig, kshape))[:max_candidates]
+    ckey = f"{dev}|canvases|{tuple(cands)}"
+    if ckey in _TUNED:
+        _TUNED[key] = _TUNED[ckey]
+        _save_cache()
+        return _TUNED[key][0], _TUNED[key][1]
+    scheds = list(SCHEDULES.values()) if schedules is None else list(schedules)
+    x = empty(sig)
+    x.fill_(1.0)
+    best, best_ms = (tuple(cands[0]), 0), float("inf")
+    for fs in cands:
+        conv = LinearFFTConvolver(psf, sig, fft_shape=fs)
+        fused = conv.fused_yz
+        seen = set()
+        for sc in scheds:
+            # the fused pass ignores the column-kernel bits; skip duplicates
+            eff = sc if not (fused and not sc & SCHED_NO_FUSED) else sc & (SCHED_ODD_RADIX | SCHED_HALF_LINES)
+            if not fused:
+                eff &= ~SCHED_NO_FUSED
+            if eff in seen:
+                continue
+            seen.add(eff)
+            conv.set_schedule(eff)
+            ms = _time_pair(conv, x, reps)
+            if ms < best_ms:
+                best, best_ms = (tuple(fs), eff), ms
+        del conv
+    _TUNED[key] = _TUNED[ckey] = (best[0], best[1], best_ms)
+    _save_cache()
+    return best
 
 
 def autotune_fft_shape(signal_shape, psf, candidates: Optional[List[tuple]] = None,
                        max_candidates: int = 6, reps: int = 3) -> tuple:
-    """Fastest canvas for a LinearFFTConvolver of ``psf`` on ``signal_shape``:
-    each candidate's forward + adjoint pair is timed with CUDA events after a
-    warm-up; the winner is cached per (signal shape, kernel shape) and per
-    candidate list, so shapes with the same candidate canvases are timed once."""
-    kshape = tuple(int(s) for s in psf.shape)
-    key = (tuple(int(s) for s in signal_shape), kshape)
-    if key in _TUNED:
-        return _TUNED[key]
-    cands = (candidates or fft_shape_candidates(signal_shape, kshape))[:max_candidates]
-    # tiles of nearby shapes share their candidate canvases: one timing serves them all
-    ckey = ("canvases", tuple(cands))
-    if ckey in _TUNED:
-        _TUNED[key] = _TUNED[ckey]
-        return _TUNED[key]
-    x = empty(key[0])
-    x.fill_(1.0)
-    best, best_ms = cands[0], float("inf")
-    for fs in cands:
-        conv = LinearFFTConvolver(psf, key[0], fft_shape=fs)
-        conv.adjoint(conv.forward(x))
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(reps):
-            conv.adjoint(conv.forward(x))
-        e1.record()
-        e1.synchronize()
-        ms = e0.elapsed_time(e1) / reps
-        if ms < best_ms:
-            best, best_ms = fs, ms
-        del conv
-    _TUNED[key] = _TUNED[ckey] = tuple(best)
-    return _TUNED[key]
+    """The canvas of ``autotune_schedule`` (kept for callers that choose the
+    canvas only)."""
+    return autotune_schedule(signal_shape, psf, candidates, max_candidates, reps)[0]
 
 
 # ---------------------------------------------------------------------------
@@ -208,13 +299,17 @@ class BatchedRL:
         bgs = list(background) if isinstance(background, (list, tuple)) else [float(background)] * n
         self.obs = [to_device(o) for o, _ in problems]
         psfs = [p for _, p in problems]
+        scheds = [0] * n
         if isinstance(fft_shapes, str) and fft_shapes == "auto":
-            fft_shapes = [autotune_fft_shape(tuple(o.shape), p) for o, p in zip(self.obs, psfs)]
+            tuned = [autotune_schedule(tuple(o.shape), p) for o, p in zip(self.obs, psfs)]
+            fft_shapes = [t[0] for t in tuned]
+            scheds = [t[1] for t in tuned]
         elif fft_shapes is None:
             fft_shapes = [None] * n
-        self.convs = [LinearFFTConvolver(p, tuple(o.shape), fft_shape=fs)
-                      for o, p, fs in zip(self.obs, psfs, fft_shapes)]
+        self.convs = [LinearFFTConvolver(p, tuple(o.shape), fft_shape=fs, schedule=sc)
+                      for o, p, fs, sc in zip(self.obs, psfs, fft_shapes, scheds)]
         self.fft_shapes = [c.fft_shape for c in self.convs]
+        self.schedules = [c.schedule for c in self.convs]
         self.x = [empty(o.shape) for o in self.obs]
         self.sens = [empty(o.shape) for o in self.obs]
         self.ratio = [empty(o.shape) for o in self.obs]

@@ -312,9 +312,9 @@ static int conv_create_impl(const float* kernel, const int64_t kshape[3],
                 T *= 2;
             return T;
         };
-        p->T_x = lines(p->ax_x.L, 32);
-        p->T_y = lines(p->ax_y.L, 16);
-        p->T_z = lines(p->ax_z.L, 16);
+        p->T_x = p->T_x0 = lines(p->ax_x.L, 32);
+        p->T_y = p->T_y0 = lines(p->ax_y.L, 16);
+        p->T_z = p->T_z0 = lines(p->ax_z.L, 16);
     }
     int st;
     const cudaStream_t s = as_stream(stream);
@@ -424,6 +424,36 @@ int decon_conv_destroy(decon_conv* p) {
     free_plan(p);
     if (cur != p->device) cudaSetDevice(cur);
     delete p;
+    return DECON_OK;
+}
+
+int decon_conv_set_schedule(decon_conv* p, int sched) {
+    if (!p) return fail(DECON_ERR_NULL, "null plan");
+    if (sched < 0 || sched > 63) return fail(DECON_ERR_VALUE, "schedule bits out of range: %d", sched);
+    // radix plans and lines per CTA of the runtime-length axes; the twiddle
+    // tables depend on the length only and stay
+    const int order = (sched & DECON_SCHED_ODD_RADIX) ? 1 : 0;
+    Axis* axes[3] = {&p->ax_x, &p->ax_y, &p->ax_z};
+    int* lines[3] = {&p->T_x, &p->T_y, &p->T_z};
+    const int lines0[3] = {p->T_x0, p->T_y0, p->T_z0};
+    for (int i = 0; i < 3; ++i) {
+        Axis a;
+        const int L = axes[i]->L;
+        if (!plan_axis(L, a, order)) return fail(DECON_ERR_UNSUPPORTED, "radix plan failed");
+        a.tw = axes[i]->tw;
+        a.tws = axes[i]->tws;
+        *axes[i] = a;
+        const bool runtime = !(L == 64 || L == 128 || L == 256 || L == 512 || L == 1024);
+        *lines[i] = (runtime && (sched & DECON_SCHED_HALF_LINES) && lines0[i] >= 2) ? lines0[i] / 2
+                                                                                  : lines0[i];
+    }
+    p->sched = sched;
+    return DECON_OK;
+}
+
+int decon_conv_get_schedule(const decon_conv* p, int* sched) {
+    if (!p || !sched) return fail(DECON_ERR_NULL, "null pointer");
+    *sched = p->sched;
     return DECON_OK;
 }
 

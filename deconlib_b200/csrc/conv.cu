@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(kFftThreads, (LS >= 512 ? 1 : 2)) k_colfft_tma
 // host: axis planning and launches
 // ---------------------------------------------------------------------------
 
-bool plan_axis(int L, Axis& ax) {
+bool plan_axis(int L, Axis& ax, int order) {
     ax = Axis{};
     ax.L = L;
     int n = L, e2 = 0;
@@ -167,12 +167,15 @@ bool plan_axis(int L, Axis& ax) {
         r.push_back(4);
     }
     for (int i = 0; i < n8; ++i) r.insert(r.begin(), 8);
+    std::vector<int> odd;
     for (int p : {5, 3, 7}) {
         while (n % p == 0) {
             n /= p;
-            r.push_back(p);
+            odd.push_back(p);
         }
     }
+    if (order == 1) r.insert(r.begin(), odd.begin(), odd.end());
+    else r.insert(r.end(), odd.begin(), odd.end());
     if (n != 1 || (int)r.size() > kMaxStages) return false;
     ax.nst = (int)r.size();
     for (int i = 0; i < ax.nst; ++i) ax.rad |= (unsigned long long)r[i] << (4 * i);
@@ -581,8 +584,10 @@ static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const C
     // axial pass of length 256: the lean two-CTA kernel (measured 153 vs 166 us
     // at 128x256x256 on the B200); DECON_PIPE_LEAN=0 / 1 overrides
     const char* le = getenv("DECON_PIPE_LEAN");
-    const bool lean = otf_mode && !h16 && (le ? le[0] == '1' : ax.L == 256);
-    void* fn = getenv("DECON_NO_PIPE") ? nullptr : pick_pipe(ax.L, mode, nin, nout, &R, &split, h16, lean);
+    const bool lean = otf_mode && !h16 &&
+                      (le ? le[0] == '1' : (ax.L == 256 && !(p.sched & DECON_SCHED_LEAN_OFF)));
+    const bool no_pipe = getenv("DECON_NO_PIPE") || (p.sched & DECON_SCHED_NO_PIPE);
+    void* fn = no_pipe ? nullptr : pick_pipe(ax.L, mode, nin, nout, &R, &split, h16, lean);
     if (!fn) return false;
     PipeArgs a;
     memset(&a, 0, sizeof(a));
@@ -624,7 +629,8 @@ static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const C
 }
 
 bool zpass_pipelined(const ConvPlan& p) {
-    if (!p.tma_z || getenv("DECON_NO_PIPE")) return false;
+    if (!p.tma_z || getenv("DECON_NO_PIPE") || (p.sched & (DECON_SCHED_NO_PIPE | DECON_SCHED_NO_TMA)))
+        return false;
     int R = 0, split = 0;
     return pick_pipe(p.ax_z.L, COL_OTF, (int)p.N[0], (int)p.N[0], &R, &split) != nullptr;
 }
@@ -671,7 +677,8 @@ bool yz_supported(const int64_t N[3], const int64_t F[3]) {
 }
 
 bool use_yz(const ConvPlan& p) {
-    return p.otft != nullptr && p.precision == 0 && getenv("DECON_NO_YZ") == nullptr;
+    return p.otft != nullptr && p.precision == 0 && !(p.sched & DECON_SCHED_NO_FUSED) &&
+           getenv("DECON_NO_YZ") == nullptr;
 }
 
 // out[(kx * Fy + ky) * Fz + kz] = otf[(kz * Fy + ky) * P + kx]: 32 x 32 tiles
@@ -760,7 +767,7 @@ int spectrum_forward(const ConvPlan& p, int pro, const float* in, Win3 win, floa
     const int64_t Nz = p.N[0], Ny = p.N[1], Fy = p.F[1], P = p.P;
     if (use_yz(p)) return launch_xr2c(p, pro, in, win, cval, bg, Nz, p.s1, st, Nz * Ny);
     DK_TRY(launch_xr2c(p, pro, in, win, cval, bg, Nz, p.s1, st));
-    if (p.tma_y) {
+    if (p.tma_y && !(p.sched & DECON_SCHED_NO_TMA)) {
         DK_TRY(launch_col_tma(p, p.ax_y, COL_FWD, p.tm_s1_j1, 1, p.s1_box, (int)Ny, p.tm_s2_j1, 1,
                               p.s2y_box, (int)Fy, Nz, st));
     } else {
@@ -775,14 +782,15 @@ int spectrum_filter_back(const ConvPlan& p, bool adjoint, cudaStream_t st) {
     if (use_yz(p)) return launch_yz(p, adjoint, st);
     const int64_t Nz = p.N[0], Ny = p.N[1], Fy = p.F[1], P = p.P;
     const int mode = adjoint ? COL_OTF_CONJ : COL_OTF;
-    if (p.tma_z) {
+    const bool tma = !(p.sched & DECON_SCHED_NO_TMA);
+    if (p.tma_z && tma) {
         DK_TRY(launch_col_tma(p, p.ax_z, mode, p.tm_s2_j2, 2, p.s2z_box, (int)Nz, p.tm_s2_j2, 2,
                               p.s2z_box, (int)Nz, Fy, st));
     } else {
         DK_TRY(launch_col(p, p.ax_z, p.T_z, mode, p.s2, P, Fy * P, (int)Nz, p.s2, P, Fy * P,
                           (int)Nz, Fy, st));
     }
-    if (p.tma_y) {
+    if (p.tma_y && tma) {
         DK_TRY(launch_col_tma(p, p.ax_y, COL_INV, p.tm_s2_j1, 1, p.s2y_box, (int)Fy, p.tm_s1_j1, 1,
                               p.s1_box, (int)Ny, Nz, st));
     } else {

@@ -131,6 +131,11 @@ struct ConvPlan {
     // [Hx][Fy][Fz]; the spectrum between the X passes is then kx-major too
     // ([Hx][Nz][Ny] in s1).  nullptr: the canvas takes the unfused passes.
     float2* otft = nullptr;
+    // Schedule (decon_conv_set_schedule): DECON_SCHED_* bits choosing among
+    // equivalent pass families; T*_0 / ax*_0 keep the default lines per CTA
+    // and radix plans the schedule modifies.
+    int sched = 0;
+    int T_x0 = 0, T_y0 = 0, T_z0 = 0;
 };
 
 // Canvas and signal extents the fused Y / axial pass implements (Fy in {256,

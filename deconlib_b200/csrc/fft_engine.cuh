@@ -322,8 +322,9 @@ __device__ __forceinline__ void fft_lines(float2* buf, int T, int t, int jb, con
 // Lengths with a compile-time path; others use the runtime radix switch.
 #define DK_STATIC_LENGTHS(X) X(64) X(128) X(256) X(512) X(1024)
 
-// Host: factor L into supported radices (8s first, then 4/2, 5, 3, 7).
+// Host: factor L into supported radices (order 0: 8s first, then 4/2, 5, 3,
+// 7; order 1: the odd radices 5, 3, 7 first, then the power-of-two stages).
 // Returns false if L has a prime factor other than 2, 3, 5, 7.
-bool plan_axis(int L, Axis& ax);
+bool plan_axis(int L, Axis& ax, int order = 0);
 
 }  // namespace dk

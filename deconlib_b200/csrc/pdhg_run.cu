@@ -32,7 +32,8 @@ struct decon_pdhg_solver {
     decon_pdhg* state = nullptr;
     int64_t N[3] = {1, 1, 1}, M[3] = {1, 1, 1};
     int64_t n = 0, m = 0;
-    float bg = 0.f, r = 1.f, alpha = 0.f;
+    float bg = 0.f, r = 1.f, alpha = 0.f;  // float32 copies the kernels take
+    double alpha_d = 0.0;                  // the loss weight in FP64
     int loss = 0, norm = 0, eval_interval = 10, num_iter = 0;
     int k = 0;  // iterations queued so far
     // device buffers
@@ -130,7 +131,7 @@ extern "C" {
 
 int decon_pdhg_solver_create(decon_conv* conv, const float* data, const int64_t data_shape[3],
                              const double scale[3], float background, int loss_type,
-                             const float* x0, float r, float alpha, int norm, int num_iter,
+                             const float* x0, double r, double alpha, int norm, int num_iter,
                              double delta, double eta, double tol, int min_iter, int patience,
                              int eval_interval, void* stream, decon_pdhg_solver** out) {
     using namespace dk;
@@ -160,8 +161,9 @@ int decon_pdhg_solver_create(decon_conv* conv, const float* data, const int64_t 
     s->n = s->N[0] * s->N[1] * s->N[2];
     s->m = s->M[0] * s->M[1] * s->M[2];
     s->bg = background;
-    s->r = r;
-    s->alpha = alpha;
+    s->r = (float)r;
+    s->alpha = (float)alpha;
+    s->alpha_d = alpha;
     s->loss = loss_type;
     s->norm = norm;
     s->eval_interval = eval_interval;
@@ -227,7 +229,7 @@ int decon_pdhg_solver_create(decon_conv* conv, const float* data, const int64_t 
     }
     // state: step_scale = 0.99 / sqrt(||A||^2 + ||H||^2) (pdhg_mlx.py:697-700)
     const double a_norm = plain ? conv->norm_sq : down_norm * conv->norm_sq;
-    const double rr = (double)r;
+    const double rr = r;
     const double h_norm = 16.0 * rr * rr * rr * rr + 4.0 * rr * rr + 34.0;
     const double step_scale = 0.99 / std::sqrt(a_norm + h_norm);
     if (int e = decon_pdhg_create(num_iter, step_scale, delta, eta, tol, min_iter, patience, &s->state))
@@ -279,7 +281,7 @@ int decon_pdhg_run(decon_pdhg_solver* s, int iterations, void* stream) {
         DK_TRY(decon_pdhg_step(h, st));
         if ((k + 1) % s->eval_interval == 0)
             DK_TRY(decon_pdhg_hess_loss(h, axn, s->data, s->bg, s->loss, s->m, xn, shp, s->r,
-                                        s->norm, (double)s->alpha, k, st));
+                                        s->norm, s->alpha_d, k, st));
         s->k = k + 1;
     }
     return DECON_OK;

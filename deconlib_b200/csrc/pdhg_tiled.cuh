@@ -74,7 +74,7 @@ struct Edge {
 // d1_cen_adj along a of (inner) then b of a staged component; a/b steps are
 // in-tile offsets (da, db are the index steps of axes a and b; planes for b = z).
 __device__ __forceinline__ float inner_s(const float* p, int c, int da, float slo, float shi, float w) {
-    return (slo * (p[c - da] * w) - shi * (p[c + da] * w)) / 2.f;
+    return __fsub_rn(slo * wmul(p[c - da], w), shi * wmul(p[c + da], w)) / 2.f;
 }
 
 // Hessian3D.adjoint at tile-local (ly, lx) from staged components:
@@ -85,20 +85,20 @@ __device__ __forceinline__ float hess_adj_smem(const float* g0m, const float* g0
                                                const float* g4m, const float* g4p, const float* g5,
                                                int ly, int lx, const Edge& e, const float w[6]) {
     const int c = ly * kHX + lx;
-    const float azz = d2v(g0m[c] * w[0], g0c[c] * w[0], g0p[c] * w[0]);
-    const float ayy = d2v(g1[c - kHX] * w[1], g1[c] * w[1], g1[c + kHX] * w[1]);
-    const float axx = d2v(g2[c - 1] * w[2], g2[c] * w[2], g2[c + 1] * w[2]);
+    const float azz = d2v(wmul(g0m[c], w[0]), wmul(g0c[c], w[0]), wmul(g0p[c], w[0]));
+    const float ayy = d2v(wmul(g1[c - kHX], w[1]), wmul(g1[c], w[1]), wmul(g1[c + kHX], w[1]));
+    const float axx = d2v(wmul(g2[c - 1], w[2]), wmul(g2[c], w[2]), wmul(g2[c + 1], w[2]));
     // yz: outer z (planes; at a z edge the staged neighbour plane is plane z
     // itself and the row is negated), inner y
-    const float ayz = (e.zlo * inner_s(g3m, c, kHX, e.ylo, e.yhi, w[3]) -
-                       e.zhi * inner_s(g3p, c, kHX, e.ylo, e.yhi, w[3])) / 2.f;
+    const float ayz = __fsub_rn(e.zlo * inner_s(g3m, c, kHX, e.ylo, e.yhi, w[3]),
+                                e.zhi * inner_s(g3p, c, kHX, e.ylo, e.yhi, w[3])) / 2.f;
     // xz: outer z, inner x
-    const float axz = (e.zlo * inner_s(g4m, c, 1, e.xlo, e.xhi, w[4]) -
-                       e.zhi * inner_s(g4p, c, 1, e.xlo, e.xhi, w[4])) / 2.f;
+    const float axz = __fsub_rn(e.zlo * inner_s(g4m, c, 1, e.xlo, e.xhi, w[4]),
+                                e.zhi * inner_s(g4p, c, 1, e.xlo, e.xhi, w[4])) / 2.f;
     // xy: outer y (rows c -+ kHX in plane z), inner x
-    const float axy = (e.ylo * inner_s(g5, c - kHX, 1, e.xlo, e.xhi, w[5]) -
-                       e.yhi * inner_s(g5, c + kHX, 1, e.xlo, e.xhi, w[5])) / 2.f;
-    return ((((azz + ayy) + axx) + ayz) + axz) + axy;
+    const float axy = __fsub_rn(e.ylo * inner_s(g5, c - kHX, 1, e.xlo, e.xhi, w[5]),
+                                e.yhi * inner_s(g5, c + kHX, 1, e.xlo, e.xhi, w[5])) / 2.f;
+    return __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(azz, ayy), axx), ayz), axz), axy);
 }
 
 // ---- software pipeline ------------------------------------------------------
@@ -288,19 +288,19 @@ __global__ void __launch_bounds__(256) k_hess_dual_p(PdhgDev* s, float* y2,
     for (int c = 0; c < 6; ++c) cs.p[c] = y2 + c * n;
     const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
     hess_pipeline<2, 1, 6, kDualDepth>(
-        d, hs, cs, [&](const float* r, float* o) { o[0] = r[0] + th * (r[0] - r[1]); },
+        d, hs, cs, [&](const float* r, float* o) { o[0] = xbar_of(r[0], r[1], th); },
         [&](int64_t, int64_t, int64_t, int64_t i, const float* cv, const float* const* W) {
             float h[6];
             hess6_smem(W[0], W[1], W[2], ty + 1, tx + 1, w.w, h);
             if constexpr (NORM == 0) {
 #pragma unroll
-                for (int c = 0; c < 6; ++c) y2[c * n + i] = fminf(fmaxf(cv[c] + sg * h[c], -alpha), alpha);
+                for (int c = 0; c < 6; ++c) y2[c * n + i] = fminf(fmaxf(dual_arg(cv[c], sg, h[c]), -alpha), alpha);
             } else {
                 float v[6];
                 float ss = 0.f;
 #pragma unroll
                 for (int c = 0; c < 6; ++c) {
-                    v[c] = cv[c] + sg * h[c];
+                    v[c] = dual_arg(cv[c], sg, h[c]);
                     ss += v[c] * v[c];
                 }
                 const float sc = fmaxf(sqrtf(ss + 1e-12f) / alpha, 1.f);
@@ -467,8 +467,8 @@ __global__ void __launch_bounds__(256) k_hess_primal_t(PdhgDev* s, const float* 
     double dx2 = 0.0, xc2 = 0.0, xn2 = 0.0;
     hess_adj_walk(y2, d, w, [&](int64_t i, float lt) {
         const float a = xc[i];
-        const float gr = aty[i] + lt;
-        const float v = fmaxf(a - tau * gr, 0.f);
+        const float gr = __fadd_rn(aty[i], lt);
+        const float v = primal_of(a, tau, gr);
         xn[i] = v;
         const float dd = v - a;
         dx2 += (double)dd * dd;
@@ -597,12 +597,12 @@ __global__ void __launch_bounds__(256) k_hess_dual_primal(
                 float v[6];
                 if constexpr (NORM == 0) {
 #pragma unroll
-                    for (int c = 0; c < 6; ++c) v[c] = fminf(fmaxf(__ldg(y2_in + c * n + i) + sg * h[c], -alpha), alpha);
+                    for (int c = 0; c < 6; ++c) v[c] = fminf(fmaxf(dual_arg(__ldg(y2_in + c * n + i), sg, h[c]), -alpha), alpha);
                 } else {
                     float ss = 0.f;
 #pragma unroll
                     for (int c = 0; c < 6; ++c) {
-                        v[c] = __ldg(y2_in + c * n + i) + sg * h[c];
+                        v[c] = dual_arg(__ldg(y2_in + c * n + i), sg, h[c]);
                         ss += v[c] * v[c];
                     }
                     const float sc = fmaxf(sqrtf(ss + 1e-12f) / alpha, 1.f);
@@ -629,8 +629,8 @@ __global__ void __launch_bounds__(256) k_hess_dual_primal(
                                            ty + 1, tx + 1, e, w.w);
             const int64_t i = z * plane + ipl;
             const float a = xc[i];
-            const float gr = aty[i] + lt;
-            const float v = fmaxf(a - tau * gr, 0.f);
+            const float gr = __fadd_rn(aty[i], lt);
+            const float v = primal_of(a, tau, gr);
             xn[i] = v;
             const float dd = v - a;
             dx2 += (double)dd * dd;
@@ -645,7 +645,7 @@ __global__ void __launch_bounds__(256) k_hess_dual_primal(
                 if (!k2[u]) continue;
                 const int64_t i = p * plane + o2[u];
                 const float a = __ldg(xc + i);
-                dst[tid + u * 256] = a + th * (a - __ldg(xp + i));
+                dst[tid + u * 256] = xbar_of(a, __ldg(xp + i), th);
             }
             __syncthreads();
             // y2_out planes whose x_bar neighbourhood is complete

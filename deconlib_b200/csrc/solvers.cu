@@ -45,8 +45,8 @@ __global__ void __launch_bounds__(256) k_dual_data(PdhgDev* s, float* __restrict
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
          i += (int64_t)gridDim.x * blockDim.x) {
         const float a = axc[i];
-        const float axbar = a + th * (a - axp[i]);
-        const float arg = y1[i] + sg * axbar;
+        const float axbar = xbar_of(a, axp[i], th);
+        const float arg = dual_arg(y1[i], sg, axbar);
         const float d = data[i];
         float out;
         if constexpr (LOSS == 0) {
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(256) k_dual_reg(PdhgDev* s, float* __restrict_
             // prox_l1_dual: clip(y, -alpha, alpha)
             for (int c = 0; c < ncomp; ++c) {
                 const int64_t j = (int64_t)c * n + i;
-                y2[j] = fminf(fmaxf(y2[j] + sg * lxbar[j], -alpha), alpha);
+                y2[j] = fminf(fmaxf(dual_arg(y2[j], sg, lxbar[j]), -alpha), alpha);
             }
         } else {
             // prox_l1_2_dual: y / max(sqrt(sum_c y^2 + 1e-12) / alpha, 1)
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(256) k_dual_reg(PdhgDev* s, float* __restrict_
             float ss = 0.f;
             for (int c = 0; c < ncomp; ++c) {
                 const int64_t j = (int64_t)c * n + i;
-                v[c] = y2[j] + sg * lxbar[j];
+                v[c] = dual_arg(y2[j], sg, lxbar[j]);
                 ss += v[c] * v[c];
             }
             const float sc = fmaxf(sqrtf(ss + 1e-12f) / alpha, 1.f);
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(256) k_xbar(PdhgDev* s, const float* __restric
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const float a = xc[i];
-        xb[i] = a + th * (a - xp[i]);
+        xb[i] = xbar_of(a, xp[i], th);
     }
 }
 
@@ -121,8 +121,8 @@ __global__ void __launch_bounds__(256) k_primal(PdhgDev* s, const float* __restr
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const float a = xc[i];
-        const float g = aty[i] + (lty ? lty[i] : 0.f);
-        const float v = fmaxf(a - tau * g, 0.f);
+        const float g = __fadd_rn(aty[i], lty ? lty[i] : 0.f);
+        const float v = primal_of(a, tau, g);
         xn[i] = v;
         const float d = v - a;
         dx2 += (double)d * d;
@@ -305,7 +305,7 @@ struct XbarField {  // x_bar = x + theta (x - x_prev)
     __device__ __forceinline__ float operator()(int64_t z, int64_t y, int64_t x) const {
         const int64_t i = (z * ny + y) * nx + x;
         const float a = __ldg(xc + i);
-        return a + th * (a - __ldg(xp + i));
+        return xbar_of(a, __ldg(xp + i), th);
     }
 };
 
@@ -346,14 +346,14 @@ __global__ void __launch_bounds__(256) k_hess_dual(PdhgDev* s, float* __restrict
 #pragma unroll
             for (int c = 0; c < 6; ++c) {
                 const int64_t j = c * n + i;
-                y2[j] = fminf(fmaxf(y2[j] + sg * h[c], -alpha), alpha);
+                y2[j] = fminf(fmaxf(dual_arg(y2[j], sg, h[c]), -alpha), alpha);
             }
         } else {
             float v[6];
             float ss = 0.f;
 #pragma unroll
             for (int c = 0; c < 6; ++c) {
-                v[c] = y2[c * n + i] + sg * h[c];
+                v[c] = dual_arg(y2[c * n + i], sg, h[c]);
                 ss += v[c] * v[c];
             }
             const float sc = fmaxf(sqrtf(ss + 1e-12f) / alpha, 1.f);
@@ -376,8 +376,8 @@ __global__ void __launch_bounds__(256) k_hess_primal(PdhgDev* s, const float* __
          i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t x = i % d.nx, t = i / d.nx, y = t % d.ny, z = t / d.ny;
         const float a = xc[i];
-        const float g = aty[i] + hess_adj_at(y2, z, y, x, d, w.w);
-        const float v = fmaxf(a - tau * g, 0.f);
+        const float g = __fadd_rn(aty[i], hess_adj_at(y2, z, y, x, d, w.w));
+        const float v = primal_of(a, tau, g);
         xn[i] = v;
         const float dd = v - a;
         dx2 += (double)dd * dd;

@@ -11,7 +11,28 @@ namespace dk {
 __device__ __forceinline__ int64_t clampi(int64_t v, int64_t n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
 
 // d2 along one axis (linops_core_mlx.py:66-76): (f[i-1] - 2 f[i]) + f[i+1].
-__device__ __forceinline__ float d2v(float fm, float f0, float fp) { return fm - 2.f * f0 + fp; }
+// The stencil arithmetic uses round-to-nearest intrinsics throughout: every
+// product and sum is rounded as the reference's float32 array operations
+// round it, and no multiply-add is contracted, so every kernel that inlines
+// these functions (fused or not) produces the same bits.
+__device__ __forceinline__ float d2v(float fm, float f0, float fp) {
+    return __fadd_rn(__fsub_rn(fm, __fmul_rn(2.f, f0)), fp);
+}
+// w * v rounded (a weighted component value)
+__device__ __forceinline__ float wmul(float v, float w) { return __fmul_rn(v, w); }
+// The element-wise PDHG updates, each operation rounded as the reference's
+// float32 arrays round it (pdhg_mlx.py:724, 733, 742, 841):
+//   x_bar = x + theta (x - x_prev), dual argument y + sigma K x_bar,
+//   x_new = max(0, x - tau g)
+__device__ __forceinline__ float xbar_of(float x, float xp, float th) {
+    return __fadd_rn(x, __fmul_rn(th, __fsub_rn(x, xp)));
+}
+__device__ __forceinline__ float dual_arg(float y, float sg, float kx) {
+    return __fadd_rn(y, __fmul_rn(sg, kx));
+}
+__device__ __forceinline__ float primal_of(float x, float tau, float g) {
+    return fmaxf(__fsub_rn(x, __fmul_rn(tau, g)), 0.f);
+}
 
 struct Dims {
     int64_t nz, ny, nx;
@@ -51,12 +72,12 @@ __device__ __forceinline__ void hess6(const F& f, int64_t z, int64_t y, int64_t 
 // component weight (H_w = H * w, linops_mlx.py:250), the float32 product the
 // reference forms.
 __device__ __forceinline__ float gext(const float* g, int64_t j, int64_t n, int64_t s, float w) {
-    return j < 0 ? -(__ldg(g) * w) : (j >= n ? -(__ldg(g + (n - 1) * s) * w) : __ldg(g + j * s) * w);
+    return j < 0 ? -wmul(__ldg(g), w) : (j >= n ? -wmul(__ldg(g + (n - 1) * s), w) : wmul(__ldg(g + j * s), w));
 }
 
 __device__ __forceinline__ float inner_adj(const float* g, int64_t ia, int64_t na, int64_t sa,
                                            float w) {
-    return (gext(g, ia - 1, na, sa, w) - gext(g, ia + 1, na, sa, w)) / 2.f;
+    return __fsub_rn(gext(g, ia - 1, na, sa, w), gext(g, ia + 1, na, sa, w)) / 2.f;
 }
 
 // d1_cen_adj along axis b of (d1_cen_adj along axis a of H) at (ib, ia) of a
@@ -68,14 +89,14 @@ __device__ __forceinline__ float mixed_adj(const float* g, int64_t ib, int64_t n
         if (jb >= nb) return -inner_adj(g + (nb - 1) * sb, ia, na, sa, w);
         return inner_adj(g + jb * sb, ia, na, sa, w);
     };
-    return (row(ib - 1) - row(ib + 1)) / 2.f;
+    return __fsub_rn(row(ib - 1), row(ib + 1)) / 2.f;
 }
 
 // d2 of a weighted component h * w along one axis with edge replication.
 __device__ __forceinline__ float d2w(const float* g, int64_t i, int64_t n, int64_t s, float w) {
-    const float fm = __ldg(g + clampi(i - 1, n) * s) * w;
-    const float f0 = __ldg(g + i * s) * w;
-    const float fp = __ldg(g + clampi(i + 1, n) * s) * w;
+    const float fm = wmul(__ldg(g + clampi(i - 1, n) * s), w);
+    const float f0 = wmul(__ldg(g + i * s), w);
+    const float fp = wmul(__ldg(g + clampi(i + 1, n) * s), w);
     return d2v(fm, f0, fp);
 }
 
@@ -88,12 +109,12 @@ template <class G>
 __device__ __forceinline__ float hess_adj_gen(const G& g, int64_t z, int64_t y, int64_t x,
                                               const Dims& d, const float w[6]) {
     // d2 of the weighted component c along one axis, edge-replicated
-    const float azz = d2v(g(0, clampi(z - 1, d.nz), y, x) * w[0], g(0, z, y, x) * w[0],
-                          g(0, clampi(z + 1, d.nz), y, x) * w[0]);
-    const float ayy = d2v(g(1, z, clampi(y - 1, d.ny), x) * w[1], g(1, z, y, x) * w[1],
-                          g(1, z, clampi(y + 1, d.ny), x) * w[1]);
-    const float axx = d2v(g(2, z, y, clampi(x - 1, d.nx)) * w[2], g(2, z, y, x) * w[2],
-                          g(2, z, y, clampi(x + 1, d.nx)) * w[2]);
+    const float azz = d2v(wmul(g(0, clampi(z - 1, d.nz), y, x), w[0]), wmul(g(0, z, y, x), w[0]),
+                          wmul(g(0, clampi(z + 1, d.nz), y, x), w[0]));
+    const float ayy = d2v(wmul(g(1, z, clampi(y - 1, d.ny), x), w[1]), wmul(g(1, z, y, x), w[1]),
+                          wmul(g(1, z, clampi(y + 1, d.ny), x), w[1]));
+    const float axx = d2v(wmul(g(2, z, y, clampi(x - 1, d.nx)), w[2]), wmul(g(2, z, y, x), w[2]),
+                          wmul(g(2, z, y, clampi(x + 1, d.nx)), w[2]));
     // d1_cen_adj(d1_cen_adj(., inner axis), outer axis); G(-1) = -g[0], G(n) = -g[n-1]
     auto ext = [&](int c, int64_t zz, int64_t yy, int64_t xx, int axis, float wc) -> float {
         int64_t n = axis == 0 ? d.nz : (axis == 1 ? d.ny : d.nx);
@@ -103,7 +124,7 @@ __device__ __forceinline__ float hess_adj_gen(const G& g, int64_t z, int64_t y, 
         if (axis == 0) zz = cl;
         else if (axis == 1) yy = cl;
         else xx = cl;
-        const float val = g(c, zz, yy, xx) * wc;
+        const float val = wmul(g(c, zz, yy, xx), wc);
         return neg ? -val : val;
     };
     // inner adjoint along axis a at outer index ob (axis b), evaluated at point p
@@ -117,7 +138,7 @@ __device__ __forceinline__ float hess_adj_gen(const G& g, int64_t z, int64_t y, 
         if (a == 0) { zm -= 1; zp += 1; }
         else if (a == 1) { ym -= 1; yp += 1; }
         else { xm -= 1; xp += 1; }
-        return (ext(c, zm, ym, xm, a, wc) - ext(c, zp, yp, xp, a, wc)) / 2.f;
+        return __fsub_rn(ext(c, zm, ym, xm, a, wc), ext(c, zp, yp, xp, a, wc)) / 2.f;
     };
     auto mixed = [&](int c, int b, int a, float wc) -> float {
         const int64_t nb = b == 0 ? d.nz : (b == 1 ? d.ny : d.nx);
@@ -127,12 +148,12 @@ __device__ __forceinline__ float hess_adj_gen(const G& g, int64_t z, int64_t y, 
             if (jb >= nb) return -inner(c, b, nb - 1, a, z, y, x, wc);
             return inner(c, b, jb, a, z, y, x, wc);
         };
-        return (row(ib - 1) - row(ib + 1)) / 2.f;
+        return __fsub_rn(row(ib - 1), row(ib + 1)) / 2.f;
     };
     const float ayz = mixed(3, 0, 1, w[3]);
     const float axz = mixed(4, 0, 2, w[4]);
     const float axy = mixed(5, 1, 2, w[5]);
-    return ((((azz + ayy) + axx) + ayz) + axz) + axy;
+    return __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(azz, ayy), axx), ayz), axz), axy);
 }
 
 // Accessor of the six components stored as hw[c * n + i].

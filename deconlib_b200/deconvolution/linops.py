@@ -173,7 +173,8 @@ class LinearFFTConvolver:
     crop in the last (pruned transforms)."""
 
     def __init__(self, kernel, signal_shape: Tuple[int, ...], normalize: bool = True,
-                 fft_shape: Optional[Tuple[int, ...]] = None, precision: str = "fp32"):
+                 fft_shape: Optional[Tuple[int, ...]] = None, precision: str = "fp32",
+                 schedule: int = 0):
         if isinstance(kernel, torch.Tensor):
             kshape = tuple(int(s) for s in kernel.shape)
         else:
@@ -205,6 +206,25 @@ class LinearFFTConvolver:
         self.precision = "fp32"
         if precision != "fp32":
             self.set_precision(precision)
+        self.schedule = 0
+        if schedule:
+            self.set_schedule(schedule)
+
+    def set_schedule(self, schedule: int) -> "LinearFFTConvolver":
+        """Choose among equivalent FFT pass families for this plan (not in the
+        reference; ``decon_conv_set_schedule`` bits, see ``SCHEDULES``):
+        results agree with the default to FP32 rounding.  Used by the
+        batched-workload autotuner."""
+        _lib.call("decon_conv_set_schedule", self._plan.handle, int(schedule))
+        self.schedule = int(schedule)
+        return self
+
+    @property
+    def fused_yz(self) -> bool:
+        """True when this plan runs the fused Y / axial cluster pass."""
+        f = C.c_int()
+        _lib.check(_lib.load().decon_conv_fused_yz(self._plan.handle, C.byref(f)))
+        return bool(f.value)
 
     def set_precision(self, precision: str) -> "LinearFFTConvolver":
         """"fp32" or "mixed" (not in the reference): "mixed" stores the OTF as

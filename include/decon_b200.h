@@ -106,6 +106,22 @@ int decon_conv_set_precision(decon_conv* plan, int precision, void* stream);
 int decon_conv_destroy(decon_conv* plan);
 /* operator_norm_sq = max |OTF|^2 (linops_mlx.py:415). */
 int decon_conv_norm_sq(const decon_conv* plan, double* out);
+/* Schedules: equivalent pass families of one plan, chosen by an autotuner
+ * (no reference counterpart; results agree to FP32 rounding, 1e-6).  Bits:
+ *   NO_FUSED     separate Y and axial passes instead of the fused Y / axial pass
+ *   NO_PIPE      one-tile TMA column kernels instead of the persistent pipelined ones
+ *   NO_TMA       plain-load column kernels (no tensor maps)
+ *   LEAN_OFF     one-CTA-per-SM axial kernel instead of the two-CTA (lean) one
+ *   ODD_RADIX    radix plans with the 5 / 3 / 7 stages first (runtime-length axes)
+ *   HALF_LINES   half the lines per CTA on runtime-length axes (more, smaller CTAs) */
+#define DECON_SCHED_NO_FUSED 1
+#define DECON_SCHED_NO_PIPE 2
+#define DECON_SCHED_NO_TMA 4
+#define DECON_SCHED_LEAN_OFF 8
+#define DECON_SCHED_ODD_RADIX 16
+#define DECON_SCHED_HALF_LINES 32
+int decon_conv_set_schedule(decon_conv* plan, int sched);
+int decon_conv_get_schedule(const decon_conv* plan, int* sched);
 /* 1 when this plan's convolutions run the fused Y / axial pass (one
  * thread-block cluster per kx column; canvases with Fy in {256, 512}, Fz in
  * {128, 256}, the signal in the first half of both axes, even Ny, FP32 OTF),
@@ -411,7 +427,7 @@ typedef struct decon_pdhg_solver decon_pdhg_solver; /* x, A x, duals, tables */
  * `stream`. */
 int decon_pdhg_solver_create(decon_conv* conv, const float* data, const int64_t data_shape[3],
                              const double scale[3], float background, int loss_type,
-                             const float* x0, float r, float alpha, int norm, int num_iter,
+                             const float* x0, double r, double alpha, int norm, int num_iter,
                              double delta, double eta, double tol, int min_iter, int patience,
                              int eval_interval, void* stream, decon_pdhg_solver** out);
 /* Queues up to `iterations` more iterations of the PDHG loop

@@ -42,8 +42,8 @@ def _solve_c(D, _lib, conv, obs, scale, iters, chunks, norm=0, loss=0, r=1.0, al
     h = C.c_void_p()
     sc = (C.c_double * 3)(*scale)
     _lib.check(lib.decon_pdhg_solver_create(conv.plan, _lib.ptr(data), _lib.i64arr(obs.shape), sc,
-                                            C.c_float(bg), loss, None, C.c_float(r),
-                                            C.c_float(alpha), norm, iters, 0.99, 0.5, tol, 20, 5,
+                                            C.c_float(bg), loss, None, C.c_double(r),
+                                            C.c_double(alpha), norm, iters, 0.99, 0.5, tol, 20, 5,
                                             eval_interval, st, C.byref(h)))
     try:
         done = 0
@@ -118,7 +118,7 @@ def test_pdhg_run_plain_operator_and_convergence(env):
     _lib.check(lib.decon_pdhg_solver_create(conv2.plan, _lib.ptr(data),
                                             _lib.i64arr(g32["pd_obs"].shape),
                                             (C.c_double * 3)(2.0, 2.0, 2.0), C.c_float(5.0), 0,
-                                            None, C.c_float(1.0), C.c_float(5.0), 0, 60, 0.99, 0.5,
+                                            None, C.c_double(1.0), C.c_double(5.0), 0, 60, 0.99, 0.5,
                                             5e-2, 3, 2, 10, st, C.byref(h)))
     try:
         _lib.check(lib.decon_pdhg_run(h, 60, st))
@@ -144,11 +144,11 @@ def test_pdhg_solver_rejects_bad_arguments(env):
     h = C.c_void_p()
     st = lib.decon_pdhg_solver_create(conv.plan, _lib.ptr(data), _lib.i64arr((8, 16, 40)),
                                       (C.c_double * 3)(2.0, 2.0, 2.0), C.c_float(0.0), 0, None,
-                                      C.c_float(1.0), C.c_float(1e-3), 0, 10, 0.99, 0.5, 1e-5, 20,
+                                      C.c_double(1.0), C.c_double(1e-3), 0, 10, 0.99, 0.5, 1e-5, 20,
                                       5, 10, _lib.stream_ptr(), C.byref(h))
     assert st == _lib.ERR_VALUE and not h.value
     st = lib.decon_pdhg_solver_create(conv.plan, _lib.ptr(data), _lib.i64arr((8, 16, 16)),
                                       (C.c_double * 3)(2.0, 2.0, 2.0), C.c_float(0.0), 3, None,
-                                      C.c_float(1.0), C.c_float(1e-3), 0, 10, 0.99, 0.5, 1e-5, 20,
+                                      C.c_double(1.0), C.c_double(1e-3), 0, 10, 0.99, 0.5, 1e-5, 20,
                                       5, 10, _lib.stream_ptr(), C.byref(h))
     assert st == _lib.ERR_VALUE

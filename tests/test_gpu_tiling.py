@@ -136,3 +136,49 @@ def test_batched_tiles_with_autotuned_canvases(D):
         assert rel(o[t.write], ref[t.crop]) <= 1e-4
     for (obs, psf_e, _), x in zip(extra, vols):
         assert rel(x, _alone(D, obs, psf_e, 20)) <= 1e-4
+
+
+@pytest.mark.parametrize("shape,fft", [((20, 60, 45), (32, 120, 90)), ((64, 128, 128), None),
+                                       ((30, 100, 90), (64, 256, 256))])
+def test_every_schedule_gives_the_same_convolution(shape, fft):
+    # the autotuner's schedules choose among equivalent pass families (fused
+    # or separate Y / axial passes, pipelined / one-tile / plain-load column
+    # kernels, one- or two-CTA axial kernel, radix order, lines per CTA):
+    # every one must give the default's result to FP32 rounding
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import deconlib_b200.deconvolution as D
+    from deconlib_b200.batch import SCHEDULES
+
+    rng = np.random.default_rng(sum(shape))
+    kshape = shape if fft is None else tuple(f - n + 1 for n, f in zip(shape, fft))
+    k = (rng.random(kshape, dtype=np.float32) ** 4).astype(np.float32)
+    x = rng.random(shape, dtype=np.float32)
+    c = D.LinearFFTConvolver(k, shape, fft_shape=fft)
+    f0, a0 = c.forward(x).cpu().numpy(), c.adjoint(x).cpu().numpy()
+    for name, sc in SCHEDULES.items():
+        c.set_schedule(sc)
+        f, a = c.forward(x).cpu().numpy(), c.adjoint(x).cpu().numpy()
+        assert np.linalg.norm(f - f0) / np.linalg.norm(f0) < 1e-6, name
+        assert np.linalg.norm(a - a0) / np.linalg.norm(a0) < 1e-6, name
+
+
+def test_autotuner_persists_its_choice(tmp_path, monkeypatch):
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import json
+
+    from deconlib_b200 import batch
+
+    monkeypatch.setenv("DECON_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    monkeypatch.setattr(batch, "_TUNED", {})
+    monkeypatch.setattr(batch, "_CACHE_LOADED", False)
+    rng = np.random.default_rng(0)
+    psf = rng.random((9, 21, 17)).astype(np.float32)
+    fs, sc = batch.autotune_schedule((24, 60, 50), psf, reps=1)
+    saved = json.load(open(tmp_path / "tune.json"))
+    assert any(v["fft_shape"] == list(fs) and v["schedule"] == sc for v in saved.values())
+    # a fresh process state reads the file instead of timing again
+    monkeypatch.setattr(batch, "_TUNED", {})
+    monkeypatch.setattr(batch, "_CACHE_LOADED", False)
+    assert batch.autotune_schedule((24, 60, 50), psf, reps=1) == (fs, sc)
