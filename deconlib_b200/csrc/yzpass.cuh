@@ -40,9 +40,11 @@ namespace dk {
 
 namespace cgx = cooperative_groups;
 
+// Default cluster: 8 CTAs of 512 threads (one CTA per SM); the alternative
+// 16 CTAs of 256 threads halves each CTA's shared memory, so two CTAs (of two
+// different clusters) share an SM and one's barriers overlap the other's work.
 constexpr int kYZCluster = 8;
 constexpr int kYZThreads = 512;
-constexpr int kYZWarps = kYZThreads / 32;
 
 struct YZArgs {
     float2* s1t;          // [Hx][Nz][Ny], transformed in place
@@ -114,15 +116,17 @@ struct WarpFFT {
     }
 };
 
-// Shared-memory bytes of k_yz for a (FY, FZ) instantiation.
-__host__ __device__ constexpr size_t yz_smem_bytes(int FY, int FZ) {
-    return (size_t)(FY + FZ) * 8 + (size_t)(FZ / (2 * kYZCluster)) * FY * 8 +
-           (size_t)(FY / kYZCluster) * FZ * 8;
+// Shared-memory bytes of k_yz for a (FY, FZ, cluster size) instantiation.
+__host__ __device__ constexpr size_t yz_smem_bytes(int FY, int FZ, int C) {
+    return (size_t)(FY + FZ) * 8 + (size_t)(FZ / (2 * C)) * FY * 8 + (size_t)(FY / C) * FZ * 8;
 }
 
-template <int FY, int FZ, int MODE>
-__global__ void __cluster_dims__(kYZCluster, 1, 1) __launch_bounds__(kYZThreads, 1)
-    k_yz(const __grid_constant__ YZArgs a) {
+// C: CTAs per cluster (launched with that cluster dimension); NT: threads.
+template <int FY, int FZ, int MODE, int C, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT) k_yz(const __grid_constant__ YZArgs a) {
+    constexpr int kYZCluster = C;
+    constexpr int kYZThreads = NT;
+    constexpr int kYZWarps = NT / 32;
     constexpr int LY = FY / 2, LZ = FZ / 2;
     using FY_ = WarpFFT<LY>;
     using FZ_ = WarpFFT<LZ>;
