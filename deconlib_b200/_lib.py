@@ -125,6 +125,7 @@ _SIGS = {
     "decon_pdhg_step": (C.c_int, [_p, _p]),
     "decon_pdhg_loss": (C.c_int, [_p, _p, _p, C.c_float, C.c_int, _i64, _p, C.c_int, C.c_int,
                                   _i64, C.c_double, C.c_int, _p]),
+    "decon_pdhg_status_async": (C.c_int, [_p, _p, _p]),
     "decon_pdhg_read": (C.c_int, [_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                   C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _dp, _dp, _dp,
                                   _dp, _p]),

@@ -8,6 +8,7 @@
 // synchronising; the FP64 reductions (||dx||^2, ||x||^2, ||dKx||^2, losses)
 // are folded in fixed order by the one-CTA step kernel.
 #include <cfloat>
+#include <cstddef>
 #include <map>
 #include <mutex>
 
@@ -835,6 +836,15 @@ int decon_pdhg_read(decon_pdhg* h, int* k, int* final_iter, int* converged, int*
     if (sigma_hist) DK_CUDA(cudaMemcpy(sigma_hist, d.sigma_hist, nh * sizeof(double), cudaMemcpyDeviceToHost));
     if (loss_hist) DK_CUDA(cudaMemcpy(loss_hist, d.loss_hist, nh * sizeof(double), cudaMemcpyDeviceToHost));
     if (rel_hist) DK_CUDA(cudaMemcpy(rel_hist, d.rel_hist, nh * sizeof(double), cudaMemcpyDeviceToHost));
+    return DECON_OK;
+}
+
+int decon_pdhg_status_async(decon_pdhg* h, int32_t* host_status, void* stream) {
+    if (!h || !host_status) return fail(DECON_ERR_NULL, "null pointer");
+    static_assert(offsetof(PdhgDev, stop) == offsetof(PdhgDev, k) + 4 * sizeof(int), "layout");
+    // k, count, converged, final_iter, stop: five consecutive ints of the state
+    DK_CUDA(cudaMemcpyAsync(host_status, &h->dev->k, 5 * sizeof(int), cudaMemcpyDeviceToHost,
+                            as_stream(stream)));
     return DECON_OK;
 }
 

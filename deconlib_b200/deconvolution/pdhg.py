@@ -321,8 +321,15 @@ class PDHGRunner:
 
     def __init__(self, data, A, reg, x0, alpha, loss_type, num_iter, background, delta, eta,
                  eval_interval, tol, min_iter, patience, verbose=False, callback=None,
-                 generic=False, fused=True, state=None):
+                 generic=False, fused=True, state=None, async_status=False):
         self.s = stream()
+        # async_status: poll the device's stop flag through a page-locked copy
+        # and an event instead of synchronising every _CHUNK iterations (a
+        # host that feeds many solves from one thread must not block on one);
+        # iterations queued after the stop are no-ops on the device
+        self.async_status = bool(async_status) and callback is None and not verbose
+        self._status = None
+        self._status_ev = None
         self.data, self.A, self.reg = data, A, reg
         self.alpha = float(alpha)
         self.bg = float(background)
@@ -419,6 +426,8 @@ class PDHGRunner:
         self.AX[(k + 1) % 2] = axn
         self.k = k + 1
         cb, verbose = self.callback, self.verbose
+        if self.async_status:
+            return self._poll_status()
         if cb is not None or (verbose and do_loss) or self.k % _CHUNK == 0:
             info = self.state.read(hist=bool(verbose and do_loss) or (self.generic and cb is not None))
             # Stop here if the solve ended before this iteration, or broke on
@@ -443,6 +452,24 @@ class PDHGRunner:
                     _lib.call("decon_pdhg_set_stop", h, k + 1, s)
                     self.stopped_at = k + 1
                     return False
+        return True
+
+    def _poll_status(self) -> bool:
+        """Non-blocking stop check: examine the last completed status copy,
+        queue a new one every _CHUNK iterations."""
+        ev = self._status_ev
+        if ev is not None and ev.query():
+            k, _, converged, final_iter, stop = (int(v) for v in self._status.tolist())
+            self._status_ev = None
+            if stop and final_iter <= k:
+                self.stopped_at = final_iter
+                return False
+        if self._status_ev is None and self.k % _CHUNK == 0:
+            if self._status is None:
+                self._status = torch.zeros(5, dtype=torch.int32, pin_memory=True)
+            _lib.call("decon_pdhg_status_async", self.h, C.c_void_p(self._status.data_ptr()), self.s)
+            self._status_ev = torch.cuda.Event()
+            self._status_ev.record(torch.cuda.current_stream())
         return True
 
     def run(self):
@@ -522,7 +549,7 @@ def pdhg_mlx_runner(observed, psf, alpha: float = 0.01,
                     delta: float = 0.99, eta: float = 0.5, eval_interval: int = 10,
                     tol: float = 1e-5, min_iter: int = 20, patience: int = 5,
                     conv: Optional[LinearFFTConvolver] = None, state=None,
-                    precision: str = "fp32"):
+                    precision: str = "fp32", async_status: bool = False):
     """Set-up of ``solve_pdhg_mlx`` without the iterations: returns the
     ``PDHGRunner`` (iterations queued on the current stream by ``iterate``)
     and the result metadata, for callers that interleave solves.
@@ -576,7 +603,7 @@ def pdhg_mlx_runner(observed, psf, alpha: float = 0.01,
         x0 = prox_nonneg(x0)
     runner = PDHGRunner(data, blur_op, reg, x0, alpha, loss_type, num_iter, background, delta, eta,
                         eval_interval, tol, min_iter, patience, verbose, callback, generic=False,
-                        state=state)
+                        state=state, async_status=async_status)
     meta = {"algorithm": "malitsky_pock_pdhg", "regularization": regularization, "norm": norm,
             "loss_type": loss_type, "alpha": alpha, "background": background, "tol": tol,
             "min_iter": min_iter, "patience": patience}

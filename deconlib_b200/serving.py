@@ -295,7 +295,7 @@ class _Slot:
                 self.state = pools.take_state(job.num_iter)
                 self.runner, self.meta = pdhg_mlx_runner(
                     job.observed, job.psf, num_iter=job.num_iter, background=job.background,
-                    conv=conv, state=self.state, **opts)
+                    conv=conv, state=self.state, async_status=True, **opts)
                 self.conv = _find_conv(self.runner.A)
                 self.state = self.runner.state
             else:

@@ -408,6 +408,13 @@ int decon_pdhg_read(decon_pdhg* h, int* k, int* final_iter, int* converged, int*
                     double* rel_hist, void* stream);
 /* Host-requested stop (a callback returned truthy). Synchronises. */
 int decon_pdhg_set_stop(decon_pdhg* h, int final_iter, void* stream);
+/* Queues a copy of {k, count, converged, final_iter, stop} (5 int32) into
+ * host_status (page-locked host memory for the copy to stay asynchronous);
+ * the values are valid once the stream has passed this point.  Lets a host
+ * that drives many solves poll convergence without synchronising (no
+ * reference counterpart: the reference reads float(rel_change) every
+ * iteration, pdhg_mlx.py:810). */
+int decon_pdhg_status_async(decon_pdhg* h, int32_t* host_status, void* stream);
 
 /* ---- resident Hessian-PDHG solve (pdhg_mlx.py:507-900) ------------------ */
 

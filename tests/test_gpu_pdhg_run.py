@@ -152,3 +152,22 @@ def test_pdhg_solver_rejects_bad_arguments(env):
                                       C.c_double(1.0), C.c_double(1e-3), 0, 10, 0.99, 0.5, 1e-5, 20,
                                       5, 10, _lib.stream_ptr(), C.byref(h))
     assert st == _lib.ERR_VALUE
+
+
+def test_async_status_polling_gives_the_same_solve(env):
+    # the serving loop's PDHG runners poll the stop flag through a pinned copy
+    # instead of synchronising; iterations queued after the device stopped are
+    # no-ops, so the result equals the synchronous driver's (early stop case)
+    D, _lib, g32, g64 = env
+    from deconlib_b200.deconvolution.pdhg import pdhg_mlx_runner, pdhg_result
+
+    kw = dict(alpha=5.0, sampling_factors=2.0, background=5.0, num_iter=60, tol=5e-2, min_iter=3,
+              patience=2)
+    ref = D.solve_pdhg_mlx(g32["pd_obs"], g32["psf_hr"], **kw)
+    runner, meta = pdhg_mlx_runner(g32["pd_obs"], g32["psf_hr"], async_status=True, **kw)
+    assert runner.async_status
+    res = pdhg_result(runner.run(), meta)
+    assert res.iterations == ref.iterations == int(g64["pd_conv_iters"])
+    assert res.converged == ref.converged
+    np.testing.assert_array_equal(res.restored.cpu().numpy(), ref.restored.cpu().numpy())
+    np.testing.assert_array_equal(res.tau_history, ref.tau_history)
