@@ -459,12 +459,81 @@ def run_mixed(D, iters=200):
             e1.record()
             torch.cuda.synchronize()
             ms += e0.elapsed_time(e1)
-            snaps[c] = runner.X[runner.k % 2].clone()
+            snaps[c] = runner.X[runner.k % 3].clone()
         pres[prec] = snaps
         out["pdhg"][prec] = {"voxel_iter_per_s": n * max(pchecks) / (ms / 1e3),
                              "ms_per_iter": ms / max(pchecks)}
         del runner
     out["pdhg"]["mixed"]["vs_fp32"] = {str(c): _errs(pres["mixed"][c], pres["fp32"][c]) for c in pchecks}
+    torch.cuda.empty_cache()
+    out["vs_fp64_oracle"] = _mixed_vs_oracle(D, checks=(10, 50, 200))
+    return out
+
+
+def _mixed_vs_oracle(D, checks=(10, 50, 200)):
+    """FP32 and mixed precision against the FP64 NumPy oracle (the reference's
+    RL and PDHG restated in float64, scipy.fft on every host core) at the
+    given iterations: RL on the 64x128x128 bead / shell workload (canvas
+    128x256x256) and Hessian-PDHG on a 64x128x128 object of the filament
+    workload type (data 32x64x64, sampling 2), so the oracle finishes in
+    about two minutes.  Relative L2 and max-abs error of x."""
+    import torch
+
+    from deconlib_b200 import synth
+    from deconlib_b200.deconvolution.pdhg import pdhg_mlx_runner
+    from deconlib_b200.deconvolution.rl import RLRunner
+    from oracle import ops, solvers
+
+    ops.set_fft_workers(len(os.sched_getaffinity(0)))
+    out = {"oracle": "oracle/ NumPy restatement of rl_mlx.py / pdhg_mlx.py in float64",
+           "checkpoints": list(checks)}
+    # RL
+    shape = (64, 128, 128)
+    psf, truth = synth.rl_workload(shape, SPACING_RL, seed=0)
+    o64 = ops.LinearFFTConvolver(psf, shape, dtype=np.float64)
+    obs = synth.poisson_observation(o64.forward(truth.astype(np.float64)), 1000.0, 10.0,
+                                    np.random.default_rng(1))
+    ref = {}
+    solvers.richardson_lucy_with_operator(
+        obs, o64, num_iter=max(checks), background=10.0, dtype=np.float64, eval_interval=10**9,
+        callback=lambda k, x: ref.__setitem__(k + 1, x.copy()) if k + 1 in checks else None)
+    rl = {}
+    for prec in ("fp32", "mixed"):
+        r = RLRunner(obs, D.LinearFFTConvolver(psf, shape, precision=prec), max(checks), 10.0,
+                     eval_interval=10**9)
+        res = {}
+        while r.k < max(checks):
+            r.iterate()
+            if r.k in checks:
+                res[str(r.k)] = _errs(r.x, torch.from_numpy(ref[r.k]).cuda())
+        rl[prec] = res
+        del r
+    out["rl_64x128x128"] = rl
+    # Hessian-PDHG
+    obj, data_shape = (64, 128, 128), (32, 64, 64)
+    ppsf, ptruth = synth.pdhg_workload(obj, SPACING_PD, seed=2)
+    fwd = ops.compose(ops.FractionalAreaDownsample(2.0, in_shape=obj, dtype=np.float64),
+                      ops.LinearFFTConvolver(ppsf, obj, dtype=np.float64))
+    pobs = synth.poisson_observation(fwd.forward(ptruth.astype(np.float64)), 500.0, 5.0,
+                                     np.random.default_rng(3))
+    kw = dict(alpha=1e-3, regularization="hessian", sampling_factors=2.0, spacing=SPACING_PD,
+              background=5.0, num_iter=max(checks), tol=0.0)
+    pref = {}
+    solvers.solve_pdhg_mlx(pobs, ppsf, dtype=np.float64, eval_interval=10**9,
+                           callback=lambda k, x: pref.__setitem__(k + 1, x.copy()) if k + 1 in checks else None,
+                           **kw)
+    pd = {}
+    for prec in ("fp32", "mixed"):
+        runner, _ = pdhg_mlx_runner(pobs, ppsf, precision=prec, eval_interval=10**9, **kw)
+        res = {}
+        while runner.k < max(checks):
+            runner.iterate()
+            if runner.k in checks:
+                res[str(runner.k)] = _errs(runner.X[runner.k % 3], torch.from_numpy(pref[runner.k]).cuda())
+        pd[prec] = res
+        del runner
+    out["pdhg_object64x128x128"] = pd
+    ops.set_fft_workers(1)
     torch.cuda.empty_cache()
     return out
 

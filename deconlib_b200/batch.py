@@ -153,14 +153,14 @@ def fft_shape_candidates(signal_shape, kernel_shape, max_growth: float = 1.35) -
 # Schedules the autotuner tries per canvas (decon_conv_set_schedule bits):
 # each names an equivalent family of FFT passes, so the winner changes the
 # speed, not the result (beyond FP32 rounding).
-SCHED_NO_FUSED, SCHED_NO_PIPE, SCHED_NO_TMA, SCHED_LEAN_OFF, SCHED_ODD_RADIX, SCHED_HALF_LINES = (
+SCHED_FUSED, SCHED_NO_PIPE, SCHED_NO_TMA, SCHED_LEAN_OFF, SCHED_ODD_RADIX, SCHED_HALF_LINES = (
     1, 2, 4, 8, 16, 32)
 SCHEDULES = {
     "default": 0,
-    "unfused": SCHED_NO_FUSED,
-    "unfused-one-tile": SCHED_NO_FUSED | SCHED_NO_PIPE,
-    "unfused-plain-loads": SCHED_NO_FUSED | SCHED_NO_TMA,
-    "unfused-one-cta-axial": SCHED_NO_FUSED | SCHED_LEAN_OFF,
+    "fused-y-axial": SCHED_FUSED,
+    "one-tile": SCHED_NO_PIPE,
+    "plain-loads": SCHED_NO_TMA,
+    "one-cta-axial": SCHED_LEAN_OFF,
     "odd-radix-first": SCHED_ODD_RADIX,
     "half-lines": SCHED_HALF_LINES,
 }
@@ -247,13 +247,13 @@ def autotune_schedule(signal_shape, psf, candidates: Optional[List[tuple]] = Non
     best, best_ms = (tuple(cands[0]), 0), float("inf")
     for fs in cands:
         conv = LinearFFTConvolver(psf, sig, fft_shape=fs)
-        fused = conv.fused_yz
         seen = set()
         for sc in scheds:
-            # the fused pass ignores the column-kernel bits; skip duplicates
-            eff = sc if not (fused and not sc & SCHED_NO_FUSED) else sc & (SCHED_ODD_RADIX | SCHED_HALF_LINES)
-            if not fused:
-                eff &= ~SCHED_NO_FUSED
+            conv.set_schedule(sc)
+            # the fused pass ignores the column-kernel bits; a canvas it does
+            # not serve ignores the fused bit: time each distinct family once
+            fused = conv.fused_yz
+            eff = sc & (SCHED_FUSED | SCHED_ODD_RADIX | SCHED_HALF_LINES) if fused else sc & ~SCHED_FUSED
             if eff in seen:
                 continue
             seen.add(eff)

@@ -341,8 +341,10 @@ static int conv_create_impl(const float* kernel, const int64_t kshape[3],
         delete p;
         return st;
     }
-    // fused Y / axial pass: the kx-major OTF copy (linear convolutions only)
-    if (!circular && yz_supported(p->N, p->F) && getenv("DECON_NO_YZ") == nullptr &&
+    // fused Y / axial pass (opt-in, DECON_YZ=1): the kx-major OTF copy now;
+    // otherwise decon_conv_set_schedule allocates it on request
+    if (!circular && yz_supported(p->N, p->F) && getenv("DECON_YZ") != nullptr &&
+        getenv("DECON_NO_YZ") == nullptr &&
         (st = dev_alloc((void**)&p->otft, (size_t)p->Hx * Fy * Fz * sizeof(float2), "kx-major OTF"))) {
         free_plan(p);
         delete p;
@@ -446,6 +448,17 @@ int decon_conv_set_schedule(decon_conv* p, int sched) {
         const bool runtime = !(L == 64 || L == 128 || L == 256 || L == 512 || L == 1024);
         *lines[i] = (runtime && (sched & DECON_SCHED_HALF_LINES) && lines0[i] >= 2) ? lines0[i] / 2
                                                                                   : lines0[i];
+    }
+    if ((sched & DECON_SCHED_FUSED) && !p->otft && yz_supported(p->N, p->F) && p->F[0] != p->N[0]) {
+        // the fused pass needs the kx-major OTF copy: allocate and fill it
+        DK_TRY(dev_alloc((void**)&p->otft, (size_t)p->Hx * p->F[1] * p->F[0] * sizeof(float2),
+                         "kx-major OTF"));
+        cudaStream_t s = nullptr;
+        DK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        const int e = build_otf_kmajor(*p, s);
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+        DK_TRY(e);
     }
     p->sched = sched;
     return DECON_OK;

@@ -677,8 +677,11 @@ bool yz_supported(const int64_t N[3], const int64_t F[3]) {
 }
 
 bool use_yz(const ConvPlan& p) {
-    return p.otft != nullptr && p.precision == 0 && !(p.sched & DECON_SCHED_NO_FUSED) &&
-           getenv("DECON_NO_YZ") == nullptr;
+    // opt-in: the plan's schedule asks for it, or DECON_YZ=1 for every plan
+    // (on the B200 the fused pass measured slower than the separate passes:
+    // it is instruction-bound, 15 eight-CTA clusters occupy 120 of 148 SMs)
+    const bool want = (p.sched & DECON_SCHED_FUSED) || getenv("DECON_YZ") != nullptr;
+    return want && p.otft != nullptr && p.precision == 0 && getenv("DECON_NO_YZ") == nullptr;
 }
 
 // out[(kx * Fy + ky) * Fz + kz] = otf[(kz * Fy + ky) * P + kx]: 32 x 32 tiles

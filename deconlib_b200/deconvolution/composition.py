@@ -7,6 +7,7 @@ argument meaning and error text.  Arrays are CUDA ``torch.Tensor`` float32.
 
 from __future__ import annotations
 
+import os
 from typing import Any, Callable, Protocol, Tuple, runtime_checkable
 
 import numpy as np
@@ -57,7 +58,9 @@ class Compose:
         self.in_shape = getattr(inner, "in_shape", None)
         self.out_shape = getattr(outer, "out_shape", None)
         self.operator_norm_sq = float(outer.operator_norm_sq * inner.operator_norm_sq)
-        self._down2 = _down2_plan(outer, inner)
+        # DECON_NO_DOWN2=1 applies the two operators in turn (same values;
+        # for measurement)
+        self._down2 = None if os.environ.get("DECON_NO_DOWN2") == "1" else _down2_plan(outer, inner)
 
     def forward(self, x):
         if self._down2 is not None:

@@ -20,6 +20,7 @@ forward and one adjoint), and ||L x_new - L x|| is computed as ||L (x_new - x)||
 from __future__ import annotations
 
 import ctypes as C
+import os
 from typing import Callable, List, Literal, Optional, Tuple, Union
 
 import numpy as np
@@ -40,6 +41,9 @@ __all__ = [
 ]
 
 _CHUNK = 16
+# DECON_SPLIT_STENCIL=1: the Hessian dual and primal updates as two kernels
+# instead of the fused z-walk (identical values; for measurement)
+_SPLIT_STENCIL = os.environ.get("DECON_SPLIT_STENCIL") == "1"
 
 
 # ---------------------------------------------------------------------------
@@ -389,11 +393,18 @@ class PDHGRunner:
         if self.fused:
             # Hessian3D: L x_bar, L^T y2 and L (x_new - x) evaluated on the fly
             shp, r = self.shp, C.c_float(self.r)
-            y2i, y2o = self.y2s[k % 2], self.y2s[(k + 1) % 2]
-            _lib.call("decon_pdhg_hess_dual_primal", h, _lib.ptr(y2i), _lib.ptr(y2o), _lib.ptr(xc),
-                      _lib.ptr(xp), _lib.ptr(aty), _lib.ptr(xo), shp, r, C.c_float(self.alpha),
-                      self.ncode, s)
-            self.y2 = y2o
+            if _SPLIT_STENCIL:
+                # the dual and the primal update as two kernels (same values)
+                _lib.call("decon_pdhg_hess_dual", h, _lib.ptr(self.y2), _lib.ptr(xc), _lib.ptr(xp),
+                          shp, r, C.c_float(self.alpha), self.ncode, s)
+                _lib.call("decon_pdhg_hess_primal", h, _lib.ptr(xc), _lib.ptr(aty),
+                          _lib.ptr(self.y2), _lib.ptr(xo), shp, r, s)
+            else:
+                y2i, y2o = self.y2s[k % 2], self.y2s[(k + 1) % 2]
+                _lib.call("decon_pdhg_hess_dual_primal", h, _lib.ptr(y2i), _lib.ptr(y2o),
+                          _lib.ptr(xc), _lib.ptr(xp), _lib.ptr(aty), _lib.ptr(xo), shp, r,
+                          C.c_float(self.alpha), self.ncode, s)
+                self.y2 = y2o
             xn = xo
             axn = to_device(A.forward(xn))
             _lib.call("decon_pdhg_hess_dk", h, _lib.ptr(axn), _lib.ptr(axc), m, _lib.ptr(xn),

@@ -108,13 +108,15 @@ int decon_conv_destroy(decon_conv* plan);
 int decon_conv_norm_sq(const decon_conv* plan, double* out);
 /* Schedules: equivalent pass families of one plan, chosen by an autotuner
  * (no reference counterpart; results agree to FP32 rounding, 1e-6).  Bits:
- *   NO_FUSED     separate Y and axial passes instead of the fused Y / axial pass
+ *   FUSED        the fused Y / axial cluster pass where the canvas allows it
+ *                (allocates the kx-major OTF copy on first request; DECON_YZ=1
+ *                selects it for every plan)
  *   NO_PIPE      one-tile TMA column kernels instead of the persistent pipelined ones
  *   NO_TMA       plain-load column kernels (no tensor maps)
  *   LEAN_OFF     one-CTA-per-SM axial kernel instead of the two-CTA (lean) one
  *   ODD_RADIX    radix plans with the 5 / 3 / 7 stages first (runtime-length axes)
  *   HALF_LINES   half the lines per CTA on runtime-length axes (more, smaller CTAs) */
-#define DECON_SCHED_NO_FUSED 1
+#define DECON_SCHED_FUSED 1
 #define DECON_SCHED_NO_PIPE 2
 #define DECON_SCHED_NO_TMA 4
 #define DECON_SCHED_LEAN_OFF 8
@@ -122,7 +124,7 @@ int decon_conv_norm_sq(const decon_conv* plan, double* out);
 #define DECON_SCHED_HALF_LINES 32
 int decon_conv_set_schedule(decon_conv* plan, int sched);
 int decon_conv_get_schedule(const decon_conv* plan, int* sched);
-/* 1 when this plan's convolutions run the fused Y / axial pass (one
+/* 1 when this plan's convolutions run the fused Y / axial pass (opt-in; one
  * thread-block cluster per kx column; canvases with Fy in {256, 512}, Fz in
  * {128, 256}, the signal in the first half of both axes, even Ny, FP32 OTF),
  * 0 when they run the separate Y and axial passes.  No reference

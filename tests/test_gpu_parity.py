@@ -265,13 +265,11 @@ def test_column_pass_variants_agree(D, monkeypatch, shape, fft):
     k = rng.random(kshape).astype(np.float32)
     x = rng.random(shape).astype(np.float32)
     outs = []
-    # DECON_NO_YZ=1 keeps these canvases on the unfused passes (without it the
-    # 256/512-point ones take the fused Y / axial pass, tests/test_gpu_yz.py)
-    keys = ("DECON_NO_PIPE", "DECON_NO_TMA", "DECON_PIPE_LEAN", "DECON_NO_YZ")
-    for env in ({}, {"DECON_NO_YZ": "1"}, {"DECON_NO_YZ": "1", "DECON_NO_PIPE": "1"},
-                {"DECON_NO_YZ": "1", "DECON_NO_TMA": "1"},
-                {"DECON_NO_YZ": "1", "DECON_PIPE_LEAN": "0"},
-                {"DECON_NO_YZ": "1", "DECON_PIPE_LEAN": "1"}):
+    # DECON_YZ=1 selects the fused Y / axial pass where the canvas allows it
+    # (tests/test_gpu_yz.py); the others choose among the separate passes
+    keys = ("DECON_NO_PIPE", "DECON_NO_TMA", "DECON_PIPE_LEAN", "DECON_YZ")
+    for env in ({}, {"DECON_YZ": "1"}, {"DECON_NO_PIPE": "1"}, {"DECON_NO_TMA": "1"},
+                {"DECON_PIPE_LEAN": "0"}, {"DECON_PIPE_LEAN": "1"}):
         for key in keys:
             monkeypatch.delenv(key, raising=False)
         for key, val in env.items():

@@ -1,6 +1,7 @@
 """The fused Y / axial pass (one thread-block cluster per kx column, the
-spectrum kx-major between the X passes) against the FP64 oracle and against
-the unfused passes (DECON_NO_YZ=1), on the canvases it serves: Fy in {256,
+spectrum kx-major between the X passes; an opt-in schedule,
+DECON_SCHED_FUSED) against the FP64 oracle and against the default separate
+passes, on the canvases it serves: Fy in {256,
 512}, Fz in {128, 256}, the signal in the first half of both, Ny even; odd
 and non-power-of-two Fx; planes that leave CTAs of a cluster without z rows.
 Tolerance: 1e-6 relative L2 against FP64 (2e-6 for the 64x128x128 canvas of
@@ -40,7 +41,7 @@ def D():
 
 
 @pytest.mark.parametrize("shape,fft", CASES)
-def test_fused_yz_pass_vs_fp64_and_unfused(D, monkeypatch, shape, fft):
+def test_fused_yz_pass_vs_fp64_and_unfused(D, shape, fft):
     from oracle import ops
 
     rng = np.random.default_rng(sum(shape) + sum(fft))
@@ -48,47 +49,45 @@ def test_fused_yz_pass_vs_fp64_and_unfused(D, monkeypatch, shape, fft):
     k = (rng.random(kshape, dtype=np.float32) ** 4).astype(np.float32)
     x = rng.random(shape, dtype=np.float32)
     o = ops.LinearFFTConvolver(k, shape, fft_shape=fft, dtype=np.float64)
-    monkeypatch.delenv("DECON_NO_YZ", raising=False)
-    c = D.LinearFFTConvolver(k, shape, fft_shape=fft)
+    c = D.LinearFFTConvolver(k, shape, fft_shape=fft, schedule=1)
+    assert c.fused_yz == (shape[1] % 2 == 0)  # every case but the odd-Ny one is served
     f1, a1 = c.forward(x), c.adjoint(x)
     tol = 2e-6 if fft == (128, 256, 256) else 1e-6
     ef, ea = rel(f1, o.forward(x.astype(np.float64))), rel(a1, o.adjoint(x.astype(np.float64)))
     print(f"\nfused Y/axial {shape} canvas {fft}: forward {ef:.2e}, adjoint {ea:.2e}")
     assert ef < tol and ea < tol
-    monkeypatch.setenv("DECON_NO_YZ", "1")
     c0 = D.LinearFFTConvolver(k, shape, fft_shape=fft)
+    assert not c0.fused_yz
     assert rel(f1, c0.forward(x).cpu().numpy()) < 1e-6
     assert rel(a1, c0.adjoint(x).cpu().numpy()) < 1e-6
-    # the switch also works on a plan built with the fused pass
+    # switching the schedule back on the same plan gives the separate passes
+    c.set_schedule(0)
+    assert not c.fused_yz
     assert rel(c.forward(x), c0.forward(x).cpu().numpy()) < 1e-6
-    monkeypatch.delenv("DECON_NO_YZ", raising=False)
     from deconlib_b200 import _lib
 
     _lib.call("decon_device_status", _lib.stream_ptr())
 
 
-def test_rl_through_fused_pass_matches_unfused(D, monkeypatch):
+def test_rl_through_fused_pass_matches_unfused(D):
     rng = np.random.default_rng(3)
     shape = (64, 128, 128)
     psf = (rng.random(shape, dtype=np.float32) ** 6).astype(np.float32)
     obs = rng.poisson(200 * rng.random(shape) + 10).astype(np.float32)
     out = []
-    for env in (None, "1"):
-        if env:
-            monkeypatch.setenv("DECON_NO_YZ", env)
-        else:
-            monkeypatch.delenv("DECON_NO_YZ", raising=False)
-        c = D.LinearFFTConvolver(psf, shape)
+    for sched in (1, 0):
+        c = D.LinearFFTConvolver(psf, shape, schedule=sched)
+        assert c.fused_yz == bool(sched)
         r = D.richardson_lucy_with_operator(obs, c, num_iter=10, background=10.0)
         out.append((r.restored.cpu().numpy(), r.loss_history))
-    monkeypatch.delenv("DECON_NO_YZ", raising=False)
     assert rel(out[0][0], out[1][0]) < 1e-5
     np.testing.assert_allclose(out[0][1], out[1][1], rtol=1e-6)
 
 
 @pytest.mark.parametrize("shape,fft", [((128, 256, 256), None), ((16, 32, 32), None),
                                        ((20, 64, 48), (64, 128, 96)), ((40, 32, 64), None)])
-def test_fused_area_sum_composition_equals_operators(D, shape, fft):
+@pytest.mark.parametrize("sched", [0, 1])
+def test_fused_area_sum_composition_equals_operators(D, shape, fft, sched):
     # compose(FractionalAreaDownsample(2), LinearFFTConvolver): the 2x area sum
     # fused into the last FFT pass and its adjoint into the first give the
     # float32 values of the two operators applied in turn (unit weights, the
@@ -96,7 +95,7 @@ def test_fused_area_sum_composition_equals_operators(D, shape, fft):
     rng = np.random.default_rng(sum(shape))
     k = (rng.random(shape if fft is None else tuple(f - n + 1 for n, f in zip(shape, fft)),
                     dtype=np.float32) ** 4).astype(np.float32)
-    conv = D.LinearFFTConvolver(k, shape, fft_shape=fft)
+    conv = D.LinearFFTConvolver(k, shape, fft_shape=fft, schedule=sched)
     down = D.FractionalAreaDownsample(2.0)
     A = D.compose(down, conv)
     assert A._down2 is not None
