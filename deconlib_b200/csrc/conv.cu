@@ -382,6 +382,9 @@ int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cva
     a.vec4 = pro == PRO_ARRAY && in != nullptr && !p.odd && (a.Nx % 4) == 0 && win.oz == 0 &&
              win.oy == 0 && win.ox == 0 && win.wz == p.N[0] && win.wy == p.N[1] &&
              win.wx == p.N[2] && (reinterpret_cast<uintptr_t>(in) & 15) == 0;
+    // the 2x adjoint prologue reads coarse rows of Nx / 2 floats as float4
+    const bool up2_vec = pro == PRO_UP2 && (a.Nx % 8) == 0 && (reinterpret_cast<uintptr_t>(in) & 15) == 0;
+    if (pro == PRO_UP2) a.vec4 = up2_vec;
     a.T = p.T_x;
     a.nrows = nz_rows * a.Ny;
     if (a.ax.L == 64 || a.ax.L == 128 || a.ax.L == 256 || a.ax.L == 512 || a.ax.L == 1024)
@@ -389,7 +392,7 @@ int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cva
     {
         const int L = a.ax.L;
         const int64_t nin = p.odd ? std::min<int64_t>(a.Nx, L) : std::min<int64_t>((a.Nx + 1) / 2, L);
-        a.fd_q4 = make_fastdiv(std::max<int64_t>(1, a.Nx / 4));
+        a.fd_q4 = make_fastdiv(std::max<int64_t>(1, pro == PRO_UP2 ? a.Nx / 8 : a.Nx / 4));
         a.fd_H = make_fastdiv(a.Hx);
         a.fd_nin = make_fastdiv(std::max<int64_t>(1, nin));
         a.fd_np = make_fastdiv(L / 2 + 1);

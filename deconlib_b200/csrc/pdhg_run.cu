@@ -11,8 +11,10 @@
 //
 //   y1   = prox(y1 + sigma A x_bar)        A x_bar from the two A x slots
 //   A^T y1                                  banded adjoint passes, conv adjoint
-//   y2'  = proj(y2 + sigma H x_bar), x_new = max(0, x - tau (A^T y1 + H^T y2'))
-//          + FP64 sums                      one fused Hessian stencil kernel
+//   y2'  = proj(y2 + sigma H x_bar)        Hessian dual kernel
+//   x_new = max(0, x - tau (A^T y1 + H^T y2')) + FP64 sums
+//                                           Hessian primal kernel (or both in
+//                                           one z-walk, DECON_FUSED_STENCIL=1)
 //   A x_new                                 conv forward, banded passes
 //   ||A dx||^2, ||H dx||^2                  FP64 sums
 //   Malitsky-Pock step (FP64, one CTA), loss every eval_interval iterations
@@ -22,6 +24,7 @@
 // graph); a converged or finished solve turns the remaining iterations into
 // no-ops on the device.
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "conv_impl.cuh"
@@ -53,6 +56,9 @@ struct decon_pdhg_solver {
     std::vector<Band> bands;
     // every axis halved exactly: A and A^T as the fused 2x area-sum passes
     bool down2 = false;
+    // dual + primal Hessian updates in one z-walk (DECON_FUSED_STENCIL=1 at
+    // creation) or as two kernels (default: measured faster on the B200)
+    bool fused_stencil = false;
     std::vector<void*> allocs;
 };
 
@@ -208,9 +214,11 @@ int decon_pdhg_solver_create(decon_conv* conv, const float* data, const int64_t 
         if (int e = pr_alloc(s, &p, (size_t)s->n * 4)) return bail(e);
         s->X[i] = (float*)p;
     }
+    s->fused_stencil = getenv("DECON_FUSED_STENCIL") != nullptr;
     for (int i = 0; i < 2; ++i) {
         if (int e = pr_alloc(s, &p, (size_t)s->m * 4)) return bail(e);
         s->AX[i] = (float*)p;
+        if (i == 1 && !s->fused_stencil) continue;  // the two-kernel form updates y2 in place
         if (int e = pr_alloc(s, &p, (size_t)6 * s->n * 4)) return bail(e);
         s->Y2[i] = (float*)p;
     }
@@ -274,8 +282,14 @@ int decon_pdhg_run(decon_pdhg_solver* s, int iterations, void* stream) {
         float* axn = s->AX[(k + 1) % 2];  // holds A x_{k-1}; overwritten with A x_new
         DK_TRY(decon_pdhg_dual_data(h, s->y1, axc, axn, s->data, s->bg, s->loss, s->m, st));
         DK_TRY(pr_adjoint(s, s->y1, s->aty, st));
-        DK_TRY(decon_pdhg_hess_dual_primal(h, s->Y2[k % 2], s->Y2[(k + 1) % 2], xc, xp, s->aty, xn,
-                                           shp, s->r, s->alpha, s->norm, st));
+        if (s->fused_stencil) {
+            DK_TRY(decon_pdhg_hess_dual_primal(h, s->Y2[k % 2], s->Y2[(k + 1) % 2], xc, xp, s->aty,
+                                               xn, shp, s->r, s->alpha, s->norm, st));
+        } else {
+            // y2 updated in place in slot 0
+            DK_TRY(decon_pdhg_hess_dual(h, s->Y2[0], xc, xp, shp, s->r, s->alpha, s->norm, st));
+            DK_TRY(decon_pdhg_hess_primal(h, xc, s->aty, s->Y2[0], xn, shp, s->r, st));
+        }
         DK_TRY(pr_forward(s, xn, axn, st));
         DK_TRY(decon_pdhg_hess_dk(h, axn, axc, s->m, xn, xc, shp, s->r, st));
         DK_TRY(decon_pdhg_step(h, st));

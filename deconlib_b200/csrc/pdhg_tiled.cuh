@@ -582,7 +582,37 @@ __global__ void __launch_bounds__(256) k_hess_dual_primal(
         e.xhi = x == d.nx - 1 ? -1.f : 1.f;
         const int64_t qa = max(z0 - 1, (int64_t)0), qb = min(z1, d.nz - 1);  // y2_out planes
         const int64_t pa = max(qa - 1, (int64_t)0), pb = min(qb + 1, d.nz - 1);  // x_bar planes
-        auto dual_plane = [&](int64_t q) {
+        // Global operands are loaded one step ahead into the registers the
+        // current step has just consumed: x and x_prev of the next x_bar plane
+        // (issued right after staging), y2_in of the next dual plane (after
+        // the dual update), x and A^T y1 of the next primal plane (after the
+        // primal update), so every load is in flight across a barrier and a
+        // plane of arithmetic.
+        auto load_x = [&](int64_t p, float ra[2], float rp[2]) {
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                if (!k2[u]) continue;
+                const int64_t i = p * plane + o2[u];
+                ra[u] = __ldg(xc + i);
+                rp[u] = __ldg(xp + i);
+            }
+        };
+        auto load_y = [&](int64_t q, float ry[2][6]) {
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                if (!k1[u]) continue;
+                const int64_t i = q * plane + o1[u];
+#pragma unroll
+                for (int c = 0; c < 6; ++c) ry[u][c] = __ldg(y2_in + c * n + i);
+            }
+        };
+        auto load_pr = [&](int64_t z, float& a, float& at) {
+            if (!in || z < z0 || z >= z1) return;
+            const int64_t i = z * plane + ipl;
+            a = __ldg(xc + i);
+            at = __ldg(aty + i);
+        };
+        auto dual_plane = [&](int64_t q, const float ry[2][6]) {
             const int64_t qm = clampi(q - 1, d.nz), qp = clampi(q + 1, d.nz);
             const float* pm = xb[qm & 3];
             const float* p0 = xb[q & 3];
@@ -597,12 +627,12 @@ __global__ void __launch_bounds__(256) k_hess_dual_primal(
                 float v[6];
                 if constexpr (NORM == 0) {
 #pragma unroll
-                    for (int c = 0; c < 6; ++c) v[c] = fminf(fmaxf(dual_arg(__ldg(y2_in + c * n + i), sg, h[c]), -alpha), alpha);
+                    for (int c = 0; c < 6; ++c) v[c] = fminf(fmaxf(dual_arg(ry[u][c], sg, h[c]), -alpha), alpha);
                 } else {
                     float ss = 0.f;
 #pragma unroll
                     for (int c = 0; c < 6; ++c) {
-                        v[c] = dual_arg(__ldg(y2_in + c * n + i), sg, h[c]);
+                        v[c] = dual_arg(ry[u][c], sg, h[c]);
                         ss += v[c] * v[c];
                     }
                     const float sc = fmaxf(sqrtf(ss + 1e-12f) / alpha, 1.f);
@@ -618,7 +648,7 @@ __global__ void __launch_bounds__(256) k_hess_dual_primal(
                 }
             }
         };
-        auto primal_plane = [&](int64_t z) {
+        auto primal_plane = [&](int64_t z, float a, float at) {
             if (!in || z < z0 || z >= z1) return;
             const int sm_ = (int)(clampi(z - 1, d.nz) & 3), sc_ = (int)(z & 3),
                       sp_ = (int)(clampi(z + 1, d.nz) & 3);
@@ -628,8 +658,7 @@ __global__ void __launch_bounds__(256) k_hess_dual_primal(
                                            yn[3][sm_], yn[3][sp_], yn[4][sm_], yn[4][sp_], yn[5][sc_],
                                            ty + 1, tx + 1, e, w.w);
             const int64_t i = z * plane + ipl;
-            const float a = xc[i];
-            const float gr = __fadd_rn(aty[i], lt);
+            const float gr = __fadd_rn(at, lt);
             const float v = primal_of(a, tau, gr);
             xn[i] = v;
             const float dd = v - a;
@@ -637,27 +666,35 @@ __global__ void __launch_bounds__(256) k_hess_dual_primal(
             xc2 += (double)a * a;
             xn2 += (double)v * v;
         };
+        float rxa[2] = {0.f, 0.f}, rxp[2] = {0.f, 0.f}, ry[2][6] = {}, pra = 0.f, prt = 0.f;
+        load_x(pa, rxa, rxp);
+        if (pa - 1 >= qa) load_y(pa - 1, ry);
+        load_pr(pa - 2, pra, prt);
         for (int64_t p = pa; p <= pb; ++p) {
-            // stage x_bar plane p (two-voxel halo)
+            // stage x_bar plane p (two-voxel halo), then fetch the next one's inputs
             float* dst = xb[p & 3];
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                if (!k2[u]) continue;
-                const int64_t i = p * plane + o2[u];
-                const float a = __ldg(xc + i);
-                dst[tid + u * 256] = xbar_of(a, __ldg(xp + i), th);
-            }
+            for (int u = 0; u < 2; ++u)
+                if (k2[u]) dst[tid + u * 256] = xbar_of(rxa[u], rxp[u], th);
+            if (p + 1 <= pb) load_x(p + 1, rxa, rxp);
             __syncthreads();
             // y2_out planes whose x_bar neighbourhood is complete
             const int64_t q = p - 1;
-            if (q >= qa && q <= qb) dual_plane(q);
-            if (p == d.nz - 1 && p >= qa && p <= qb) dual_plane(p);
+            const bool last = p == d.nz - 1 && p >= qa && p <= qb;
+            if (q >= qa && q <= qb) dual_plane(q, ry);
+            if (p >= qa && p <= qb) load_y(p, ry);  // the next dual plane, or this last one
+            if (last) dual_plane(p, ry);
             __syncthreads();
             // x_new planes whose y2_out neighbourhood is complete
-            if (q >= qa && q <= qb) primal_plane(q - 1);
-            if (p == d.nz - 1 && p >= qa && p <= qb) {
-                if (q >= qa) primal_plane(q);
-                primal_plane(p);
+            if (q >= qa && q <= qb) {
+                primal_plane(q - 1, pra, prt);
+                load_pr(q, pra, prt);  // the next primal plane
+            }
+            if (last) {
+                // the volume's last plane: planes q and p complete together
+                if (q >= qa && q <= qb) primal_plane(q, pra, prt);
+                load_pr(p, pra, prt);
+                primal_plane(p, pra, prt);
             }
         }
         __syncthreads();  // the rings are reused by the next tile

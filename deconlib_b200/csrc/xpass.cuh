@@ -101,6 +101,39 @@ __global__ void __launch_bounds__(kFftThreads, 3) k_xr2c(XR2CArgs a) {
         // 2n + 1 both take coarse value n of coarse row (z / 2, y / 2), so the
         // packed point n is (c[n], c[n]) (even Fx, even extents)
         const int64_t mx = a.Nx >> 1, my = a.Ny >> 1;
+        if (a.vec4) {
+            // four coarse values (one float4) per thread step, several in flight
+            const int q4 = (int)(mx >> 2), nq = T * q4;
+            constexpr int U = 4;
+            #pragma unroll 1
+            for (int c0 = tid; c0 < nq; c0 += U * blockDim.x) {
+                float4 v[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int c = c0 + u * blockDim.x;
+                    const int t = fdiv(c, a.fd_q4);
+                    const int64_t row = row0 + t;
+                    float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (c < nq && row < a.nrows) {
+                        const int64_t z = row / a.Ny, y = row - z * a.Ny;
+                        w = __ldg(reinterpret_cast<const float4*>(a.in + ((z >> 1) * my + (y >> 1)) * mx) +
+                                  (c - t * q4));
+                    }
+                    v[u] = w;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int c = c0 + u * blockDim.x;
+                    if (c < nq) {
+                        const int t = fdiv(c, a.fd_q4), n = 4 * (c - t * q4);
+                        sm[phys(n, t, T)] = make_float2(v[u].x, v[u].x);
+                        sm[phys(n + 1, t, T)] = make_float2(v[u].y, v[u].y);
+                        sm[phys(n + 2, t, T)] = make_float2(v[u].z, v[u].z);
+                        sm[phys(n + 3, t, T)] = make_float2(v[u].w, v[u].w);
+                    }
+                }
+            }
+        } else {
         #pragma unroll 1
         for (int q = tid; q < T * nin; q += blockDim.x) {
             const int t = fdiv(q, a.fd_nin), n = q - t * nin;
@@ -111,6 +144,7 @@ __global__ void __launch_bounds__(kFftThreads, 3) k_xr2c(XR2CArgs a) {
                 v = __ldg(a.in + ((z >> 1) * my + (y >> 1)) * mx + n);
             }
             sm[phys(n, t, T)] = make_float2(v, v);
+        }
         }
     } else if (PRO == PRO_ARRAY && a.vec4) {
         const int q4 = (int)(a.Nx >> 2);  // float4 per row

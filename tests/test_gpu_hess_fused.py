@@ -75,9 +75,10 @@ def test_fused_dual_primal_equals_separate_kernels(env, shape, norm):
     assert not torch.isnan(outs[0][1]).any()
 
 
-def test_pdhg_fused_stencil_trajectory_matches_operator_path():
+def test_pdhg_fused_stencil_trajectory_matches_operator_path(monkeypatch):
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
+    monkeypatch.setenv("DECON_FUSED_STENCIL", "1")
     import os
 
     import deconlib_b200.deconvolution as D
@@ -95,6 +96,7 @@ def test_pdhg_fused_stencil_trajectory_matches_operator_path():
         x0 = D.prox_nonneg(A.adjoint(data))
         run = PDHGRunner(data, A, reg, x0, 1e-3, "poisson", 40, 5.0, 0.99, 0.5, 10, 1e-5, 20, 5,
                          fused=fused)
+        assert run.fused == fused and (not fused or run.fused_stencil)
         out.append(run.run().result())
     x = out[0][0].cpu().numpy()
     ref = out[1][0].cpu().numpy()
