@@ -777,15 +777,18 @@ int decon_pdhg_hess_dual_primal(decon_pdhg* h, const float* y2_in, float* y2_out
 int decon_pdhg_hess_dk(decon_pdhg* h, const float* ax_new, const float* ax_cur, int64_t m,
                        const float* xn, const float* xc, const int64_t shape[3], float r,
                        void* stream) {
-    if (!h || !ax_new || !ax_cur || !xn || !xc || !shape) return fail(DECON_ERR_NULL, "null pointer");
+    if (!h || !xn || !xc || !shape || (ax_new && !ax_cur)) return fail(DECON_ERR_NULL, "null pointer");
     W6 w;
     hessian_weights(r, w.w);
     int per_sm = 1;
     const Dims d{shape[0], shape[1], shape[2]};
     DK_TRY(smem_prepare((const void*)k_hess_dk_r, 0, &per_sm));
     const int grid = (int)std::min<int64_t>(kPdhgGrid, std::max<int64_t>(TileGeo(d).ntiles, 1));
-    k_hess_dk_r<<<grid, 256, 0, as_stream(stream)>>>(h->dev, ax_new, ax_cur, m, xn, xc, d, w, kSlotDA2,
-                                                    kSlotDL2);
+    // ax_new == NULL: only ||H dx||^2 (the data term's ||A dx||^2 then comes
+    // from decon_pdhg_dk with l_dx = NULL); the empty A sum goes to the spare
+    // slot 7 so that the two kernels may run concurrently
+    k_hess_dk_r<<<grid, 256, 0, as_stream(stream)>>>(h->dev, ax_new, ax_cur, ax_new ? m : 0, xn, xc, d,
+                                                    w, ax_new ? kSlotDA2 : kPdhgSlots - 1, kSlotDL2);
     DK_LAUNCHED();
     return DECON_OK;
 }

@@ -50,6 +50,14 @@ def _fused_stencil() -> bool:
     return os.environ.get("DECON_FUSED_STENCIL") == "1"
 
 
+def _overlap() -> bool:
+    """DECON_PDHG_OVERLAP=1: the Hessian dual update and ||H dx||^2 on a
+    second stream, beside the adjoint and the forward convolution (they read
+    nothing those produce).  Same kernels and values except the FP64 sum of
+    ||A dx||^2, which is then split over a different grid."""
+    return os.environ.get("DECON_PDHG_OVERLAP") == "1"
+
+
 # ---------------------------------------------------------------------------
 # proximal maps (element-wise; exposed for API parity, pdhg_mlx.py:115-233)
 # ---------------------------------------------------------------------------
@@ -374,6 +382,7 @@ class PDHGRunner:
         # fused Hessian3D kernels (fused=False keeps the operator-by-operator path)
         self.fused = (fused and isinstance(reg, HessianRegularizer) and reg.ndim == 3
                       and x0.dim() == 3)
+        self.side = None
         if self.fused:
             self.shp = _lib.i64arr(tuple(x0.shape))
             self.r = float(reg.r)
@@ -382,6 +391,9 @@ class PDHGRunner:
             # buffer and writes iteration k + 1's into the other
             self.fused_stencil = _fused_stencil()
             self.y2s = [self.y2, zeros((self.ncomp,) + tuple(x0.shape))] if self.fused_stencil else None
+            if _overlap() and not self.fused_stencil:
+                self.side = torch.cuda.Stream()
+                self.evs = [torch.cuda.Event() for _ in range(4)]
 
     def iterate(self) -> bool:
         """Queue iteration k; returns False once the solve has stopped."""
@@ -391,6 +403,18 @@ class PDHGRunner:
         m, n = self.m, self.n
         xc, xp, xo = self.X[k % 3], self.X[(k + 2) % 3], self.X[(k + 1) % 3]
         axc, axp = self.AX[k % 2], self.AX[(k + 1) % 2]
+        side = self.side if self.fused else None
+        if side is not None:
+            # the Hessian dual update reads x_k, x_{k-1} and the step sizes
+            # only: queue it on the side stream beside the adjoint
+            cur = torch.cuda.current_stream()
+            e0, e1, e2, e3 = self.evs
+            e0.record(cur)
+            side.wait_event(e0)
+            _lib.call("decon_pdhg_hess_dual", h, _lib.ptr(self.y2), _lib.ptr(xc), _lib.ptr(xp),
+                      self.shp, C.c_float(self.r), C.c_float(self.alpha), self.ncode,
+                      C.c_void_p(side.cuda_stream))
+            e1.record(side)
         _lib.call("decon_pdhg_dual_data", h, _lib.ptr(self.y1), _lib.ptr(axc), _lib.ptr(axp),
                   _lib.ptr(self.data), C.c_float(self.bg), self.lcode, m, s)
         aty = to_device(A.adjoint(self.y1))
@@ -398,7 +422,23 @@ class PDHGRunner:
         if self.fused:
             # Hessian3D: L x_bar, L^T y2 and L (x_new - x) evaluated on the fly
             shp, r = self.shp, C.c_float(self.r)
-            if not self.fused_stencil:
+            if side is not None:
+                # primal update after the side stream's dual, then
+                # ||H (x_new - x)||^2 on the side stream beside the forward
+                # convolution, ||A x_new - A x||^2 here, the step after both
+                cur.wait_event(e1)
+                _lib.call("decon_pdhg_hess_primal", h, _lib.ptr(xc), _lib.ptr(aty),
+                          _lib.ptr(self.y2), _lib.ptr(xo), shp, r, s)
+                e2.record(cur)
+                side.wait_event(e2)
+                _lib.call("decon_pdhg_hess_dk", h, None, None, 0, _lib.ptr(xo), _lib.ptr(xc), shp, r,
+                          C.c_void_p(side.cuda_stream))
+                e3.record(side)
+                xn = xo
+                axn = to_device(A.forward(xn))
+                _lib.call("decon_pdhg_dk", h, _lib.ptr(axn), _lib.ptr(axc), m, None, 0, s)
+                cur.wait_event(e3)
+            elif not self.fused_stencil:
                 # the dual and the primal update as two kernels (same values)
                 _lib.call("decon_pdhg_hess_dual", h, _lib.ptr(self.y2), _lib.ptr(xc), _lib.ptr(xp),
                           shp, r, C.c_float(self.alpha), self.ncode, s)
@@ -410,10 +450,11 @@ class PDHGRunner:
                           _lib.ptr(xc), _lib.ptr(xp), _lib.ptr(aty), _lib.ptr(xo), shp, r,
                           C.c_float(self.alpha), self.ncode, s)
                 self.y2 = y2o
-            xn = xo
-            axn = to_device(A.forward(xn))
-            _lib.call("decon_pdhg_hess_dk", h, _lib.ptr(axn), _lib.ptr(axc), m, _lib.ptr(xn),
-                      _lib.ptr(xc), shp, r, s)
+            if side is None:
+                xn = xo
+                axn = to_device(A.forward(xn))
+                _lib.call("decon_pdhg_hess_dk", h, _lib.ptr(axn), _lib.ptr(axc), m, _lib.ptr(xn),
+                          _lib.ptr(xc), shp, r, s)
             _lib.call("decon_pdhg_step", h, s)
             if do_loss:
                 _lib.call("decon_pdhg_hess_loss", h, _lib.ptr(axn), _lib.ptr(self.data),

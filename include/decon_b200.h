@@ -380,7 +380,10 @@ int decon_pdhg_loss(decon_pdhg* h, const float* ax, const float* data, float bac
  *   hess_dual:   y2 = proj(y2 + sigma H x_bar), x_bar = x + theta (x - x_prev)
  *   hess_primal: x_new = max(0, x - tau (aty + H^T y2)) + the FP64 sums of
  *                decon_pdhg_primal
- *   hess_dk:     ||A x_new - A x||^2 and ||H (x_new - x)||^2
+ *   hess_dk:     ||A x_new - A x||^2 and ||H (x_new - x)||^2 (ax_new NULL:
+ *                only the Hessian term, so that it may run beside the
+ *                forward convolution; decon_pdhg_dk(l_dx = NULL) adds the
+ *                data term)
  *   hess_loss:   objective at iteration k with the H x_new norm fused. */
 int decon_pdhg_hess_dual(decon_pdhg* h, float* y2, const float* xc, const float* xp,
                          const int64_t shape[3], float r, float alpha, int norm, void* stream);

@@ -75,10 +75,14 @@ def test_fused_dual_primal_equals_separate_kernels(env, shape, norm):
     assert not torch.isnan(outs[0][1]).any()
 
 
-def test_pdhg_fused_stencil_trajectory_matches_operator_path(monkeypatch):
+@pytest.mark.parametrize("switch", ["DECON_FUSED_STENCIL", "DECON_PDHG_OVERLAP"])
+def test_pdhg_fused_stencil_trajectory_matches_operator_path(monkeypatch, switch):
+    """The opt-in schedules of the Hessian path (one fused dual + primal
+    kernel; dual and ||H dx||^2 on a second stream) follow the
+    operator-by-operator trajectory."""
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
-    monkeypatch.setenv("DECON_FUSED_STENCIL", "1")
+    monkeypatch.setenv(switch, "1")
     import os
 
     import deconlib_b200.deconvolution as D
@@ -96,7 +100,9 @@ def test_pdhg_fused_stencil_trajectory_matches_operator_path(monkeypatch):
         x0 = D.prox_nonneg(A.adjoint(data))
         run = PDHGRunner(data, A, reg, x0, 1e-3, "poisson", 40, 5.0, 0.99, 0.5, 10, 1e-5, 20, 5,
                          fused=fused)
-        assert run.fused == fused and (not fused or run.fused_stencil)
+        assert run.fused == fused
+        if fused:
+            assert (run.fused_stencil if switch == "DECON_FUSED_STENCIL" else run.side is not None)
         out.append(run.run().result())
     x = out[0][0].cpu().numpy()
     ref = out[1][0].cpu().numpy()
