@@ -414,6 +414,8 @@ int decon_conv_set_precision(decon_conv* p, int precision, void* stream) {
     if (!p->otf_inv && (st = dev_alloc((void**)&p->otf_inv, (size_t)p->F[0] * sizeof(float), "OTF scales")))
         return st;
     DK_TRY(quantize_otf(*p, as_stream(stream)));
+    if (!p->tma_otf16)
+        p->tma_otf16 = encode_half_plane_map(&p->tm_otf16_z, p->otf16, p->P, p->F[1], p->F[0], p->otf_box);
     p->precision = 1;
     return DECON_OK;
 }

@@ -46,10 +46,12 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
     constexpr int NS = pipe_slots(L, LEAN);
     constexpr bool OTF = (MODE == COL_OTF || MODE == COL_OTF_CONJ);
     constexpr bool INV_FIRST = (MODE == COL_INV);
-    constexpr bool OTFT = OTF && !H16;              // OTF tile staged by TMA
-    // LEAN axial pass: one OTF buffer beside a two-slot spectrum ring, loaded
-    // for the next tile as soon as the current tile's product is done
-    constexpr bool OTF1 = OTFT && LEAN;
+    constexpr bool OTFT = OTF && !H16;              // FP32 OTF tile staged by TMA
+    // LEAN axial pass: one OTF buffer (FP32, or FP16 under H16) beside a
+    // two-slot spectrum ring, loaded for the next tile as soon as the current
+    // tile's product is done
+    constexpr bool OTF1 = OTF && LEAN;
+    constexpr bool OTF1H = OTF1 && H16;             // FP16 OTF tile staged by TMA
     constexpr int SLOT = L * 16 * (OTFT && !OTF1 ? 2 : 1);  // float2 per ring slot
     constexpr int D1 = INV_FIRST ? +1 : -1;  // direction of the first transform
     extern __shared__ unsigned char smraw[];
@@ -90,8 +92,11 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
     };
 
     // FP16 OTF: this thread's kz planes are fixed, so are their scales
-    float os[H16 ? SPLIT : 1][H16 ? R : 1];
-    if constexpr (H16) {
+    float os[H16 && !LEAN ? SPLIT : 1][H16 && !LEAN ? R : 1];
+    __shared__ float oss[OTF1H ? L : 1];  // OTF1H: the scales of all L kz planes
+    if constexpr (OTF1H) {
+        for (int q = tid; q < L; q += blockDim.x) oss[q] = __ldg(a.otf_inv + q);
+    } else if constexpr (H16) {
 #pragma unroll
         for (int h = 0; h < SPLIT; ++h)
 #pragma unroll
@@ -99,6 +104,7 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
     }
 
     float2* otf1 = base + NS * SLOT;  // OTF1 buffer
+    const __half2* otf1h = reinterpret_cast<const __half2*>(otf1);  // OTF1H view: [L][16] half2
     if (tid == 0) {
         for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
         if constexpr (OTF1) mbar_init(&obar, 1);
@@ -122,8 +128,15 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
     auto issue_otf = [&](int tile) {
         const int o = tile / a.ntiles;
         const int c0 = (tile - o * a.ntiles) * 32;
-        mbar_expect_tx(&obar, (uint32_t)(L * 128));
-        for (int r0 = 0; r0 < L; r0 += a.otf_box) tma_load_3d(otf1 + r0 * 16, &a.otfmap, c0, o, r0, &obar);
+        if constexpr (OTF1H) {
+            // half2 elements: column c0 / 2, rows of 64 bytes
+            mbar_expect_tx(&obar, (uint32_t)(L * 64));
+            for (int r0 = 0; r0 < L; r0 += a.otf_box)
+                tma_load_3d(reinterpret_cast<__half2*>(otf1) + r0 * 16, &a.otfmap16, c0 >> 1, o, r0, &obar);
+        } else {
+            mbar_expect_tx(&obar, (uint32_t)(L * 128));
+            for (int r0 = 0; r0 < L; r0 += a.otf_box) tma_load_3d(otf1 + r0 * 16, &a.otfmap, c0, o, r0, &obar);
+        }
     };
     if (tid == 0) {
         for (int s = 0; s < NS; ++s) {
@@ -148,8 +161,8 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
         // FP16 OTF (H16): raw values and plane scales are only loaded here and
         // converted where they are used, so the loads stay in flight across
         // the tile wait and the forward transform like the FP32 ones.
-        __half2 oh[H16 ? SPLIT : 1][H16 ? R : 1];
-        if constexpr (OTF && H16) {
+        __half2 oh[H16 && !LEAN ? SPLIT : 1][H16 && !LEAN ? R : 1];
+        if constexpr (OTF && H16 && !LEAN) {
             const __half2* op = a.otf16 + o * a.otf_os + (c0 >> 1) + t;
 #pragma unroll
             for (int h = 0; h < SPLIT; ++h)
@@ -201,7 +214,11 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     float2 w;
-                    if constexpr (H16) {
+                    if constexpr (OTF1H) {
+                        const int kz = SPLIT * (j + R * r) + h;
+                        const float2 q = __half22float2(otf1h[kz * 16 + t]);
+                        w = make_float2(q.x * oss[kz], q.y * oss[kz]);
+                    } else if constexpr (H16) {
                         const float2 q = __half22float2(oh[h][r]);
                         w = make_float2(q.x * os[h][r], q.y * os[h][r]);
                     } else {

@@ -512,8 +512,7 @@ static void* pick_col_tma(int L) {
 
 bool tma_length_ok(int L) { return L == 64 || L == 128 || L == 256 || L == 512; }
 
-bool encode_spectrum_map(CUtensorMap* map, const float2* base, int64_t pitch, int64_t d1, int64_t d2,
-                         int b1, int b2) {
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
     static bool tried = false;
     if (!tried) {
@@ -527,6 +526,28 @@ bool encode_spectrum_map(CUtensorMap* map, const float2* base, int64_t pitch, in
         else
             cudaGetLastError();
     }
+    return enc;
+}
+
+bool encode_half_plane_map(CUtensorMap* map, const __half2* base, int64_t pitch, int64_t d1, int64_t d2,
+                           int b2) {
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    // one half2 = one 4-byte element; rows of 16 elements (64 bytes), no swizzle
+    cuuint64_t dims[3] = {(cuuint64_t)pitch, (cuuint64_t)d1, (cuuint64_t)d2};
+    cuuint64_t strides[2] = {(cuuint64_t)(pitch * sizeof(__half2)),
+                             (cuuint64_t)(pitch * sizeof(__half2) * d1)};
+    cuuint32_t box[3] = {16u, 1u, (cuuint32_t)b2};
+    cuuint32_t estr[3] = {1u, 1u, 1u};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<__half2*>(base), dims, strides,
+                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+bool encode_spectrum_map(CUtensorMap* map, const float2* base, int64_t pitch, int64_t d1, int64_t d2,
+                         int b1, int b2) {
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     if (!enc) return false;
     cuuint64_t dims[3] = {(cuuint64_t)(2 * pitch), (cuuint64_t)d1, (cuuint64_t)d2};
     cuuint64_t strides[2] = {(cuuint64_t)(2 * pitch * sizeof(float)),
@@ -557,11 +578,13 @@ static void* pick_pipe(int L, int mode, int nin, int nout, int* R, int* split, b
             case COL_FWD: return (void*)k_col_pipe<RR, SS, COL_FWD>;                             \
             case COL_INV: return (void*)k_col_pipe<RR, SS, COL_INV>;                             \
             case COL_OTF:                                                                        \
-                return h16 ? (void*)k_col_pipe<RR, SS, COL_OTF, true>                           \
+                return h16 ? (lean ? (void*)k_col_pipe<RR, SS, COL_OTF, true, true>              \
+                                   : (void*)k_col_pipe<RR, SS, COL_OTF, true>)                  \
                            : (lean ? (void*)k_col_pipe<RR, SS, COL_OTF, false, true>            \
                                    : (void*)k_col_pipe<RR, SS, COL_OTF>);                       \
             case COL_OTF_CONJ:                                                                   \
-                return h16 ? (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, true>                      \
+                return h16 ? (lean ? (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, true, true>         \
+                                   : (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, true>)             \
                            : (lean ? (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, false, true>       \
                                    : (void*)k_col_pipe<RR, SS, COL_OTF_CONJ>);                  \
         }                                                                                        \
@@ -585,9 +608,10 @@ static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const C
     const bool otf_mode = mode == COL_OTF || mode == COL_OTF_CONJ;
     const bool h16 = otf_mode && p.precision == 1 && p.otf16 != nullptr;
     // axial pass of length 256: the lean two-CTA kernel (measured 153 vs 166 us
-    // at 128x256x256 on the B200); DECON_PIPE_LEAN=0 / 1 overrides
+    // at 128x256x256 on the B200); DECON_PIPE_LEAN=0 / 1 overrides.  Its FP16
+    // form stages the half OTF tile by TMA (needs the plan's half-OTF map).
     const char* le = getenv("DECON_PIPE_LEAN");
-    const bool lean = otf_mode && !h16 &&
+    const bool lean = otf_mode && (!h16 || p.tma_otf16) &&
                       (le ? le[0] == '1' : (ax.L == 256 && !(p.sched & DECON_SCHED_LEAN_OFF)));
     const bool no_pipe = getenv("DECON_NO_PIPE") || (p.sched & DECON_SCHED_NO_PIPE);
     void* fn = no_pipe ? nullptr : pick_pipe(ax.L, mode, nin, nout, &R, &split, h16, lean);
@@ -600,6 +624,7 @@ static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const C
     a.otf16 = p.otf16;
     a.otf_inv = p.otf_inv;
     a.otfmap = p.tm_otf_z;
+    a.otfmap16 = p.tm_otf16_z;
     a.otf_box = p.otf_box;
     a.otf_js = p.F[1] * p.P;
     a.otf_os = p.P;
@@ -615,10 +640,11 @@ static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const C
     a.dst_box = dst_box;
     const int L = ax.L;
     const int ns = pipe_slots(L, lean);
-    const bool otf_tile = otf_mode && !h16;  // FP32 OTF tile: in each ring slot, or (lean) one buffer
+    // OTF tile: FP32 in each ring slot, or (lean) one buffer of FP32 or FP16
+    const bool otf_tile = otf_mode && !h16;
     const size_t tile_bytes = (size_t)L * 16 * sizeof(float2);
     const size_t smem = 1024 + (size_t)ns * tile_bytes * (otf_tile && !lean ? 2 : 1) +
-                        (otf_tile && lean ? tile_bytes : 0);
+                        (otf_mode && lean ? (h16 ? tile_bytes / 2 : tile_bytes) : 0);
     const int nthr = 16 * R;
     *status = DECON_OK;
     int per_sm = 1;

@@ -74,6 +74,7 @@ struct ColTmaArgs {
 struct PipeArgs {
     CUtensorMap src, dst;
     CUtensorMap otfmap;     // FP32 OTF [Fz][Fy][P] as TMA boxes (axial pass)
+    CUtensorMap otfmap16;   // FP16 OTF [Fz][Fy][P] half2, (16, 1, otf_box) boxes (lean mixed axial pass)
     int otf_box;
     const float2* otf;      // OTF base for the axial pass
     const __half2* otf16;   // mixed precision: FP16 OTF, OTF = otf16 * otf_inv[kz]
@@ -127,6 +128,8 @@ struct ConvPlan {
     int precision = 0;
     __half2* otf16 = nullptr;
     float* otf_inv = nullptr;
+    CUtensorMap tm_otf16_z;   // valid when tma_otf16
+    bool tma_otf16 = false;
     // Fused Y / axial pass (yzpass.cuh): the OTF also stored kx-major
     // [Hx][Fy][Fz]; the spectrum between the X passes is then kx-major too
     // ([Hx][Nz][Ny] in s1).  nullptr: the canvas takes the unfused passes.
@@ -156,6 +159,10 @@ bool zpass_pipelined(const ConvPlan& p);
 int kernel_prepare(void* fn, size_t smem, int nthr, int* per_sm);
 
 bool tma_length_ok(int L);
+// Rank-3 map over an FP16 complex [d2][d1][pitch] buffer (one half2 = one
+// 4-byte element) with (16, 1, b2) boxes and no swizzle.
+bool encode_half_plane_map(CUtensorMap* map, const __half2* base, int64_t pitch, int64_t d1, int64_t d2,
+                           int b2);
 bool encode_spectrum_map(CUtensorMap* map, const float2* base, int64_t pitch, int64_t d1, int64_t d2,
                          int b1, int b2);
 

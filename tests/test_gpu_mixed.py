@@ -82,3 +82,25 @@ def test_mixed_rl_against_fp64_oracle(D):
     print(f"RL {shape} x{n}: FP32 rel-L2 vs FP64 oracle {e32:.2e}, mixed {e16:.2e}")
     assert e32 < 1e-4
     assert e16 < 1e-2
+
+
+def test_mixed_lean_axial_pass_bit_identical_to_register_form(D, monkeypatch):
+    """Axial length 256: the lean two-CTA kernel stages each FP16 OTF tile by
+    TMA into shared memory, the one-CTA form (DECON_PIPE_LEAN=0) loads it into
+    registers; the products and transforms are the same, so are the bits."""
+    from deconlib_b200 import synth
+
+    shape = (64, 128, 128)
+    rng = np.random.default_rng(4)
+    psf = synth.widefield_psf(shape, 0.1, 0.085)
+    x = rng.random(shape).astype(np.float32)
+    c = D.LinearFFTConvolver(psf, shape, fft_shape=(256, 256, 256), precision="mixed")
+    f_lean, a_lean = c.forward(x).cpu().numpy(), c.adjoint(x).cpu().numpy()
+    monkeypatch.setenv("DECON_PIPE_LEAN", "0")
+    f_reg, a_reg = c.forward(x).cpu().numpy(), c.adjoint(x).cpu().numpy()
+    np.testing.assert_array_equal(f_lean, f_reg)
+    np.testing.assert_array_equal(a_lean, a_reg)
+    c32 = D.LinearFFTConvolver(psf, shape, fft_shape=(256, 256, 256))
+    e = rel(f_lean, c32.forward(x))
+    print(f"mixed lean axial pass vs FP32: {e:.2e}")
+    assert 0 < e < 2e-3
