@@ -306,15 +306,9 @@ static int conv_create_impl(const float* kernel, const int64_t kshape[3],
     p->T_x = 0;
     // lines per CTA
     {
-        auto lines = [](int L, int cap) {
-            int T = 1;
-            while (T * 2 <= cap && (T * 2) * L <= kSmemElems && (T * 2) * ((L + 31) / 32) <= kFftThreads)
-                T *= 2;
-            return T;
-        };
-        p->T_x = p->T_x0 = lines(p->ax_x.L, 32);
-        p->T_y = p->T_y0 = lines(p->ax_y.L, 16);
-        p->T_z = p->T_z0 = lines(p->ax_z.L, 16);
+        p->T_x = p->T_x0 = fft_lines_per_cta(p->ax_x, 32);
+        p->T_y = p->T_y0 = fft_lines_per_cta(p->ax_y, 16);
+        p->T_z = p->T_z0 = fft_lines_per_cta(p->ax_z, 16);
     }
     int st;
     const cudaStream_t s = as_stream(stream);
@@ -447,7 +441,7 @@ int decon_conv_set_schedule(decon_conv* p, int sched) {
         a.tw = axes[i]->tw;
         a.tws = axes[i]->tws;
         *axes[i] = a;
-        const bool runtime = !(L == 64 || L == 128 || L == 256 || L == 512 || L == 1024);
+        const bool runtime = !static_length(L);
         *lines[i] = (runtime && (sched & DECON_SCHED_HALF_LINES) && lines0[i] >= 2) ? lines0[i] / 2
                                                                                   : lines0[i];
     }

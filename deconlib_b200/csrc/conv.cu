@@ -38,7 +38,7 @@ namespace dk {
 // ---------------------------------------------------------------------------
 
 template <int LS>
-__global__ void __launch_bounds__(kFftThreads) k_colfft(ColArgs a) {
+__global__ void __launch_bounds__(LS > 0 ? kFftThreads : kDynThreads, 1) k_colfft(ColArgs a) {
     extern __shared__ float2 sm[];
     const int T = a.T, L = a.ax.L, tid = threadIdx.x;
     const int64_t o = blockIdx.x / a.ntiles;
@@ -179,7 +179,7 @@ bool plan_axis(int L, Axis& ax, int order) {
     if (n != 1 || (int)r.size() > kMaxStages) return false;
     ax.nst = (int)r.size();
     for (int i = 0; i < ax.nst; ++i) ax.rad |= (unsigned long long)r[i] << (4 * i);
-    ax.tpl = (L + 31) / 32;
+    ax.tpl = static_length(L) ? (L + 31) / 32 : (L + kDynPPT - 1) / kDynPPT;
     return true;
 }
 

@@ -15,6 +15,16 @@ constexpr int kSmemElems = 8192;  // complex values per CTA (64 KB)
 // CTA to kSmemElems / 32 threads.
 constexpr int kFftThreads = kSmemElems / 32;
 
+// Lines per CTA for an axis: the largest power of two <= cap whose tile fits
+// kSmemElems complex values and whose threads (T x tpl) fit the CTA limit of
+// the length's path.
+inline int fft_lines_per_cta(const Axis& ax, int cap) {
+    const int lim = static_length(ax.L) ? kFftThreads : kDynThreads;
+    int T = 1;
+    while (T * 2 <= cap && (T * 2) * ax.L <= kSmemElems && (T * 2) * ax.tpl <= lim) T *= 2;
+    return T;
+}
+
 // A float32 array of shape (wz, wy, wx) placed at offset (oz, oy, ox) inside
 // the N-space volume; voxels outside the box read as zero / are not written.
 struct Win3 {

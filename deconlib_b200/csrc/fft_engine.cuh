@@ -24,11 +24,25 @@ namespace dk {
 
 constexpr int kMaxStages = 16;
 
+// Lengths with a compile-time radix sequence (fft_lines_pow2); every other
+// 7-smooth length takes the runtime-radix path.
+__host__ __device__ constexpr bool static_length(int L) {
+    return L == 64 || L == 128 || L == 256 || L == 512 || L == 1024;
+}
+// Runtime-radix path: each thread holds ceil(kDynPPT / R) butterflies per
+// stage (<= 14 values, all in registers), so a line takes ceil(L / kDynPPT)
+// threads and a CTA up to kDynThreads.  (Holding 32 points per thread across
+// a stage's barrier, as the compile-time path does, spilled every value to
+// local memory on the runtime path and ran the strided passes at ~7 % of
+// HBM bandwidth.)
+constexpr int kDynPPT = 8;
+constexpr int kDynThreads = 1024;
+
 struct Axis {
     int L;                  // complex points per line
     int nst;                // radix stages
     unsigned long long rad; // radix of stage s in bits [4s, 4s+4), product == L
-    int tpl;                // threads per line = ceil(L / 32)
+    int tpl;                // threads per line: ceil(L / 32), runtime path ceil(L / kDynPPT)
     int tws;                // table stride: W_L^m = tw[m * tws]
     const float2* tw;       // twiddle table (device)
     __host__ __device__ int radix(int s) const { return (int)((rad >> (4 * s)) & 15ull); }
@@ -212,16 +226,16 @@ __device__ __forceinline__ void dft(float2* v) {
 }
 
 // One Stockham stage.  (t, jb): this thread's line and first butterfly.
-template <int R, int DIR, int NS_STATIC, int SW = 0>
+template <int R, int DIR, int NS_STATIC, int SW = 0, int PPT = 32>
 __device__ __forceinline__ void stage_body(float2* buf, int T, int L, int Ns_dyn, int t, int jb,
                                            int tpl, const float2* __restrict__ tw, int tws,
                                            int nin = 1 << 30, int nout = 1 << 30) {
     // nin: points >= nin are known zeros (only meaningful in a first stage,
     // where point index = input index); nout: points >= nout are not stored
     // (only in a last stage, where point index = output index).
-    // ceil(32 / R) butterflies per thread cover L / R butterflies with
-    // ceil(L / 32) threads per line for every radix (<= 35 values held).
-    constexpr int K = (32 + R - 1) / R;
+    // ceil(PPT / R) butterflies per thread cover L / R butterflies with
+    // ceil(L / PPT) threads per line for every radix (<= PPT + R - 1 values held).
+    constexpr int K = (PPT + R - 1) / R;
     const int Ns = NS_STATIC > 0 ? NS_STATIC : Ns_dyn;
     const int nb = L / R;
     const int step = L / (Ns * R);  // twiddle index step in units of W_L
@@ -263,7 +277,7 @@ __device__ __forceinline__ void stage_body(float2* buf, int T, int L, int Ns_dyn
 template <int R, int DIR>
 __device__ __noinline__ void fft_stage_dyn(float2* buf, int T, int L, int Ns, int t, int jb,
                                            int tpl, const float2* tw, int tws) {
-    stage_body<R, DIR, 0>(buf, T, L, Ns, t, jb, tpl, tw, tws);
+    stage_body<R, DIR, 0, 0, kDynPPT>(buf, T, L, Ns, t, jb, tpl, tw, tws);
 }
 
 template <int DIR>

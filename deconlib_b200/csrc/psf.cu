@@ -67,7 +67,7 @@ __global__ void k_psf_energy(const float2* __restrict__ pupil, int64_t n, double
 
 // Pass 1: one CTA = T columns of one plane; defocus on load, inverse FFT along y.
 template <int LS>
-__global__ void __launch_bounds__(kFftThreads) k_psf_cols(const PsfColArgs a) {
+__global__ void __launch_bounds__(LS > 0 ? kFftThreads : kDynThreads, 1) k_psf_cols(const PsfColArgs a) {
     extern __shared__ float2 sm[];
     const int T = a.T, L = a.ax.L, tid = threadIdx.x;
     const int64_t o = blockIdx.x / a.ntiles;
@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kFftThreads) k_psf_cols(const PsfColArgs a) {
 
 // Pass 2: one CTA = T contiguous rows; inverse FFT along x, |.|^2 * scale.
 template <int LS>
-__global__ void __launch_bounds__(kFftThreads) k_psf_rows(const PsfRowArgs a) {
+__global__ void __launch_bounds__(LS > 0 ? kFftThreads : kDynThreads, 1) k_psf_rows(const PsfRowArgs a) {
     extern __shared__ float2 sm[];
     const int T = a.T, L = a.ax.L, tid = threadIdx.x;
     const int64_t row0 = (int64_t)blockIdx.x * T;
@@ -176,11 +176,6 @@ static int psf_pool(cudaMemPool_t* out) {
     return DECON_OK;
 }
 
-static int lines_for(int L, int cap) {
-    int T = 1;
-    while (T * 2 <= cap && (T * 2) * L <= kSmemElems && (T * 2) * ((L + 31) / 32) <= kFftThreads) T *= 2;
-    return T;
-}
 
 static int threads_for_lines(int T, const Axis& ax) {
     return std::max(64, (int)round_up((int64_t)T * ax.tpl, 32));
@@ -258,11 +253,11 @@ extern "C" int decon_pupil_to_psf(const float* pupil, const double* kz, const do
         ca.nyx = nyx;
         ca.nx = (int)nx;
         ca.ax = axy;
-        ca.T = lines_for((int)ny, 32);
+        ca.T = fft_lines_per_cta(axy, 32);
         ca.ntiles = (int)cdiv(nx, ca.T);
         ra.a = a;
         ra.ax = axx;
-        ra.T = lines_for((int)nx, 32);
+        ra.T = fft_lines_per_cta(axx, 32);
         ra.fd_L = make_fastdiv(nx);
         void* fc = pick((int)ny, true);
         void* fr = pick((int)nx, false);

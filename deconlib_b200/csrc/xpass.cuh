@@ -87,7 +87,7 @@ __device__ __forceinline__ float fetch_x(const XR2CArgs& a, const RowSrc& r, int
 __host__ __device__ constexpr int x_lines(int LS) { return LS >= 1024 ? 8 : (LS >= 512 ? 16 : 32); }
 
 template <int PRO, int LS>
-__global__ void __launch_bounds__(kFftThreads, 3) k_xr2c(XR2CArgs a) {
+__global__ void __launch_bounds__(LS > 0 ? kFftThreads : kDynThreads, LS > 0 ? 3 : 1) k_xr2c(XR2CArgs a) {
     extern __shared__ float2 sm[];
     __shared__ RowSrc rsrc[32];  // per-row source (general path)
     constexpr int TC = LS > 0 ? x_lines(LS) : 0;  // compile-time lines per CTA
@@ -314,7 +314,7 @@ __device__ __forceinline__ void epilogue(const XC2RArgs& a, int64_t i, float v, 
 }
 
 template <int EPI, int LS>
-__global__ void __launch_bounds__(kFftThreads, 2) k_xc2r(XC2RArgs a) {
+__global__ void __launch_bounds__(LS > 0 ? kFftThreads : kDynThreads, LS > 0 ? 2 : 1) k_xc2r(XC2RArgs a) {
     extern __shared__ float2 sm[];
     __shared__ float2 nyq[32];    // X[M] of each row (even Fx)
     __shared__ int64_t obase[32];  // output index of x = 0 of each row (general path)
