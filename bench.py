@@ -184,14 +184,16 @@ def serve_jobs(D, n_jobs, seed=4):
     return jobs, rate
 
 
-def solve_alone(D, job):
-    """One job through the public API (the plain FP32 GPU form)."""
+def solve_alone(D, job, fft=None):
+    """One job through the public API (the plain FP32 GPU form; ``fft``: the
+    canvas, default the reference's)."""
     if job.kind == "rl":
-        r = D.richardson_lucy_with_operator(job.observed, D.LinearFFTConvolver(job.psf, job.observed.shape),
-                                            num_iter=job.num_iter, background=job.background)
+        conv = D.LinearFFTConvolver(job.psf, job.observed.shape, fft_shape=fft)
+        r = D.richardson_lucy_with_operator(job.observed, conv, num_iter=job.num_iter,
+                                            background=job.background)
     else:
         r = D.solve_pdhg_mlx(job.observed, job.psf, num_iter=job.num_iter, background=job.background,
-                             **job.options)
+                             fft_shape=fft, **job.options)
     return r.restored.cpu().numpy(), r.iterations
 
 
@@ -199,7 +201,7 @@ def run_serving(D, n_jobs):
     """Served stream vs the same jobs solved one at a time through the API."""
     import torch
 
-    from deconlib_b200.serving import DeconServer, job_signal_shape
+    from deconlib_b200.serving import DeconServer, job_fft_shape, job_signal_shape
 
     jobs, rate = serve_jobs(D, n_jobs)
     server = DeconServer(budget_bytes=150 * 10**9, max_active=8, chunk=8)
@@ -208,23 +210,93 @@ def run_serving(D, n_jobs):
     burst = server.run(jobs, realtime=False)
     flat = DeconServer(budget_bytes=150 * 10**9, max_active=8, chunk=8, prioritise=False).run(
         jobs, realtime=True)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    alone = [solve_alone(D, j) for j in jobs]
-    torch.cuda.synchronize()
-    t_seq = time.perf_counter() - t0
+    ref_canvas = DeconServer(budget_bytes=150 * 10**9, max_active=8, chunk=8,
+                             canvas="reference").run(jobs, realtime=True)
+
+    def sequential(fft_of):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = [solve_alone(D, j, fft_of(j)) for j in jobs]
+        torch.cuda.synchronize()
+        return res, time.perf_counter() - t0
+
+    alone, t_seq = sequential(lambda j: None)
+    alone_static, t_seq_static = sequential(lambda j: job_fft_shape(j, "static"))
     vi = sum(int(np.prod(job_signal_shape(j))) * it for j, (_, it) in zip(jobs, alone))
-    worst = 0.0
-    for res, (ref, _) in zip(live.results, alone):
-        worst = max(worst, float(np.linalg.norm(res.restored - ref) / max(np.linalg.norm(ref), 1e-30)))
+
+    def worst(results, refs):
+        w = 0.0
+        for res, (ref, _) in zip(results, refs):
+            w = max(w, float(np.linalg.norm(res.restored - ref) / max(np.linalg.norm(ref), 1e-30)))
+        return w
+
     out = {"workload": "poisson_stream_rl50_pdhg100_mixed_shapes", "jobs": len(jobs),
            "rate_jobs_per_s": rate, "budget_bytes": server.budget, "max_active": server.max_active,
+           "canvas": server.canvas,
+           "vs_fp64_oracle": _served_vs_oracle(D),
            "realtime": live.summary(), "all_at_once": burst.summary(),
            "realtime_equal_priority": flat.summary(),
+           "realtime_reference_canvas": ref_canvas.summary(),
            "plain_sequential_voxel_iter_per_s": vi / t_seq, "plain_sequential_s": t_seq,
-           "max_rel_l2_served_vs_alone": worst,
+           "plain_sequential_static_canvas_voxel_iter_per_s": vi / t_seq_static,
+           "served_vs_plain_sequential": live.voxel_iters_per_s / (vi / t_seq),
+           "max_rel_l2_served_vs_alone_same_canvas": worst(live.results, alone_static),
+           "max_rel_l2_served_static_vs_reference_canvas": worst(live.results, alone),
            "note": "latency = arrival to restored volume on the host; plain = the same jobs "
-                   "one at a time through richardson_lucy_with_operator / solve_pdhg_mlx"}
+                   "one at a time through richardson_lucy_with_operator / solve_pdhg_mlx on the "
+                   "reference's canvases (fast_padded_shape); the server puts each job on "
+                   "static_fft_shape (compile-time FFT lengths)"}
+    return out
+
+
+def _served_vs_oracle(D):
+    """Accuracy of the served form against the FP64 NumPy oracle (the
+    reference's solvers restated in float64 on the reference's canvas,
+    scipy.fft on every host core): one RL job (50 iterations) and one
+    Hessian-PDHG job (100 iterations, sampling 2) of the stream's smallest
+    object shape, 32x128x128, served together; relative L2 and max-abs error
+    of each restored volume.  (The full-size jobs of the stream would keep
+    the oracle busy for many minutes.)"""
+    from deconlib_b200 import synth
+    from deconlib_b200.serving import DeconServer, Job
+    from oracle import ops, solvers
+
+    ops.set_fft_workers(len(os.sched_getaffinity(0)))
+    rng = np.random.default_rng(11)
+    shp = (32, 128, 128)
+    jobs = []
+    for i, (kind, sp) in enumerate((("rl", SPACING_RL), ("pdhg", SPACING_PD))):
+        psf = synth.widefield_psf(shp, sp[0], sp[1], wavelength=0.52, na=1.2, ni=1.45, ns=1.334,
+                                  depth=8.0)
+        truth = synth.beads(shp, 100, rng)
+        synth.shells(shp, sp, 3, rng, out=truth)
+        if kind == "rl":
+            blur = ops.LinearFFTConvolver(psf, shp, dtype=np.float64).forward(truth.astype(np.float64))
+            obs = synth.poisson_observation(blur, 1000.0, 10.0, rng)
+            jobs.append(Job(i, "rl", obs, psf, 50, 0.0, 10.0))
+        else:
+            fwd = ops.compose(ops.FractionalAreaDownsample(2.0, in_shape=shp, dtype=np.float64),
+                              ops.LinearFFTConvolver(psf, shp, dtype=np.float64))
+            obs = synth.poisson_observation(fwd.forward(truth.astype(np.float64)), 500.0, 5.0, rng)
+            opts = dict(alpha=1e-3, regularization="hessian", sampling_factors=2.0, spacing=SPACING_PD)
+            jobs.append(Job(i, "pdhg", obs, psf, 100, 0.0, 5.0, opts))
+    rep = DeconServer(budget_bytes=150 * 10**9, max_active=8, chunk=8).run(jobs, realtime=False)
+    out = {"oracle": "oracle/ NumPy restatement of rl_mlx.py / pdhg_mlx.py in float64"}
+    for job, res in zip(jobs, rep.results):
+        if job.kind == "rl":
+            o64 = ops.LinearFFTConvolver(job.psf, shp, dtype=np.float64)
+            ref = solvers.richardson_lucy_with_operator(job.observed, o64, num_iter=job.num_iter,
+                                                        background=job.background,
+                                                        dtype=np.float64)["restored"]
+        else:
+            ref = solvers.solve_pdhg_mlx(job.observed, job.psf, num_iter=job.num_iter,
+                                         background=job.background, dtype=np.float64,
+                                         **job.options)["restored"]
+        x = res.restored.astype(np.float64)
+        out[f"{job.kind}_{'x'.join(map(str, shp))}_{job.num_iter}it"] = {
+            "rel_l2": float(np.linalg.norm(x - ref) / np.linalg.norm(ref)),
+            "max_abs": float(np.abs(x - ref).max()), "ref_max": float(np.abs(ref).max())}
+    ops.set_fft_workers(1)
     return out
 
 

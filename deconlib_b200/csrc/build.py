@@ -18,7 +18,8 @@ PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 OBJ = os.path.join(ROOT, "_build", "obj")
 LIB = os.path.join(PKG, "libdecon_b200.so")
-SOURCES = ["capi.cu", "conv.cu", "reduce.cu", "ops.cu", "solvers.cu", "noalloc.cu", "batch.cu", "psf.cu", "nlcg.cu", "pdhg_run.cu", "pupil.cu"]
+SOURCES = ["capi.cu", "conv.cu", "reduce.cu", "ops.cu", "solvers.cu", "noalloc.cu", "batch.cu", "psf.cu", "nlcg.cu", "pdhg_run.cu", "pupil.cu",
+           "xstatic_r2c.cu", "xstatic_c2r.cu", "xstatic_col.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -34,51 +34,6 @@
 namespace dk {
 
 // ---------------------------------------------------------------------------
-// passes 2-4: complex FFT along a strided axis over 16-wide column tiles
-// ---------------------------------------------------------------------------
-
-template <int LS>
-__global__ void __launch_bounds__(LS > 0 ? kFftThreads : kDynThreads, 1) k_colfft(ColArgs a) {
-    extern __shared__ float2 sm[];
-    const int T = a.T, L = a.ax.L, tid = threadIdx.x;
-    const int64_t o = blockIdx.x / a.ntiles;
-    const int64_t kx0 = (int64_t)(blockIdx.x - o * a.ntiles) * T;
-    const float2* src = a.src + o * a.src_os + kx0;
-    const int lgT = 31 - __clz(T);  // T is a power of two
-    for (int q = tid; q < L * T; q += blockDim.x) {
-        const int j = q >> lgT, t = q & (T - 1);
-        float2 v = make_float2(0.f, 0.f);
-        if (j < a.nin && kx0 + t < a.ncols) v = src[(int64_t)j * a.src_js + t];
-        sm[phys(j, t, T)] = v;
-    }
-    __syncthreads();
-    const int t = tid % T, jb = tid / T;
-    if (a.mode == COL_INV) {
-        fft_lines<+1, LS>(sm, T, t, jb, a.ax);
-    } else {
-        fft_lines<-1, LS>(sm, T, t, jb, a.ax);
-    }
-    if (a.mode == COL_OTF || a.mode == COL_OTF_CONJ) {
-        const float2* otf = a.otf + o * a.otf_os + kx0;
-        for (int q = tid; q < L * T; q += blockDim.x) {
-            const int j = q >> lgT, tt = q & (T - 1);
-            if (kx0 + tt < a.ncols) {
-                const float2 w = __ldg(&otf[(int64_t)j * a.otf_js + tt]);
-                const int p = phys(j, tt, T);
-                sm[p] = a.mode == COL_OTF ? cmul(sm[p], w) : cmulc(sm[p], w);
-            }
-        }
-        __syncthreads();
-        fft_lines<+1, LS>(sm, T, t, jb, a.ax);
-    }
-    float2* dst = a.dst + o * a.dst_os + kx0;
-    for (int q = tid; q < a.nout * T; q += blockDim.x) {
-        const int j = q >> lgT, tt = q & (T - 1);
-        if (kx0 + tt < a.ncols) dst[(int64_t)j * a.dst_js + tt] = sm[phys(j, tt, T)];
-    }
-}
-
-// ---------------------------------------------------------------------------
 // passes 2-4 on TMA: the same column transform with the tile moved by
 // cp.async.bulk.tensor (one elected thread issues the boxes; an mbarrier with
 // a bounded wait signals arrival; results leave through a TMA store).
@@ -120,9 +75,9 @@ __global__ void __launch_bounds__(kFftThreads, (LS >= 512 ? 1 : 2)) k_colfft_tma
     if (!ok) return;
     const int t = tid & 15, jb = tid >> 4;
     if (a.mode == COL_INV) {
-        fft_lines_pow2<LS, +1, 1, 1>(sm, 16, t, jb, a.tw, a.tws);
+        fft_lines_static<LS, +1, 1, 1>(sm, 16, t, jb, a.tw, a.tws);
     } else {
-        fft_lines_pow2<LS, -1, 1, 1>(sm, 16, t, jb, a.tw, a.tws);
+        fft_lines_static<LS, -1, 1, 1>(sm, 16, t, jb, a.tw, a.tws);
     }
     if (otf) {
         for (int q = tid; q < LS * 16; q += blockDim.x) {
@@ -130,7 +85,7 @@ __global__ void __launch_bounds__(kFftThreads, (LS >= 512 ? 1 : 2)) k_colfft_tma
             sm[q] = a.mode == COL_OTF ? cmul(sm[q], w) : cmulc(sm[q], w);
         }
         __syncthreads();
-        fft_lines_pow2<LS, +1, 1, 1>(sm, 16, t, jb, a.tw, a.tws);
+        fft_lines_static<LS, +1, 1, 1>(sm, 16, t, jb, a.tw, a.tws);
     }
     fence_proxy_async_smem();
     __syncthreads();
@@ -187,33 +142,6 @@ static int threads_for(int T, const Axis& ax) {
     int n = T * ax.tpl;
     n = (int)round_up(n, 32);
     return std::max(n, 64);
-}
-
-// Kernel selection: one instantiation per static length (0 = runtime radices).
-template <int PRO, int LS>
-static void* xr2c_ptr() { return (void*)k_xr2c<PRO, LS>; }
-template <int EPI, int LS>
-static void* xc2r_ptr() { return (void*)k_xc2r<EPI, LS>; }
-
-template <int PRO>
-static void* pick_xr2c(int L) {
-#define DK_CASE(n) if (L == n) return xr2c_ptr<PRO, n>();
-    DK_STATIC_LENGTHS(DK_CASE)
-#undef DK_CASE
-    return xr2c_ptr<PRO, 0>();
-}
-template <int EPI>
-static void* pick_xc2r(int L) {
-#define DK_CASE(n) if (L == n) return xc2r_ptr<EPI, n>();
-    DK_STATIC_LENGTHS(DK_CASE)
-#undef DK_CASE
-    return xc2r_ptr<EPI, 0>();
-}
-static void* pick_col(int L) {
-#define DK_CASE(n) if (L == n) return (void*)k_colfft<n>;
-    DK_STATIC_LENGTHS(DK_CASE)
-#undef DK_CASE
-    return (void*)k_colfft<0>;
 }
 
 // Kernel-class timing (decon_profile_start / _stop): CUDA events recorded
@@ -387,7 +315,7 @@ int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cva
     if (pro == PRO_UP2) a.vec4 = up2_vec;
     a.T = p.T_x;
     a.nrows = nz_rows * a.Ny;
-    if (a.ax.L == 64 || a.ax.L == 128 || a.ax.L == 256 || a.ax.L == 512 || a.ax.L == 1024)
+    if (static_length(a.ax.L))
         if (a.T != x_lines(a.ax.L)) return fail(DECON_ERR_UNSUPPORTED, "X pass lines per CTA mismatch");
     {
         const int L = a.ax.L;
@@ -400,15 +328,8 @@ int launch_xr2c(const ConvPlan& p, int pro, const float* in, Win3 win, float cva
     const int nthr = threads_for(a.T, a.ax);
     const int64_t nblk = cdiv(a.nrows, a.T);
     const size_t smem = (size_t)a.T * a.ax.L * sizeof(float2);
-    void* fn = nullptr;
-    switch (pro) {
-        case PRO_ARRAY: fn = pick_xr2c<PRO_ARRAY>(a.ax.L); break;
-        case PRO_CONST: fn = pick_xr2c<PRO_CONST>(a.ax.L); break;
-        case PRO_KERNEL: fn = pick_xr2c<PRO_KERNEL>(a.ax.L); break;
-        case PRO_RLINIT: fn = pick_xr2c<PRO_RLINIT>(a.ax.L); break;
-        case PRO_UP2: fn = pick_xr2c<PRO_UP2>(a.ax.L); break;
-        default: return fail(DECON_ERR_VALUE, "bad prologue %d", pro);
-    }
+    void* fn = pick_xr2c_kernel(pro, a.ax.L);
+    if (!fn) return fail(DECON_ERR_VALUE, "bad prologue %d", pro);
     return launch(fn, nblk, nthr, smem, st, &a, PROF_XR2C);
 }
 
@@ -435,7 +356,7 @@ int launch_col(const ConvPlan& p, const Axis& ax, int T, int mode, const float2*
     const int nthr = threads_for(T, ax);
     const int64_t nblk = nouter * a.ntiles;
     const size_t smem = (size_t)T * ax.L * sizeof(float2);
-    return launch(pick_col(ax.L), nblk, nthr, smem, st, &a,
+    return launch(pick_colfft_kernel(ax.L), nblk, nthr, smem, st, &a,
                   (mode == COL_OTF || mode == COL_OTF_CONJ) ? PROF_ZOTF : PROF_COL);
 }
 
@@ -459,7 +380,7 @@ int launch_xc2r(const ConvPlan& p, int epi, const float2* in, Win3 win, float* o
         a.vec4 = full && !p.odd && (p.N[2] % 4) == 0 && al(out) && al(aux0) && al(aux1);
     }
     a.T = p.T_x;
-    if (a.ax.L == 64 || a.ax.L == 128 || a.ax.L == 256 || a.ax.L == 512 || a.ax.L == 1024)
+    if (static_length(a.ax.L))
         if (a.T != x_lines(a.ax.L)) return fail(DECON_ERR_UNSUPPORTED, "X pass lines per CTA mismatch");
     a.scale = (float)(1.0 / ((double)p.F[0] * (double)p.F[1] * (double)p.F[2]));
     a.win = win;
@@ -488,15 +409,8 @@ int launch_xc2r(const ConvPlan& p, int epi, const float2* in, Win3 win, float* o
     const int64_t nblk = cdiv(a.nrows, a.T);
     if (nblk_out) *nblk_out = (int)nblk;
     const size_t smem = (size_t)a.T * a.ax.L * sizeof(float2);
-    void* fn = nullptr;
-    switch (epi) {
-        case EPI_STORE: fn = pick_xc2r<EPI_STORE>(a.ax.L); break;
-        case EPI_RL_RATIO: fn = pick_xc2r<EPI_RL_RATIO>(a.ax.L); break;
-        case EPI_RL_UPDATE: fn = pick_xc2r<EPI_RL_UPDATE>(a.ax.L); break;
-        case EPI_PRED: fn = pick_xc2r<EPI_PRED>(a.ax.L); break;
-        case EPI_DOWN2: fn = pick_xc2r<EPI_DOWN2>(a.ax.L); break;
-        default: return fail(DECON_ERR_VALUE, "bad epilogue %d", epi);
-    }
+    void* fn = pick_xc2r_kernel(epi, a.ax.L);
+    if (!fn) return fail(DECON_ERR_VALUE, "bad epilogue %d", epi);
     return launch(fn, nblk, nthr, smem, st, &a, PROF_XC2R);
 }
 

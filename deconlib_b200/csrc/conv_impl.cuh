@@ -169,6 +169,14 @@ bool zpass_pipelined(const ConvPlan& p);
 int kernel_prepare(void* fn, size_t smem, int nthr, int* per_sm);
 
 bool tma_length_ok(int L);
+// Kernels of the X R2C / X C2R / plain column passes for one axis length
+// (the static-length instantiation, or the runtime-radix one), by prologue /
+// epilogue code; nullptr for an unknown code.  One translation unit each
+// (xstatic_r2c.cu, xstatic_c2r.cu, xstatic_col.cu), so they build in parallel.
+void* pick_xr2c_kernel(int pro, int L);
+void* pick_xc2r_kernel(int epi, int L);
+void* pick_colfft_kernel(int L);
+
 // Rank-3 map over an FP16 complex [d2][d1][pitch] buffer (one half2 = one
 // 4-byte element) with (16, 1, b2) boxes and no swizzle.
 bool encode_half_plane_map(CUtensorMap* map, const __half2* base, int64_t pitch, int64_t d1, int64_t d2,

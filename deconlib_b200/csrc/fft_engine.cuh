@@ -24,10 +24,17 @@ namespace dk {
 
 constexpr int kMaxStages = 16;
 
-// Lengths with a compile-time radix sequence (fft_lines_pow2); every other
-// 7-smooth length takes the runtime-radix path.
+// Lengths with a compile-time radix sequence (fft_lines_static): 2^a x {1, 3,
+// 5, 15} from 64 to 1024, so that a canvas rounded up to one of them grows an
+// axis by at most 1/3; every other 7-smooth length takes the runtime-radix
+// path.
+#define DK_STATIC_LENGTHS(X) \
+    X(64) X(80) X(96) X(128) X(160) X(192) X(240) X(256) X(320) X(384) X(480) X(512) X(640) X(768) \
+    X(960) X(1024)
 __host__ __device__ constexpr bool static_length(int L) {
-    return L == 64 || L == 128 || L == 256 || L == 512 || L == 1024;
+#define DK_IS(n) L == n ||
+    return DK_STATIC_LENGTHS(DK_IS) false;
+#undef DK_IS
 }
 // Runtime-radix path: each thread holds ceil(kDynPPT / R) butterflies per
 // stage (<= 14 values, all in registers), so a line takes ceil(L / kDynPPT)
@@ -298,24 +305,30 @@ __device__ __forceinline__ void fft_lines_dyn(float2* buf, int T, int t, int jb,
     }
 }
 
-// Power-of-two lengths with the radix sequence fixed at compile time
-// (pow2_radix): straight-line stages, shifts for j div Ns.  The runtime
-// path (plan_axis, for non-instantiated lengths) uses radices <= 8.
-// Radix-16 stages first (fewest shared-memory round trips), then 8 / 4 / 2:
-// 64 = 16.4, 128 = 16.8, 256 = 16.16, 512 = 16.8.4, 1024 = 16.16.4.
-constexpr int pow2_radix(int rem) {
-    return rem >= 16 && rem != 32 ? 16 : (rem == 32 ? 8 : rem);
+// Static lengths with the radix sequence fixed at compile time
+// (static_radix): straight-line stages, constant divisors for j div Ns.  The
+// runtime path (plan_axis, for non-instantiated lengths) uses radices <= 8.
+// The power-of-two part first, radix-16 stages first (fewest shared-memory
+// round trips), then 8 / 4 / 2, then the odd factors 5 and 3:
+// 64 = 16.4, 128 = 16.8, 256 = 16.16, 512 = 16.8.4, 1024 = 16.16.4,
+// 80 = 16.5, 96 = 8.4.3, 160 = 8.4.5, 192 = 16.4.3, 240 = 16.5.3,
+// 320 = 16.4.5, 384 = 16.8.3, 480 = 8.4.5.3, 640 = 16.8.5, 768 = 16.16.3,
+// 960 = 16.4.5.3.
+constexpr int static_radix(int rem) {
+    const int p = rem & -rem;  // power-of-two part
+    if (p > 1) return p >= 16 && p != 32 ? 16 : (p == 32 ? 8 : p);
+    return rem % 5 == 0 ? 5 : (rem % 3 == 0 ? 3 : (rem % 7 == 0 ? 7 : rem));
 }
 
 template <int L, int DIR, int NS, int SW = 0>
-__device__ __forceinline__ void fft_lines_pow2(float2* buf, int T, int t, int jb,
-                                               const float2* __restrict__ tw, int tws,
-                                               int nin = 1 << 30, int nout = 1 << 30) {
+__device__ __forceinline__ void fft_lines_static(float2* buf, int T, int t, int jb,
+                                                 const float2* __restrict__ tw, int tws,
+                                                 int nin = 1 << 30, int nout = 1 << 30) {
     if constexpr (NS < L) {
-        constexpr int R = pow2_radix(L / NS);
+        constexpr int R = static_radix(L / NS);
         stage_body<R, DIR, NS, SW>(buf, T, L, NS, t, jb, (L + 31) / 32, tw, tws,
                                    NS == 1 ? nin : (1 << 30), NS * R == L ? nout : (1 << 30));
-        fft_lines_pow2<L, DIR, NS * R, SW>(buf, T, t, jb, tw, tws, nin, nout);
+        fft_lines_static<L, DIR, NS * R, SW>(buf, T, t, jb, tw, tws, nin, nout);
     }
 }
 
@@ -327,14 +340,11 @@ template <int DIR, int LS>
 __device__ __forceinline__ void fft_lines(float2* buf, int T, int t, int jb, const Axis ax,
                                           int nin = 1 << 30, int nout = 1 << 30) {
     if constexpr (LS > 0) {
-        fft_lines_pow2<LS, DIR, 1>(buf, T, t, jb, ax.tw, ax.tws, nin, nout);
+        fft_lines_static<LS, DIR, 1>(buf, T, t, jb, ax.tw, ax.tws, nin, nout);
     } else {
         fft_lines_dyn<DIR>(buf, T, t, jb, ax);
     }
 }
-
-// Lengths with a compile-time path; others use the runtime radix switch.
-#define DK_STATIC_LENGTHS(X) X(64) X(128) X(256) X(512) X(1024)
 
 // Host: factor L into supported radices (order 0: 8s first, then 4/2, 5, 3,
 // 7; order 1: the odd radices 5, 3, 7 first, then the power-of-two stages).

@@ -82,9 +82,14 @@ __device__ __forceinline__ float fetch_x(const XR2CArgs& a, const RowSrc& r, int
 // pass 1: X R2C
 // ---------------------------------------------------------------------------
 
-// Lines per CTA of the X passes for a compile-time length (the host's rule:
-// T x L <= 8192 complex values and T x L / 32 <= 256 threads, T <= 32).
-__host__ __device__ constexpr int x_lines(int LS) { return LS >= 1024 ? 8 : (LS >= 512 ? 16 : 32); }
+// Lines per CTA of the X passes for a compile-time length (the host's rule,
+// fft_lines_per_cta: T x L <= kSmemElems complex values and T x ceil(L / 32)
+// <= kFftThreads threads, T <= 32, a power of two).
+__host__ __device__ constexpr int x_lines(int LS) {
+    int T = 1;
+    while (T * 2 <= 32 && T * 2 * LS <= kSmemElems && T * 2 * ((LS + 31) / 32) <= kFftThreads) T *= 2;
+    return T;
+}
 
 template <int PRO, int LS>
 __global__ void __launch_bounds__(LS > 0 ? kFftThreads : kDynThreads, LS > 0 ? 3 : 1) k_xr2c(XR2CArgs a) {
@@ -208,7 +213,7 @@ __global__ void __launch_bounds__(LS > 0 ? kFftThreads : kDynThreads, LS > 0 ? 3
         }
     }
     __syncthreads();
-    if constexpr (LS > 0) fft_lines_pow2<LS, -1, 1, TC>(sm, T, tid % T, tid / T, a.ax.tw, a.ax.tws, nin);
+    if constexpr (LS > 0) fft_lines_static<LS, -1, 1, TC>(sm, T, tid % T, tid / T, a.ax.tw, a.ax.tws, nin);
     else fft_lines<-1, LS>(sm, T, tid % T, tid / T, a.ax, nin);
     const int H = a.Hx;
     const int lgT = 31 - __clz(T);  // T is a power of two
@@ -441,7 +446,7 @@ __global__ void __launch_bounds__(LS > 0 ? kFftThreads : kDynThreads, LS > 0 ? 2
     }
     // outputs beyond the kept x range are not needed
     const int nout = a.odd ? (int)(a.Nx < L ? a.Nx : L) : (int)(((a.Nx + 1) >> 1) < L ? ((a.Nx + 1) >> 1) : L);
-    if constexpr (LS > 0) fft_lines_pow2<LS, +1, 1, TC>(sm, T, tid % T, tid / T, a.ax.tw, a.ax.tws, 1 << 30, nout);
+    if constexpr (LS > 0) fft_lines_static<LS, +1, 1, TC>(sm, T, tid % T, tid / T, a.ax.tw, a.ax.tws, 1 << 30, nout);
     else fft_lines<+1, LS>(sm, T, tid % T, tid / T, a.ax, 1 << 30, nout);
 
     double acc = 0.0;

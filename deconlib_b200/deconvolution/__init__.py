@@ -12,7 +12,8 @@ from .base import MLXDeconvolutionResult
 from .composition import Compose, LinearOperator, as_numpy_op, compose
 from .core_operators import Crop, FractionalAreaDownsample, FractionalAreaUpsample, Pad
 from .linops import (FFTConvolver, Gradient1D, Gradient2D, Gradient3D, Hessian1D, Hessian2D,
-                     Hessian3D, LinearFFTConvolver, fast_padded_shape, pad_corner_origin_kernel)
+                     Hessian3D, LinearFFTConvolver, STATIC_FFT_LENGTHS, fast_padded_shape,
+                     pad_corner_origin_kernel, static_fft_shape)
 from .pdhg import (GradientRegularizer, HessianRegularizer, IdentityRegularizer, PDHGRunner,
                    pdhg_mlx_runner, pdhg_result, prox_gaussian_dual, prox_l1_2_dual, prox_l1_dual,
                    prox_nonneg, prox_poisson_dual, solve_pdhg_mlx, solve_pdhg_with_operator)
@@ -28,7 +29,8 @@ __all__ = [
     "MLXDeconvolutionResult", "Compose", "LinearOperator", "as_numpy_op", "compose", "Crop",
     "FractionalAreaDownsample", "FractionalAreaUpsample", "Pad", "FFTConvolver", "Gradient1D",
     "Gradient2D", "Gradient3D", "Hessian1D", "Hessian2D", "Hessian3D", "LinearFFTConvolver",
-    "fast_padded_shape", "pad_corner_origin_kernel", "GradientRegularizer", "HessianRegularizer",
+    "fast_padded_shape", "static_fft_shape", "STATIC_FFT_LENGTHS", "pad_corner_origin_kernel",
+    "GradientRegularizer", "HessianRegularizer",
     "IdentityRegularizer", "prox_gaussian_dual", "prox_l1_2_dual", "prox_l1_dual", "prox_nonneg",
     "prox_poisson_dual", "solve_pdhg_mlx", "solve_pdhg_with_operator", "RLResult",
     "poisson_i_divergence", "richardson_lucy_solver", "richardson_lucy_with_operator",

@@ -24,6 +24,7 @@ from ._device import empty, shape3, stream, to_device
 __all__ = [
     "Gradient1D", "Gradient2D", "Gradient3D", "Hessian1D", "Hessian2D", "Hessian3D",
     "FFTConvolver", "LinearFFTConvolver", "fast_padded_shape", "pad_corner_origin_kernel",
+    "STATIC_FFT_LENGTHS", "static_fft_shape",
 ]
 
 SQRT2 = float(np.sqrt(np.float32(2.0)))
@@ -55,6 +56,32 @@ def fast_padded_shape(signal_shape, kernel_shape, min_pad=None) -> Tuple[int, ..
     for n, m, p in zip(signal_shape, kernel_shape, pads):
         need = (m - 1) if p is None else int(p)
         out.append(_next_smooth_number(max(n + need, m)))
+    return tuple(out)
+
+
+# FFT lengths with a compile-time radix sequence in the library (2^a x {1, 3,
+# 5, 15}, 64 to 1024): the strided passes of these lengths run straight-line
+# stages; other 7-smooth lengths take the runtime-radix path, which measured
+# ~4x slower per canvas voxel on the B200.
+STATIC_FFT_LENGTHS = (64, 80, 96, 128, 160, 192, 240, 256, 320, 384, 480, 512, 640, 768, 960, 1024)
+
+
+def static_fft_shape(signal_shape, kernel_shape) -> Tuple[int, ...]:
+    """Wrap-free canvas on the compile-time FFT lengths (not in the reference).
+
+    Per axis the smallest length >= N + M - 1 in ``STATIC_FFT_LENGTHS`` (the
+    last axis, transformed as packed complex pairs, twice such a length), when
+    that grows the axis by at most 1/3 over ``fast_padded_shape``'s 5-smooth
+    length; otherwise the 5-smooth length.  A convolution's result does not
+    depend on the canvas beyond FP32 rounding."""
+    ref = fast_padded_shape(signal_shape, kernel_shape)
+    nd = len(ref)
+    out = []
+    for ax, (n, m, r) in enumerate(zip(signal_shape, kernel_shape, ref)):
+        need = max(int(n) + int(m) - 1, int(m))
+        scale = 2 if ax == nd - 1 else 1
+        c = next((scale * L for L in STATIC_FFT_LENGTHS if scale * L >= need), None)
+        out.append(c if c is not None and 3 * c <= 4 * r else r)
     return tuple(out)
 
 

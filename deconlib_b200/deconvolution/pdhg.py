@@ -553,11 +553,13 @@ class PDHGRunner:
         return x, final_iter, converged, taus, sigmas, losses
 
 
-def _conv_for(conv, psf, signal_shape, precision="fp32"):
+def _conv_for(conv, psf, signal_shape, precision="fp32", fft_shape=None):
     """A normalised LinearFFTConvolver of ``psf`` on ``signal_shape``: the
-    given pooled one with its OTF rebuilt, or a new one."""
+    given pooled one with its OTF rebuilt, or a new one (on ``fft_shape``,
+    default the reference's 5-smooth canvas)."""
     if conv is None:
-        return LinearFFTConvolver(psf, signal_shape=signal_shape, normalize=True, precision=precision)
+        return LinearFFTConvolver(psf, signal_shape=signal_shape, normalize=True, precision=precision,
+                                  fft_shape=fft_shape)
     if tuple(conv.signal_shape) != tuple(signal_shape) or not conv.normalize:
         raise ValueError(f"pooled convolver is for {conv.signal_shape}, the solve needs {signal_shape}")
     if conv.precision != precision:
@@ -574,18 +576,19 @@ def solve_pdhg_mlx(observed, psf, alpha: float = 0.01,
                    init=None, verbose: bool = False, callback: Optional[Callable] = None,
                    delta: float = 0.99, eta: float = 0.5, eval_interval: int = 10,
                    tol: float = 1e-5, min_iter: int = 20, patience: int = 5,
-                   precision: str = "fp32") -> MLXDeconvolutionResult:
+                   precision: str = "fp32", fft_shape=None) -> MLXDeconvolutionResult:
     """PSF entry point of adaptive PDHG (pdhg_mlx.py:507-920).
 
-    ``precision="mixed"`` (not in the reference) stores the OTF as FP16 with
-    per-plane scales (``LinearFFTConvolver.set_precision``)."""
+    Not in the reference: ``precision="mixed"`` stores the OTF as FP16 with
+    per-plane scales (``LinearFFTConvolver.set_precision``); ``fft_shape``
+    chooses the convolution canvas (e.g. ``static_fft_shape``)."""
     runner, meta = pdhg_mlx_runner(
         observed, psf, alpha=alpha, regularization=regularization, norm=norm, loss_type=loss_type,
         num_iter=num_iter, background=background, spacing=spacing, bin_factors=bin_factors,
         sampling_factors=sampling_factors, icf_sigmas=icf_sigmas, icf_spacings=icf_spacings,
         init=init, verbose=verbose, callback=callback, delta=delta, eta=eta,
         eval_interval=eval_interval, tol=tol, min_iter=min_iter, patience=patience,
-        precision=precision)
+        precision=precision, fft_shape=fft_shape)
     return pdhg_result(runner.run(), meta)
 
 
@@ -606,7 +609,7 @@ def pdhg_mlx_runner(observed, psf, alpha: float = 0.01,
                     delta: float = 0.99, eta: float = 0.5, eval_interval: int = 10,
                     tol: float = 1e-5, min_iter: int = 20, patience: int = 5,
                     conv: Optional[LinearFFTConvolver] = None, state=None,
-                    precision: str = "fp32", async_status: bool = False):
+                    precision: str = "fp32", async_status: bool = False, fft_shape=None):
     """Set-up of ``solve_pdhg_mlx`` without the iterations: returns the
     ``PDHGRunner`` (iterations queued on the current stream by ``iterate``)
     and the result metadata, for callers that interleave solves.
@@ -632,7 +635,7 @@ def pdhg_mlx_runner(observed, psf, alpha: float = 0.01,
                 "For sampling_factors, psf.shape must match the reconstructed "
                 f"high-resolution shape {highres}; got {psf_shape}"
             )
-        conv = _conv_for(conv, psf, highres, precision)
+        conv = _conv_for(conv, psf, highres, precision, fft_shape)
         blur_op = compose(FractionalAreaDownsample(scale=factors), conv)
     elif bin_factors is not None:
         factors = _normalize_bin_factors(bin_factors, ndim)
@@ -646,10 +649,10 @@ def pdhg_mlx_runner(observed, psf, alpha: float = 0.01,
                 "For bin_factors, observed.shape must match psf.shape divided "
                 f"by bin_factors; expected {lowres}, got {tuple(data.shape)}"
             )
-        conv = _conv_for(conv, psf, highres, precision)
+        conv = _conv_for(conv, psf, highres, precision, fft_shape)
         blur_op = compose(FractionalAreaDownsample(scale=factors), conv)
     else:
-        blur_op = _conv_for(conv, psf, tuple(data.shape), precision)
+        blur_op = _conv_for(conv, psf, tuple(data.shape), precision, fft_shape)
         highres = tuple(data.shape)
     r = _compute_spacing_ratio(spacing, ndim)
     reg = _create_regularizer(regularization, ndim, r, norm)

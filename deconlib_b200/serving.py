@@ -16,7 +16,13 @@ time.  The server
     kernel and signal shapes, which rebuilds the OTF in place
     (``LinearFFTConvolver.set_kernel``), and its PDHG state to the next PDHG
     job (``decon_pdhg_reset``).  Nothing is freed while jobs run, because
-    ``cudaFree`` synchronises the whole device and would drain every stream.
+    ``cudaFree`` synchronises the whole device and would drain every stream;
+  * puts every job's convolution on a canvas of compile-time FFT lengths
+    (``canvas="static"``: ``static_fft_shape``, each axis at most 1/3 longer
+    than the reference's 5-smooth canvas), because the runtime-radix FFT path
+    that most 5-smooth lengths take measured ~4x slower per canvas voxel;
+    ``canvas="reference"`` keeps ``fast_padded_shape``.  The canvas changes a
+    result by FP32 rounding only.
 
 Latency is arrival -> restored volume on the host.  The reference has no
 serving layer; each job computes exactly what ``richardson_lucy_with_operator``
@@ -34,7 +40,7 @@ from typing import Callable, Dict, List, Optional, Sequence, Tuple
 import numpy as np
 
 __all__ = ["Job", "JobResult", "ServeReport", "Scheduler", "DeconServer", "job_signal_shape",
-           "job_device_bytes", "poisson_arrivals"]
+           "job_fft_shape", "job_device_bytes", "poisson_arrivals"]
 
 
 @dataclass
@@ -109,8 +115,21 @@ def job_signal_shape(job: Job) -> Tuple[int, ...]:
     return tuple(int(s) for s in job.observed.shape)
 
 
-def _plan_bytes(signal, kernel) -> int:
-    f = _fast_padded(signal, kernel)
+def job_fft_shape(job: Job, canvas: str = "reference") -> Tuple[int, ...]:
+    """The job's convolution canvas under a canvas policy ("reference":
+    ``fast_padded_shape``; "static": ``static_fft_shape``)."""
+    sig = job_signal_shape(job)
+    if canvas == "reference":
+        return _fast_padded(sig, job.psf.shape)
+    if canvas == "static":
+        from .deconvolution.linops import static_fft_shape
+
+        return tuple(int(v) for v in static_fft_shape(sig, tuple(job.psf.shape)))
+    raise ValueError(f"canvas must be 'reference' or 'static', got {canvas!r}")
+
+
+def _plan_bytes(signal, kernel, fft=None) -> int:
+    f = tuple(fft) if fft is not None else _fast_padded(signal, kernel)
     while len(f) < 3:
         f = (1,) + f
     s = (1,) * (3 - len(signal)) + tuple(signal)
@@ -118,14 +137,15 @@ def _plan_bytes(signal, kernel) -> int:
     return 8 * pitch * (f[0] * f[1] + s[0] * s[1] + s[0] * f[1])
 
 
-def job_device_bytes(job: Job) -> int:
+def job_device_bytes(job: Job, canvas: str = "reference") -> int:
     """Device bytes the job holds while admitted: its convolution plan (OTF
-    and the two scratch spectra), its iterates and temporaries."""
+    and the two scratch spectra) on the policy's canvas, its iterates and
+    temporaries."""
     sig = job_signal_shape(job)
     n = int(np.prod(sig))
     m = int(np.prod(job.observed.shape))
     k = int(np.prod(job.psf.shape))
-    plan = _plan_bytes(sig, job.psf.shape)
+    plan = _plan_bytes(sig, job.psf.shape, job_fft_shape(job, canvas))
     if job.kind == "rl":
         arrays = 4 * (5 * n + k)
     else:
@@ -266,7 +286,7 @@ class _Pools:
 class _Slot:
     """One admitted job on its own stream."""
 
-    def __init__(self, job: Job, nbytes: int, pools: _Pools, now: float):
+    def __init__(self, job: Job, nbytes: int, pools: _Pools, now: float, canvas: str = "reference"):
         import torch
 
         from .deconvolution.linops import LinearFFTConvolver
@@ -279,12 +299,13 @@ class _Slot:
         self.event = None
         self.finished = False
         self.sig = job_signal_shape(job)
-        self.key = (tuple(job.psf.shape), self.sig)
+        self.fft = job_fft_shape(job, canvas)
+        self.key = (tuple(job.psf.shape), self.sig, self.fft)
         with torch.cuda.stream(self.stream):
             conv = pools.take_plan(self.key)
             if job.kind == "rl":
                 if conv is None:
-                    conv = LinearFFTConvolver(job.psf, self.sig)
+                    conv = LinearFFTConvolver(job.psf, self.sig, fft_shape=self.fft)
                 else:
                     conv.set_kernel(job.psf)
                 self.conv = conv
@@ -295,7 +316,7 @@ class _Slot:
                 self.state = pools.take_state(job.num_iter)
                 self.runner, self.meta = pdhg_mlx_runner(
                     job.observed, job.psf, num_iter=job.num_iter, background=job.background,
-                    conv=conv, state=self.state, async_status=True, **opts)
+                    conv=conv, state=self.state, async_status=True, fft_shape=self.fft, **opts)
                 self.conv = _find_conv(self.runner.A)
                 self.state = self.runner.state
             else:
@@ -331,7 +352,7 @@ class _Slot:
     def release(self) -> None:
         pools = self.pools
         if self.conv is not None:
-            pools.give_plan(self.key, self.conv, _plan_bytes(self.sig, self.job.psf.shape))
+            pools.give_plan(self.key, self.conv, _plan_bytes(self.sig, self.job.psf.shape, self.fft))
         if self.state is not None:
             pools.states.append(self.state)
         self.runner = None
@@ -357,14 +378,18 @@ class DeconServer:
 
     ``budget_bytes``: device bytes admitted jobs (plus idle pooled plans) may
     hold; ``max_active``: concurrent jobs (one stream each); ``chunk``:
-    iterations queued per job per scheduling round."""
+    iterations queued per job per scheduling round; ``canvas``: "static"
+    (compile-time FFT lengths) or "reference" (the reference's canvases)."""
 
     def __init__(self, budget_bytes: int = 150 * 10**9, max_active: int = 8, chunk: int = 8,
-                 prioritise: bool = True):
+                 prioritise: bool = True, canvas: str = "static"):
+        if canvas not in ("static", "reference"):
+            raise ValueError(f"canvas must be 'static' or 'reference', got {canvas!r}")
         self.budget = int(budget_bytes)
         self.max_active = int(max_active)
         self.chunk = int(chunk)
         self.prioritise = bool(prioritise)
+        self.canvas = canvas
 
     def run(self, jobs: Sequence[Job], clock: Callable[[], float] = time.perf_counter,
             realtime: bool = True) -> ServeReport:
@@ -374,7 +399,8 @@ class DeconServer:
         import torch
 
         order = sorted(jobs, key=lambda j: j.arrival)
-        sched = Scheduler(self.budget, self.max_active)
+        sched = Scheduler(self.budget, self.max_active,
+                          footprint=lambda j: job_device_bytes(j, self.canvas))
         pools = _Pools(self.max_active, self.prioritise)
         active: List[_Slot] = []
         results: List[JobResult] = []
@@ -391,7 +417,7 @@ class DeconServer:
             if lack > 0 and pools.idle_plan_bytes() > 0:
                 pools.evict_plans(lack)
             for job, b in sched.admit(pools.idle_plan_bytes()):
-                active.append(_Slot(job, b, pools, clock() - t0))
+                active.append(_Slot(job, b, pools, clock() - t0, self.canvas))
             max_conc = max(max_conc, len(active))
             progressed = False
             for slot in list(active):

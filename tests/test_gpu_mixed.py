@@ -2,10 +2,16 @@
 per kz plane, read by the pipelined axial pass.
 
 The FP16 mantissa (11 bits) bounds the relative error of each OTF value by
-2^-12 after rounding; a convolution output is a sum over many such products,
-so its relative L2 error against the FP32 path is a few 1e-4.  Tolerances
-here: 2e-3 for one convolution, 1e-2 for 50 RL iterations against the FP64
-oracle (the FP32 path is at ~1e-6 there).  Every result states its error."""
+2^-12 after rounding (per-plane power-of-two scales keep every plane's
+largest value near the top of the FP16 range); a convolution output is a sum
+over many such products, so its relative L2 error against the FP32 path is
+~1e-4 (measured 7-9e-5 at 64x128x128 and 128x256x256).  RL multiplies
+these errors into its iterate: against the FP64 oracle the mixed form
+measured 8.2e-5 / 8.5e-5 / 1.3e-4 at iterations 10 / 50 / 200 (the FP32 form
+6.8e-7 / 3.1e-6 / 1.2e-5).  Tolerances here: 2e-3 for one convolution,
+3e-4 for 20 RL iterations against the FP64 oracle (3x the measured error;
+a 1e-4 bound would need about two more mantissa bits than FP16 stores).
+Every result states its error."""
 
 import numpy as np
 import pytest
@@ -81,7 +87,7 @@ def test_mixed_rl_against_fp64_oracle(D):
     e32, e16 = rel(r32, ref), rel(r16, ref)
     print(f"RL {shape} x{n}: FP32 rel-L2 vs FP64 oracle {e32:.2e}, mixed {e16:.2e}")
     assert e32 < 1e-4
-    assert e16 < 1e-2
+    assert e16 < 3e-4
 
 
 def test_mixed_lean_axial_pass_bit_identical_to_register_form(D, monkeypatch):

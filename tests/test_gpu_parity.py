@@ -107,6 +107,35 @@ def test_conv_sizes_vs_fp64_oracle(D, shape, kshape):
     assert rel(c.adjoint(x), o.adjoint(x.astype(np.float64))) < 2e-6
 
 
+@pytest.mark.parametrize("fft", [(80, 96, 160), (160, 192, 192), (240, 320, 320), (384, 480, 384),
+                                 (64, 640, 480), (64, 768, 640), (64, 960, 768), (64, 64, 960),
+                                 (64, 64, 1280), (64, 64, 1536), (64, 64, 1920)])
+def test_static_length_canvases_vs_fp64_oracle(D, fft):
+    """Every compile-time FFT length of 2^a x {3, 5, 15} in the strided
+    passes (z, y) and in the X passes (packed length Fx / 2)."""
+    from oracle import ops
+
+    shape, kshape = (16, 24, 32), (7, 9, 11)
+    rng = np.random.default_rng(sum(fft))
+    k = rng.random(kshape).astype(np.float32)
+    x = rng.random(shape).astype(np.float32)
+    c = D.LinearFFTConvolver(k, shape, fft_shape=fft)
+    o = ops.LinearFFTConvolver(k, shape, fft_shape=fft, dtype=np.float64)
+    ef = rel(c.forward(x), o.forward(x.astype(np.float64)))
+    ea = rel(c.adjoint(x), o.adjoint(x.astype(np.float64)))
+    assert ef < 2e-6 and ea < 2e-6, (ef, ea)
+
+
+def test_static_fft_shape_rule(D):
+    assert D.static_fft_shape((76, 362, 244), (76, 362, 244)) == (160, 768, 512)
+    assert D.static_fft_shape((128, 256, 256), (128, 256, 256)) == (256, 512, 512)
+    # small axes keep the 5-smooth length when the static one is > 4/3 of it
+    assert D.static_fft_shape((16, 32, 32), (16, 32, 32)) == (32, 64, 64)
+    c = D.LinearFFTConvolver(np.ones((5, 5, 5), np.float32), (60, 70, 90),
+                             fft_shape=D.static_fft_shape((60, 70, 90), (5, 5, 5)))
+    assert c.fft_shape == (64, 80, 128)
+
+
 def test_conv_adjoint_identity(D):
     # <A x, y> == <x, A^T y>  (tests/test_composition.py:66-73, rtol 1e-4)
     rng = np.random.default_rng(3)

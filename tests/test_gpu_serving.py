@@ -41,30 +41,37 @@ def _mix():
     return jobs
 
 
-def _alone(job):
+def _alone(job, canvas="static"):
+    """The job through the public API on the canvas the server gives it."""
     import deconlib_b200.deconvolution as D
+    from deconlib_b200.serving import job_fft_shape
 
+    fft = job_fft_shape(job, canvas)
     if job.kind == "rl":
-        op = D.LinearFFTConvolver(job.psf, job.observed.shape)
+        op = D.LinearFFTConvolver(job.psf, job.observed.shape, fft_shape=fft)
         r = D.richardson_lucy_with_operator(job.observed, op, num_iter=job.num_iter,
                                             background=job.background)
     else:
         r = D.solve_pdhg_mlx(job.observed, job.psf, num_iter=job.num_iter,
-                             background=job.background, **job.options)
+                             background=job.background, fft_shape=fft, **job.options)
     return r.restored.cpu().numpy(), r.iterations
 
 
-@pytest.mark.parametrize("max_active,budget", [(3, 150 * 10**9), (8, 150 * 10**9), (8, 3 * 10**6)])
-def test_each_result_is_the_same_alone_and_in_the_mix(max_active, budget):
+@pytest.mark.parametrize("max_active,budget,canvas", [(3, 150 * 10**9, "static"),
+                                                      (8, 150 * 10**9, "static"),
+                                                      (8, 3 * 10**6, "static"),
+                                                      (8, 150 * 10**9, "reference")])
+def test_each_result_is_the_same_alone_and_in_the_mix(max_active, budget, canvas):
     from deconlib_b200.serving import DeconServer
 
     jobs = _mix()
-    rep = DeconServer(budget_bytes=budget, max_active=max_active, chunk=4).run(jobs, realtime=False)
+    rep = DeconServer(budget_bytes=budget, max_active=max_active, chunk=4, canvas=canvas).run(
+        jobs, realtime=False)
     assert [r.job_id for r in rep.results] == [j.job_id for j in jobs]
     if budget < 10**7:
         assert rep.peak_device_bytes <= budget
     for job, res in zip(jobs, rep.results):
-        ref, iters = _alone(job)
+        ref, iters = _alone(job, canvas)
         assert res.iterations == iters
         d = np.linalg.norm(res.restored - ref) / np.linalg.norm(ref)
         assert d <= 1e-6, (job.job_id, d, float(np.abs(res.restored - ref).max()))

@@ -64,6 +64,20 @@ def test_footprint_model_counts_plan_and_arrays():
     assert job_device_bytes(p) == plan + 4 * (6 * m + 11 * n + n)
 
 
+def test_static_canvas_policy_sizes_the_footprint():
+    from deconlib_b200.serving import job_fft_shape
+
+    j = _job(0, shape=(76, 362, 244))
+    assert job_fft_shape(j, "reference") == (160, 729, 500)
+    assert job_fft_shape(j, "static") == (160, 768, 512)
+    pitch = 272  # 512 / 2 + 1 rounded up to 16
+    plan = 8 * pitch * (160 * 768 + 76 * 362 + 76 * 768)
+    n = 76 * 362 * 244
+    assert job_device_bytes(j, "static") == plan + 4 * (5 * n + n)
+    with pytest.raises(ValueError):
+        job_fft_shape(j, "largest")
+
+
 def test_poisson_arrivals_are_seeded_with_the_requested_rate():
     a = poisson_arrivals(4000, 20.0, np.random.default_rng(5))
     b = poisson_arrivals(4000, 20.0, np.random.default_rng(5))
