@@ -34,7 +34,7 @@ import torch
 
 from . import _lib
 from .deconvolution._device import empty, stream, to_device
-from .deconvolution.linops import LinearFFTConvolver, _next_smooth_number
+from .deconvolution.linops import LinearFFTConvolver, _next_smooth_number, static_fft_shape
 
 __all__ = ["BatchTile", "plan_uneven_tiles", "fft_shape_candidates", "autotune_fft_shape",
            "autotune_schedule", "SCHEDULES", "tune_cache_path", "BatchedRL", "batched_tiled_rl"]
@@ -123,12 +123,14 @@ def fft_shape_candidates(signal_shape, kernel_shape, max_growth: float = 1.35) -
     """Canvases to try: the reference's 5-smooth minimum on every axis, and
     variants with 2^a 3^b or power-of-two lengths (other radix sequences;
     power-of-two y / z lengths <= 512 also select the TMA-pipelined column
-    kernels) where they grow an axis by <= max_growth.  Sorted by volume."""
+    kernels) where they grow an axis by <= max_growth, and the lengths of
+    ``static_fft_shape`` (compile-time radix sequences).  Sorted by volume."""
     m = [int(n) + int(k) - 1 for n, k in zip(signal_shape, kernel_shape)]
     s5 = [_next_smooth_number(v) for v in m]
+    st = static_fft_shape(signal_shape, kernel_shape)
     alt = []
-    for v, base in zip(m, s5):
-        opts = {base}
+    for v, base, sl in zip(m, s5, st):
+        opts = {base, sl}
         for f in (_next_23, _next_pow2):
             c = f(v)
             if c <= max_growth * base:
@@ -147,6 +149,7 @@ def fft_shape_candidates(signal_shape, kernel_shape, max_growth: float = 1.35) -
                 t[-2], t[-1] = cy, cx
                 cands.add(tuple(t))
     cands.add(tuple(max(a) for a in alt))
+    cands.add(tuple(st))
     return sorted(cands, key=lambda t: (int(np.prod(t)), t))
 
 
@@ -235,7 +238,12 @@ def autotune_schedule(signal_shape, psf, candidates: Optional[List[tuple]] = Non
     key = f"{dev}|{sig}|{kshape}"
     if key in _TUNED:
         return _TUNED[key][0], _TUNED[key][1]
-    cands = (candidates or fft_shape_candidates(sig, kshape))[:max_candidates]
+    cands = list((candidates or fft_shape_candidates(sig, kshape))[:max_candidates])
+    if candidates is None:
+        # always time the canvas of compile-time FFT lengths
+        st = tuple(static_fft_shape(sig, kshape))
+        if st not in cands:
+            cands[-1:] = [st]
     ckey = f"{dev}|canvases|{tuple(cands)}"
     if ckey in _TUNED:
         _TUNED[key] = _TUNED[ckey]
