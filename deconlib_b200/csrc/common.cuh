@@ -20,9 +20,13 @@ int fail(int code, const char* fmt, ...);
 #define DK_CUDA(call)                                                                     \
     do {                                                                                  \
         cudaError_t e_ = (call);                                                          \
-        if (e_ != cudaSuccess)                                                            \
+        if (e_ != cudaSuccess) {                                                          \
+            /* a refused call leaves its error as the thread's last error: */             \
+            /* clear it, or the next launch check would report it again */                \
+            (void)cudaGetLastError();                                                     \
             return ::dk::fail(DECON_ERR_CUDA, "%s failed: %s (%s:%d)", #call,             \
                               cudaGetErrorString(e_), __FILE__, __LINE__);                \
+        }                                                                                 \
     } while (0)
 
 // Count of kernels launched by the library (decon_launch_count), for the

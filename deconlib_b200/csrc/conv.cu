@@ -171,7 +171,11 @@ int kernel_prepare(void* fn, size_t smem, int nthr, int* per_sm) {
         if (per_sm) *per_sm = it->second;
         return DECON_OK;
     }
-    if (smem > 48 * 1024) {
+    // the 48 KB default covers static plus dynamic shared memory: opt in
+    // whenever their sum exceeds it
+    cudaFuncAttributes fa{};
+    DK_CUDA(cudaFuncGetAttributes(&fa, fn));
+    if (smem + fa.sharedSizeBytes > 48 * 1024) {
         size_t& cur = opt_in[std::make_pair(dev, fn)];
         if (smem > cur) {
             DK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -532,7 +532,9 @@ static int smem_prepare(const void* fn, size_t bytes, int* per_sm) {
     const auto key = std::make_pair(dev, fn);
     auto it = done.find(key);
     if (it == done.end()) {
-        if (bytes > 48 * 1024)
+        cudaFuncAttributes fa{};
+        DK_CUDA(cudaFuncGetAttributes(&fa, fn));
+        if (bytes + fa.sharedSizeBytes > 48 * 1024)  // the default covers static + dynamic
             DK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
         DK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      (int)cudaSharedmemCarveoutMaxShared));
