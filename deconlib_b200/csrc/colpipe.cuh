@@ -39,14 +39,7 @@ __host__ __device__ constexpr int pipe_slots(int L, bool lean) { return lean ? 2
 // LEAN: twiddles in shared memory instead of registers, one ring slot,
 // <= 128 registers, so two CTAs share an SM and one CTA's barriers and loads
 // overlap the other's arithmetic.
-// WCOL: the R threads of a column are R consecutive lanes (column t =
-// tid / R, butterfly j = tid % R), so the exchanges between the radix stages
-// stay inside a warp (__syncwarp instead of CTA barriers); between the
-// stages butterfly b's value v sits at row R v + ((b + v) mod R) of its
-// block, which keeps the writes and the reads free of bank conflicts under
-// the 128-byte swizzle.  Same loads, twiddles and float operations, so the
-// results equal the CTA-wide form bit for bit.
-template <int R, int SPLIT, int MODE, bool H16 = false, bool LEAN = false, bool WCOL = false>
+template <int R, int SPLIT, int MODE, bool H16 = false, bool LEAN = false>
 __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_constant__ PipeArgs a) {
     constexpr int LH = R * R;          // sub-transform length
     constexpr int L = LH * SPLIT;      // axis length
@@ -65,14 +58,7 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
     float2* base = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
     __shared__ uint64_t full[NS];
     __shared__ uint64_t obar;  // OTF1: the OTF buffer arrived
-    const int tid = threadIdx.x, t = WCOL ? tid / R : tid & 15, j = WCOL ? tid % R : tid >> 4;
-    // exchange barrier between radix stages (a column's threads share a warp under WCOL)
-    auto sync_x = [] {
-        if constexpr (WCOL) __syncwarp();
-        else __syncthreads();
-    };
-    // row of butterfly b's value v between the stages (block offset h LH added by the caller)
-    auto mid = [](int b, int v) { return WCOL ? R * v + ((b + v) & (R - 1)) : R * b + v; };
+    const int tid = threadIdx.x, t = tid & 15, j = tid >> 4;
     const int total = a.nouter * a.ntiles;
 
     // second-stage twiddles W_LH^(r j) = W_L^(SPLIT r j): registers, or (LEAN)
@@ -203,18 +189,18 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
         }
 #pragma unroll
         for (int h = 0; h < SPLIT; ++h) dft<R, D1>(v[h]);
-        sync_x();
+        __syncthreads();
 #pragma unroll
         for (int h = 0; h < SPLIT; ++h)
 #pragma unroll
-            for (int r = 0; r < R; ++r) buf[p1(h * LH + mid(j, r), t)] = v[h][r];
-        sync_x();
+            for (int r = 0; r < R; ++r) buf[p1(h * LH + j * R + r, t)] = v[h][r];
+        __syncthreads();
         // ---- stage 2 (Ns = R): reads and writes point j + R r ----
 #pragma unroll
         for (int h = 0; h < SPLIT; ++h) {
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                const float2 x = buf[p1(h * LH + mid(r, j), t)];
+                const float2 x = buf[p1(h * LH + j + R * r, t)];
                 v[h][r] = r == 0 ? x : (D1 < 0 ? cmul(x, w2(r)) : cmulc(x, w2(r)));
             }
             dft<R, D1>(v[h]);
@@ -247,24 +233,22 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
             // its reads before it with a proxy fence, then the barrier.
             // Without the fence the refill could land under a slow warp's
             // reads when other kernels share the SM.
+            if constexpr (OTF1) fence_proxy_async_smem();
+            __syncthreads();
             if constexpr (OTF1) {
-                fence_proxy_async_smem();
-                __syncthreads();
                 // every thread has read the OTF buffer: refill it for the next tile
                 if (tid == 0 && tile + (int)gridDim.x < total) issue_otf(tile + gridDim.x);
-            } else {
-                sync_x();
             }
 #pragma unroll
             for (int h = 0; h < SPLIT; ++h)
 #pragma unroll
-                for (int r = 0; r < R; ++r) buf[p1(h * LH + mid(j, r), t)] = v[h][r];
-            sync_x();
+                for (int r = 0; r < R; ++r) buf[p1(h * LH + j * R + r, t)] = v[h][r];
+            __syncthreads();
 #pragma unroll
             for (int h = 0; h < SPLIT; ++h) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    const float2 x = buf[p1(h * LH + mid(r, j), t)];
+                    const float2 x = buf[p1(h * LH + j + R * r, t)];
                     v[h][r] = r == 0 ? x : cmulc(x, w2(r));
                 }
                 dft<R, +1>(v[h]);
@@ -273,7 +257,7 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
         // ---- outputs in natural order ----
         if constexpr (MODE == COL_FWD) {
             // X[SPLIT m + h], m = j + R r
-            if constexpr (SPLIT == 2 || WCOL) sync_x();  // other threads still read rows h LH + m
+            if constexpr (SPLIT == 2) __syncthreads();  // other threads still read rows h LH + m
 #pragma unroll
             for (int h = 0; h < SPLIT; ++h)
 #pragma unroll
@@ -282,10 +266,8 @@ __global__ void __launch_bounds__(16 * R, LEAN ? 2 : 1) k_col_pipe(const __grid_
                     if (k < a.nout) buf[p1(k, t)] = v[h][r];
                 }
         } else {
-            // y[n] = y0[n] (+ W_L^-n y1[n]), n = j + R r; without WCOL this
-            // thread alone read rows n and LH + n, so no barrier is needed
-            // before writing (under WCOL the reads were the skewed rows)
-            if constexpr (WCOL) sync_x();
+            // y[n] = y0[n] (+ W_L^-n y1[n]), n = j + R r; this thread alone
+            // read rows n and LH + n, so no barrier is needed before writing.
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int n = j + R * r;

@@ -21,7 +21,6 @@
 #include <map>
 #include <mutex>
 #include <tuple>
-#include <type_traits>
 #include <vector>
 
 #include <algorithm>
@@ -483,46 +482,40 @@ bool encode_spectrum_map(CUtensorMap* map, const float2* base, int64_t pitch, in
 // Pipelined kernel for (L, mode, nin, nout), or nullptr.  R x R (SPLIT 1) for
 // L = 64, 256; the half-zero split (SPLIT 2) for L = 128, 512 when the
 // non-zero input / kept output fits in half the axis.
-// h16: the axial (OTF) modes read the FP16 OTF (mixed precision); lean: the
-// two-CTA axial form; wcol: warp-owned columns (k_col_pipe's WCOL).
-template <int RR, int SS, bool W>
-static void* pipe_for(int mode, bool h16, bool lean) {
-    switch (mode) {
-        case COL_FWD: return (void*)k_col_pipe<RR, SS, COL_FWD, false, false, W>;
-        case COL_INV: return (void*)k_col_pipe<RR, SS, COL_INV, false, false, W>;
-        case COL_OTF:
-            return h16 ? (lean ? (void*)k_col_pipe<RR, SS, COL_OTF, true, true, W>
-                               : (void*)k_col_pipe<RR, SS, COL_OTF, true, false, W>)
-                       : (lean ? (void*)k_col_pipe<RR, SS, COL_OTF, false, true, W>
-                               : (void*)k_col_pipe<RR, SS, COL_OTF, false, false, W>);
-        case COL_OTF_CONJ:
-            return h16 ? (lean ? (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, true, true, W>
-                               : (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, true, false, W>)
-                       : (lean ? (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, false, true, W>
-                               : (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, false, false, W>);
-        default: return nullptr;
-    }
-}
-
+// h16: the axial (OTF) modes read the FP16 OTF (mixed precision).
 static void* pick_pipe(int L, int mode, int nin, int nout, int* R, int* split, bool h16 = false,
-                       bool lean = false, bool wcol = false) {
+                       bool lean = false) {
     const bool otf = mode == COL_OTF || mode == COL_OTF_CONJ;
     const bool half_ok = (mode == COL_FWD && nin <= L / 2) || (mode == COL_INV && nout <= L / 2) ||
                          (otf && nin <= L / 2 && nout <= L / 2);
-    auto pick = [&](auto rr, auto ss) -> void* {
-        constexpr int RR = decltype(rr)::value, SS = decltype(ss)::value;
-        *R = RR;
-        *split = SS;
-        return wcol ? pipe_for<RR, SS, true>(mode, h16, lean) : pipe_for<RR, SS, false>(mode, h16, lean);
-    };
-    using I1 = std::integral_constant<int, 1>;
-    using I2 = std::integral_constant<int, 2>;
-    using I8 = std::integral_constant<int, 8>;
-    using I16 = std::integral_constant<int, 16>;
-    if (L == 256) return pick(I16{}, I1{});
-    if (L == 64) return pick(I8{}, I1{});
-    if (L == 128 && half_ok) return pick(I8{}, I2{});
-    if (L == 512 && half_ok && !otf) return pick(I16{}, I2{});
+#define DK_PIPE(RR, SS)                                                                          \
+    do {                                                                                         \
+        *R = RR;                                                                                 \
+        *split = SS;                                                                             \
+        switch (mode) {                                                                          \
+            case COL_FWD: return (void*)k_col_pipe<RR, SS, COL_FWD>;                             \
+            case COL_INV: return (void*)k_col_pipe<RR, SS, COL_INV>;                             \
+            case COL_OTF:                                                                        \
+                return h16 ? (lean ? (void*)k_col_pipe<RR, SS, COL_OTF, true, true>              \
+                                   : (void*)k_col_pipe<RR, SS, COL_OTF, true>)                  \
+                           : (lean ? (void*)k_col_pipe<RR, SS, COL_OTF, false, true>            \
+                                   : (void*)k_col_pipe<RR, SS, COL_OTF>);                       \
+            case COL_OTF_CONJ:                                                                   \
+                return h16 ? (lean ? (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, true, true>         \
+                                   : (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, true>)             \
+                           : (lean ? (void*)k_col_pipe<RR, SS, COL_OTF_CONJ, false, true>       \
+                                   : (void*)k_col_pipe<RR, SS, COL_OTF_CONJ>);                  \
+        }                                                                                        \
+    } while (0)
+    if (L == 256) DK_PIPE(16, 1);
+    if (L == 64) DK_PIPE(8, 1);
+    if (L == 128 && half_ok) DK_PIPE(8, 2);
+#undef DK_PIPE
+    if (L == 512 && half_ok && !otf) {
+        *R = 16;
+        *split = 2;
+        return mode == COL_FWD ? (void*)k_col_pipe<16, 2, COL_FWD> : (void*)k_col_pipe<16, 2, COL_INV>;
+    }
     return nullptr;
 }
 
@@ -539,10 +532,7 @@ static bool launch_col_pipe(const ConvPlan& p, const Axis& ax, int mode, const C
     const bool lean = otf_mode && (!h16 || p.tma_otf16) &&
                       (le ? le[0] == '1' : (ax.L == 256 && !(p.sched & DECON_SCHED_LEAN_OFF)));
     const bool no_pipe = getenv("DECON_NO_PIPE") || (p.sched & DECON_SCHED_NO_PIPE);
-    // warp-owned columns: DECON_PIPE_WCOL=1 / 0 overrides the default
-    const char* wc = getenv("DECON_PIPE_WCOL");
-    const bool wcol = wc ? wc[0] == '1' : false;
-    void* fn = no_pipe ? nullptr : pick_pipe(ax.L, mode, nin, nout, &R, &split, h16, lean, wcol);
+    void* fn = no_pipe ? nullptr : pick_pipe(ax.L, mode, nin, nout, &R, &split, h16, lean);
     if (!fn) return false;
     PipeArgs a;
     memset(&a, 0, sizeof(a));

@@ -339,29 +339,6 @@ def test_pdhg_fused_hessian_matches_operator_path(D, g32, norm):
     np.testing.assert_allclose(out[0][5], out[1][5], rtol=1e-6)
 
 
-@pytest.mark.parametrize("shape,fft,precision", [((64, 128, 128), (128, 256, 256), "fp32"),
-                                                 ((128, 256, 256), (256, 512, 512), "fp32"),
-                                                 ((20, 30, 40), (64, 64, 128), "fp32"),
-                                                 ((64, 128, 128), (256, 256, 256), "mixed")])
-def test_warp_owned_columns_bit_identical(D, monkeypatch, shape, fft, precision):
-    """DECON_PIPE_WCOL=1: the pipelined column kernel with each column's
-    threads in one warp (stage exchanges under __syncwarp, skewed rows
-    between the stages) gives the CTA-wide kernel's results bit for bit:
-    lengths 64 (8 x 8), 128 and 512 (half-zero split), 256 (lean axial,
-    FP32 and FP16 OTF)."""
-    rng = np.random.default_rng(12)
-    kshape = tuple(f - n + 1 for n, f in zip(shape, fft))
-    k = rng.random(kshape).astype(np.float32)
-    x = rng.random(shape).astype(np.float32)
-    c = D.LinearFFTConvolver(k, shape, fft_shape=fft, precision=precision)
-    outs = []
-    for v in ("0", "1"):
-        monkeypatch.setenv("DECON_PIPE_WCOL", v)
-        outs.append((c.forward(x).cpu().numpy(), c.adjoint(x).cpu().numpy()))
-    np.testing.assert_array_equal(outs[0][0], outs[1][0])
-    np.testing.assert_array_equal(outs[0][1], outs[1][1])
-
-
 def test_kernel_shared_memory_opt_in_never_shrinks(D):
     # The runtime-radix X-pass kernel serves every non-power-of-two length with
     # a dynamic shared-memory size that depends on the length: a plan that
