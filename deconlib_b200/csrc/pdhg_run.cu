@@ -291,7 +291,10 @@ int decon_pdhg_run(decon_pdhg_solver* s, int iterations, void* stream) {
             DK_TRY(decon_pdhg_hess_primal(h, xc, s->aty, s->Y2[0], xn, shp, s->r, st));
         }
         DK_TRY(pr_forward(s, xn, axn, st));
-        DK_TRY(decon_pdhg_hess_dk(h, axn, axc, s->m, xn, xc, shp, s->r, st));
+        // ||A dx||^2 and ||H dx||^2 as two sums (the split the two-stream
+        // Python driver uses, so both drivers give the same bits)
+        DK_TRY(decon_pdhg_dk(h, axn, axc, s->m, nullptr, 0, st));
+        DK_TRY(decon_pdhg_hess_dk(h, nullptr, nullptr, 0, xn, xc, shp, s->r, st));
         DK_TRY(decon_pdhg_step(h, st));
         if ((k + 1) % s->eval_interval == 0)
             DK_TRY(decon_pdhg_hess_loss(h, axn, s->data, s->bg, s->loss, s->m, xn, shp, s->r,
