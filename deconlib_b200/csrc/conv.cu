@@ -424,11 +424,22 @@ static void* pick_col_tma(int L) {
         case 128: return (void*)k_colfft_tma<128>;
         case 256: return (void*)k_colfft_tma<256>;
         case 512: return (void*)k_colfft_tma<512>;
+        case 80: return (void*)k_colfft_tma<80>;
+        case 96: return (void*)k_colfft_tma<96>;
+        case 160: return (void*)k_colfft_tma<160>;
+        case 192: return (void*)k_colfft_tma<192>;
+        case 240: return (void*)k_colfft_tma<240>;
         default: return nullptr;
     }
 }
 
-bool tma_length_ok(int L) { return L == 64 || L == 128 || L == 256 || L == 512; }
+// Lengths with a TMA column kernel: the powers of two up to 512, and the
+// other compile-time lengths up to 256 (one TMA box spans the whole line, so
+// no box reaches past the tile).
+bool tma_length_ok(int L) {
+    return L == 64 || L == 128 || L == 256 || L == 512 || L == 80 || L == 96 || L == 160 || L == 192 ||
+           L == 240;
+}
 
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
@@ -606,7 +617,7 @@ static int launch_col_tma(const ConvPlan& p, const Axis& ax, int mode, const CUt
     a.tw = ax.tw;
     a.tws = ax.tws;
     const int L = ax.L;
-    const int nthr = std::max(64, L / 2);
+    const int nthr = std::max(64, 16 * ((L + 31) / 32));  // 16 lines x the static path's threads per line
     const bool otf = mode == COL_OTF || mode == COL_OTF_CONJ;
     const size_t smem = 1024 + (size_t)L * 16 * sizeof(float2) * (otf ? 2 : 1);
     return launch(pick_col_tma(L), nouter * a.ntiles, nthr, smem, st, &a,

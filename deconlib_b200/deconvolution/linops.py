@@ -72,8 +72,13 @@ def static_fft_shape(signal_shape, kernel_shape) -> Tuple[int, ...]:
     Per axis the smallest length >= N + M - 1 in ``STATIC_FFT_LENGTHS`` (the
     last axis, transformed as packed complex pairs, twice such a length), when
     that grows the axis by at most 1/3 over ``fast_padded_shape``'s 5-smooth
-    length; otherwise the 5-smooth length.  A convolution's result does not
-    depend on the canvas beyond FP32 rounding."""
+    length; otherwise the 5-smooth length.  The axial (first) axis of a 3-D
+    canvas takes 64, 128 or 256 instead when that is at most twice the
+    length chosen so: those lengths run the TMA-pipelined axial kernels,
+    which measured faster per iteration on the B200 even on the larger canvas
+    (RL at 76x362x244: 1.43 ms on 256x768x512 vs 2.29 ms on 160x768x512).
+    A convolution's result does not depend on the canvas beyond FP32
+    rounding."""
     ref = fast_padded_shape(signal_shape, kernel_shape)
     nd = len(ref)
     out = []
@@ -82,6 +87,11 @@ def static_fft_shape(signal_shape, kernel_shape) -> Tuple[int, ...]:
         scale = 2 if ax == nd - 1 else 1
         c = next((scale * L for L in STATIC_FFT_LENGTHS if scale * L >= need), None)
         out.append(c if c is not None and 3 * c <= 4 * r else r)
+    if nd == 3:
+        need = max(int(signal_shape[0]) + int(kernel_shape[0]) - 1, int(kernel_shape[0]))
+        p = 1 << max(0, (need - 1).bit_length())
+        if p in (64, 128, 256) and p <= 2 * out[0]:
+            out[0] = p
     return tuple(out)
 
 

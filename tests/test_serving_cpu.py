@@ -69,9 +69,9 @@ def test_static_canvas_policy_sizes_the_footprint():
 
     j = _job(0, shape=(76, 362, 244))
     assert job_fft_shape(j, "reference") == (160, 729, 500)
-    assert job_fft_shape(j, "static") == (160, 768, 512)
+    assert job_fft_shape(j, "static") == (256, 768, 512)
     pitch = 272  # 512 / 2 + 1 rounded up to 16
-    plan = 8 * pitch * (160 * 768 + 76 * 362 + 76 * 768)
+    plan = 8 * pitch * (256 * 768 + 76 * 362 + 76 * 768)
     n = 76 * 362 * 244
     assert job_device_bytes(j, "static") == plan + 4 * (5 * n + n)
     with pytest.raises(ValueError):
