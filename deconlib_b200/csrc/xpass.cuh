@@ -319,7 +319,7 @@ __device__ __forceinline__ void epilogue(const XC2RArgs& a, int64_t i, float v, 
 }
 
 template <int EPI, int LS>
-__global__ void __launch_bounds__(LS > 0 ? kFftThreads : kDynThreads, LS > 0 ? 2 : 1) k_xc2r(XC2RArgs a) {
+__global__ void __launch_bounds__(LS > 0 ? kFftThreads : kDynThreads, LS > 0 ? (LS <= 256 ? 3 : 2) : 1) k_xc2r(XC2RArgs a) {
     extern __shared__ float2 sm[];
     __shared__ float2 nyq[32];    // X[M] of each row (even Fx)
     __shared__ int64_t obase[32];  // output index of x = 0 of each row (general path)
