@@ -318,8 +318,11 @@ __device__ __forceinline__ void epilogue(const XC2RArgs& a, int64_t i, float v, 
     }
 }
 
+// Three CTAs per SM below length 512 (80 registers, no spills; at 256 the
+// PDHG iteration measured 1.04-1.05 vs 1.06-1.07 ms with two); from 512 on
+// the compile-time lines per CTA need more registers, so two.
 template <int EPI, int LS>
-__global__ void __launch_bounds__(LS > 0 ? kFftThreads : kDynThreads, LS > 0 ? (LS <= 256 ? 3 : 2) : 1) k_xc2r(XC2RArgs a) {
+__global__ void __launch_bounds__(LS > 0 ? kFftThreads : kDynThreads, LS > 0 ? (LS < 512 ? 3 : 2) : 1) k_xc2r(XC2RArgs a) {
     extern __shared__ float2 sm[];
     __shared__ float2 nyq[32];    // X[M] of each row (even Fx)
     __shared__ int64_t obase[32];  // output index of x = 0 of each row (general path)
