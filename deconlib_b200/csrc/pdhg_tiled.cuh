@@ -376,11 +376,14 @@ __global__ void __launch_bounds__(256) k_hess_regloss_p(PdhgDev* s, const float*
 
 // H^T y2 over this CTA's tiles from staged planes: components 0, 3, 4 (read
 // at z -+ 1) in rings of three planes, components 1, 2, 5 (read in plane z
-// only) one plane each, a one-plane register prefetch.  body(i, lt) receives
-// the adjoint at interior voxel i (the float operations of hess_adj_gen).
-template <class Body>
-__device__ __forceinline__ void hess_adj_walk(const float* __restrict__ y2, const Dims& d, const W6& w,
-                                              const Body& body) {
+// only) one plane each, a one-plane register prefetch.  body(i, lt, cv)
+// receives the adjoint at interior voxel i (the float operations of
+// hess_adj_gen) and the NC centre operands cen[c][i], which are prefetched
+// into registers one plane ahead with the y2 halo values (a load issued in
+// the body would wait a full memory latency per plane).
+template <int NC, class Body>
+__device__ __forceinline__ void hess_adj_walk_c(const float* __restrict__ y2, const Dims& d, const W6& w,
+                                                const float* const* cen, const Body& body) {
     __shared__ float rz[3][3][kPL];  // components 0, 3, 4
     __shared__ float pz[3][kPL];     // components 1, 2, 5
     const int64_t n = d.nz * d.ny * d.nx, plane = d.ny * d.nx;
@@ -415,6 +418,7 @@ __device__ __forceinline__ void hess_adj_walk(const float* __restrict__ y2, cons
         st.store(rz[0][1], p0);
         st.store(rz[1][1], p3);
         st.store(rz[2][1], p4);
+        float cv[NC > 0 ? NC : 1], cn[NC > 0 ? NC : 1];
         {
             const int64_t zn = clampi(z0 + 1, d.nz);
             st.load(p0, c0, zn, plane);
@@ -423,8 +427,12 @@ __device__ __forceinline__ void hess_adj_walk(const float* __restrict__ y2, cons
             st.load(p1, c1, z0, plane);
             st.load(p2, c2, z0, plane);
             st.load(p5, c5, z0, plane);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) cn[c] = in ? __ldg(cen[c] + z0 * plane + ipl) : 0.f;
         }
         for (int64_t z = z0; z < z1; ++z) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) cv[c] = cn[c];
             const int sp = (int)((z - z0) % 3), sc = (int)((z - z0 + 1) % 3),
                       sn = (int)((z - z0 + 2) % 3);
             st.store(rz[0][sn], p0);
@@ -442,6 +450,8 @@ __device__ __forceinline__ void hess_adj_walk(const float* __restrict__ y2, cons
                 st.load(p1, c1, z + 1, plane);
                 st.load(p2, c2, z + 1, plane);
                 st.load(p5, c5, z + 1, plane);
+#pragma unroll
+                for (int c = 0; c < NC; ++c) cn[c] = in ? __ldg(cen[c] + (z + 1) * plane + ipl) : 0.f;
             }
             if (in) {
                 e.zlo = z == 0 ? -1.f : 1.f;
@@ -449,11 +459,17 @@ __device__ __forceinline__ void hess_adj_walk(const float* __restrict__ y2, cons
                 const float lt = hess_adj_smem(rz[0][sp], rz[0][sc], rz[0][sn], pz[0], pz[1],
                                                rz[1][sp], rz[1][sn], rz[2][sp], rz[2][sn], pz[2],
                                                ty + 1, tx + 1, e, w.w);
-                body(z * plane + ipl, lt);
+                body(z * plane + ipl, lt, cv);
             }
             __syncthreads();
         }
     }
+}
+
+template <class Body>
+__device__ __forceinline__ void hess_adj_walk(const float* __restrict__ y2, const Dims& d, const W6& w,
+                                              const Body& body) {
+    hess_adj_walk_c<0>(y2, d, w, nullptr, [&](int64_t i, float lt, const float*) { body(i, lt); });
 }
 
 // x_new = max(0, x - tau (A^T y1 + H^T y2)) and its FP64 sums.
@@ -465,9 +481,10 @@ __global__ void __launch_bounds__(256) k_hess_primal_t(PdhgDev* s, const float* 
     if (s->stop) return;
     const float tau = (float)s->tau;
     double dx2 = 0.0, xc2 = 0.0, xn2 = 0.0;
-    hess_adj_walk(y2, d, w, [&](int64_t i, float lt) {
-        const float a = xc[i];
-        const float gr = __fadd_rn(aty[i], lt);
+    const float* cen[2] = {xc, aty};
+    hess_adj_walk_c<2>(y2, d, w, cen, [&](int64_t i, float lt, const float* cv) {
+        const float a = cv[0];
+        const float gr = __fadd_rn(cv[1], lt);
         const float v = primal_of(a, tau, gr);
         xn[i] = v;
         const float dd = v - a;
