@@ -910,7 +910,7 @@ def run_ours(args, ws, rank, local):
         "iteration_model": {
             "bytes": pdhg_model_bytes(OBJ, DATA, conv.fft_shape),
             "hbm_frac": pdhg_model_bytes(OBJ, DATA, conv.fft_shape) / (ms / K / 1e3) / 1e9 / hbm,
-            "note": "SURVEY minimal-byte model of one PDHG iteration (FP32 spectra) / ms_per_step"},
+            "note": "minimal-byte model of one PDHG iteration (X and Y transforms fused, FP32 spectra) / ms_per_step"},
         "roofline": {
             "bound": "hbm",
             "kernel": ("k_yz<512,256> fused Y FFT / axial FFT x OTF x IFFT / Y IFFT, one 8-CTA "
