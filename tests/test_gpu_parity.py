@@ -286,7 +286,7 @@ def test_column_pass_variants_agree(D, monkeypatch, shape, fft):
     # The pipelined column kernel (R x R Stockham, half-zero split for 128 /
     # 512), the one-tile TMA kernel (DECON_NO_PIPE) and the plain-load kernel
     # (DECON_NO_TMA) compute the same transforms with different factorings;
-    # so does the fused Y / axial pass (the default where it applies);
+    # so does the fused Y / axial pass (opt-in, DECON_YZ=1);
     # DECON_PIPE_LEAN selects the two-CTA axial kernel (twiddles in shared
     # memory, one ring slot) or the one-CTA kernel (same arithmetic).
     rng = np.random.default_rng(11)
