@@ -19,7 +19,10 @@ torch = pytest.importorskip("torch")
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(1, 9, 40), (2, 9, 33), (17, 10, 35), (33, 16, 64), (40, 70, 90), (5, 1, 1), (3, 20, 1)]
+SHAPES = [(1, 9, 40), (2, 9, 33), (17, 10, 35), (33, 16, 64), (40, 70, 90), (5, 1, 1), (3, 20, 1),
+          # partial x / y tiles whose x extent is a multiple of 4, one row,
+          # four columns
+          (17, 10, 36), (40, 70, 92), (5, 1, 4), (3, 20, 4)]
 
 
 @pytest.fixture(scope="module")
@@ -131,3 +134,4 @@ def test_pdhg_two_stream_schedule_bit_identical(monkeypatch):
     np.testing.assert_array_equal(out[0].restored.cpu().numpy(), out[1].restored.cpu().numpy())
     assert out[0].tau_history == out[1].tau_history
     assert out[0].sigma_history == out[1].sigma_history
+
