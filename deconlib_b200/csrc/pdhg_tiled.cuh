@@ -381,98 +381,136 @@ __global__ void __launch_bounds__(256) k_hess_regloss_p(PdhgDev* s, const float*
 // hess_adj_gen) and the NC centre operands cen[c][i], which are prefetched
 // into registers one plane ahead with the y2 halo values (a load issued in
 // the body would wait a full memory latency per plane).
-template <int NC, class Body>
+//
+// The walk is bound by instruction issue, so its index arithmetic is kept
+// lean: IDX is the type of element offsets (uint32_t when 6 n < 2^32, which
+// the launchers check, else int64_t), every per-tile quantity is set once
+// per tile, plane offsets advance by additions and the three ring slots
+// rotate instead of being recomputed modulo 3.
+template <class IDX, int NC, class Body>
 __device__ __forceinline__ void hess_adj_walk_c(const float* __restrict__ y2, const Dims& d, const W6& w,
                                                 const float* const* cen, const Body& body) {
     __shared__ float rz[3][3][kPL];  // components 0, 3, 4
     __shared__ float pz[3][kPL];     // components 1, 2, 5
-    const int64_t n = d.nz * d.ny * d.nx, plane = d.ny * d.nx;
+    const IDX n = (IDX)(d.nz * d.ny * d.nx), plane = (IDX)(d.ny * d.nx);
+    const int nz = (int)d.nz;
     const TileGeo g(d);
-    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-    auto comp = [&](int c) { return [=](int64_t i) -> float { return __ldg(y2 + c * n + i); }; };
-    const auto c0 = comp(0), c1 = comp(1), c2 = comp(2), c3 = comp(3), c4 = comp(4), c5 = comp(5);
+    const int tid = threadIdx.x, tx = tid % kTX, ty = tid / kTX;
+    // this thread's two halo-window slots (the second exists for tid < kPL - 256)
+    const int q1 = tid + 256;
+    const bool ok1 = q1 < kPL;
+    const int ly0 = tid / kHX, lx0 = tid - ly0 * kHX, ly1 = q1 / kHX, lx1 = q1 - ly1 * kHX;
+    const float* const y2c1 = y2 + n;
+    const float* const y2c2 = y2 + 2 * n;
+    const float* const y2c3 = y2 + 3 * n;
+    const float* const y2c4 = y2 + 4 * n;
+    const float* const y2c5 = y2 + 5 * n;
     for (int64_t tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
         const int64_t bx = tile % g.ntx, r = tile / g.ntx, by = r % g.nty, bz = r / g.nty;
-        const int64_t x0 = bx * kTX, y0 = by * kTY, z0 = bz * kZChunk;
-        const int64_t z1 = min(z0 + kZChunk, d.nz);
+        const int64_t x0 = bx * kTX, y0 = by * kTY;
+        const int z0 = (int)(bz * kZChunk);
+        const int z1 = z0 + kZChunk < nz ? z0 + kZChunk : nz;
         const int64_t x = x0 + tx, y = y0 + ty;
         const bool in = x < d.nx && y < d.ny;
-        const int64_t ipl = y * d.nx + x;
+        const IDX ipl = in ? (IDX)(y * d.nx + x) : (IDX)0;
         Edge e;
         e.ylo = y == 0 ? -1.f : 1.f;
         e.yhi = y == d.ny - 1 ? -1.f : 1.f;
         e.xlo = x == 0 ? -1.f : 1.f;
         e.xhi = x == d.nx - 1 ? -1.f : 1.f;
-        const StageSlots st(x0, y0, d);
+        const IDX off0 = (IDX)(clampi(y0 - 1 + ly0, d.ny) * d.nx + clampi(x0 - 1 + lx0, d.nx));
+        const IDX off1 = ok1 ? (IDX)(clampi(y0 - 1 + ly1, d.ny) * d.nx + clampi(x0 - 1 + lx1, d.nx)) : (IDX)0;
+        // the two slots' values of one component base at plane offset zo
+        auto ld = [&](const float* cb, IDX zo, float v[2]) {
+            v[0] = __ldg(cb + (zo + off0));
+            v[1] = ok1 ? __ldg(cb + (zo + off1)) : 0.f;
+        };
+        auto st = [&](float* pl, const float v[2]) {
+            pl[tid] = v[0];
+            if (ok1) pl[q1] = v[1];
+        };
         float p0[2], p3[2], p4[2], p1[2], p2[2], p5[2];
-        const int64_t zb = clampi(z0 - 1, d.nz);
-        st.load(p0, c0, zb, plane);
-        st.load(p3, c3, zb, plane);
-        st.load(p4, c4, zb, plane);
-        st.store(rz[0][0], p0);
-        st.store(rz[1][0], p3);
-        st.store(rz[2][0], p4);
-        st.load(p0, c0, z0, plane);
-        st.load(p3, c3, z0, plane);
-        st.load(p4, c4, z0, plane);
-        st.store(rz[0][1], p0);
-        st.store(rz[1][1], p3);
-        st.store(rz[2][1], p4);
-        float cv[NC > 0 ? NC : 1], cn[NC > 0 ? NC : 1];
         {
-            const int64_t zn = clampi(z0 + 1, d.nz);
-            st.load(p0, c0, zn, plane);
-            st.load(p3, c3, zn, plane);
-            st.load(p4, c4, zn, plane);
-            st.load(p1, c1, z0, plane);
-            st.load(p2, c2, z0, plane);
-            st.load(p5, c5, z0, plane);
-#pragma unroll
-            for (int c = 0; c < NC; ++c) cn[c] = in ? __ldg(cen[c] + z0 * plane + ipl) : 0.f;
+            const IDX zb = (IDX)(z0 > 0 ? z0 - 1 : 0) * plane;
+            ld(y2, zb, p0);
+            ld(y2c3, zb, p3);
+            ld(y2c4, zb, p4);
+            st(rz[0][0], p0);
+            st(rz[1][0], p3);
+            st(rz[2][0], p4);
+            const IDX zc = (IDX)z0 * plane;
+            ld(y2, zc, p0);
+            ld(y2c3, zc, p3);
+            ld(y2c4, zc, p4);
+            st(rz[0][1], p0);
+            st(rz[1][1], p3);
+            st(rz[2][1], p4);
         }
-        for (int64_t z = z0; z < z1; ++z) {
+        float cv[NC > 0 ? NC : 1], cn[NC > 0 ? NC : 1];
+        IDX zo = (IDX)z0 * plane;  // offset of plane z
+        {
+            const IDX zn = (IDX)(z0 + 1 < nz ? z0 + 1 : nz - 1) * plane;
+            ld(y2, zn, p0);
+            ld(y2c3, zn, p3);
+            ld(y2c4, zn, p4);
+            ld(y2c1, zo, p1);
+            ld(y2c2, zo, p2);
+            ld(y2c5, zo, p5);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) cn[c] = in ? __ldg(cen[c] + (zo + ipl)) : 0.f;
+        }
+        int sp = 0, sc = 1, sn = 2;  // ring slots of planes z - 1, z, z + 1
+        for (int z = z0; z < z1; ++z) {
 #pragma unroll
             for (int c = 0; c < NC; ++c) cv[c] = cn[c];
-            const int sp = (int)((z - z0) % 3), sc = (int)((z - z0 + 1) % 3),
-                      sn = (int)((z - z0 + 2) % 3);
-            st.store(rz[0][sn], p0);
-            st.store(rz[1][sn], p3);
-            st.store(rz[2][sn], p4);
-            st.store(pz[0], p1);
-            st.store(pz[1], p2);
-            st.store(pz[2], p5);
+            st(rz[0][sn], p0);
+            st(rz[1][sn], p3);
+            st(rz[2][sn], p4);
+            st(pz[0], p1);
+            st(pz[1], p2);
+            st(pz[2], p5);
             __syncthreads();
+            const IDX zi = zo;  // plane z
+            zo += plane;        // plane z + 1
             if (z + 1 < z1) {
-                const int64_t zn = clampi(z + 2, d.nz);
-                st.load(p0, c0, zn, plane);
-                st.load(p3, c3, zn, plane);
-                st.load(p4, c4, zn, plane);
-                st.load(p1, c1, z + 1, plane);
-                st.load(p2, c2, z + 1, plane);
-                st.load(p5, c5, z + 1, plane);
+                const IDX zn = z + 2 < nz ? zo + plane : zo;  // clamp(z + 2)
+                ld(y2, zn, p0);
+                ld(y2c3, zn, p3);
+                ld(y2c4, zn, p4);
+                ld(y2c1, zo, p1);
+                ld(y2c2, zo, p2);
+                ld(y2c5, zo, p5);
 #pragma unroll
-                for (int c = 0; c < NC; ++c) cn[c] = in ? __ldg(cen[c] + (z + 1) * plane + ipl) : 0.f;
+                for (int c = 0; c < NC; ++c) cn[c] = in ? __ldg(cen[c] + (zo + ipl)) : 0.f;
             }
             if (in) {
                 e.zlo = z == 0 ? -1.f : 1.f;
-                e.zhi = z == d.nz - 1 ? -1.f : 1.f;
+                e.zhi = z == nz - 1 ? -1.f : 1.f;
                 const float lt = hess_adj_smem(rz[0][sp], rz[0][sc], rz[0][sn], pz[0], pz[1],
                                                rz[1][sp], rz[1][sn], rz[2][sp], rz[2][sn], pz[2],
                                                ty + 1, tx + 1, e, w.w);
-                body(z * plane + ipl, lt, cv);
+                body(zi + ipl, lt, cv);
             }
             __syncthreads();
+            const int t = sp;
+            sp = sc;
+            sc = sn;
+            sn = t;
         }
     }
 }
 
-template <class Body>
+template <class IDX, class Body>
 __device__ __forceinline__ void hess_adj_walk(const float* __restrict__ y2, const Dims& d, const W6& w,
                                               const Body& body) {
-    hess_adj_walk_c<0>(y2, d, w, nullptr, [&](int64_t i, float lt, const float*) { body(i, lt); });
+    hess_adj_walk_c<IDX, 0>(y2, d, w, nullptr, [&](IDX i, float lt, const float*) { body(i, lt); });
 }
 
+// Element offsets fit 32 bits when all six components do.
+inline bool offsets_fit_u32(const Dims& d) { return 6 * d.nz * d.ny * d.nx < (int64_t(1) << 32); }
+
 // x_new = max(0, x - tau (A^T y1 + H^T y2)) and its FP64 sums.
+template <class IDX>
 __global__ void __launch_bounds__(256) k_hess_primal_t(PdhgDev* s, const float* __restrict__ xc,
                                                        const float* __restrict__ aty,
                                                        const float* __restrict__ y2,
@@ -482,7 +520,7 @@ __global__ void __launch_bounds__(256) k_hess_primal_t(PdhgDev* s, const float* 
     const float tau = (float)s->tau;
     double dx2 = 0.0, xc2 = 0.0, xn2 = 0.0;
     const float* cen[2] = {xc, aty};
-    hess_adj_walk_c<2>(y2, d, w, cen, [&](int64_t i, float lt, const float* cv) {
+    hess_adj_walk_c<IDX, 2>(y2, d, w, cen, [&](IDX i, float lt, const float* cv) {
         const float a = cv[0];
         const float gr = __fadd_rn(cv[1], lt);
         const float v = primal_of(a, tau, gr);
@@ -499,9 +537,10 @@ __global__ void __launch_bounds__(256) k_hess_primal_t(PdhgDev* s, const float* 
 
 // Hessian3D.adjoint of six stored components on the staged tile walk:
 // bit-identical to the per-voxel global-memory form (hess_adj_gen).
+template <class IDX>
 __global__ void __launch_bounds__(256) k_hessian_adj_t(const float* __restrict__ hw, float* __restrict__ out,
                                                        Dims d, W6 w) {
-    hess_adj_walk(hw, d, w, [&](int64_t i, float lt) { out[i] = lt; });
+    hess_adj_walk<IDX>(hw, d, w, [&](IDX i, float lt) { out[i] = lt; });
 }
 
 

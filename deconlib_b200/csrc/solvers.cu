@@ -512,7 +512,10 @@ __global__ void k_clamp_min(const float* __restrict__ a, float lo, float* __rest
 
 int hess_adjoint_tiled(const float* hw, float* out, const Dims& d, const W6& w, cudaStream_t st) {
     const int64_t grid = std::min<int64_t>(TileGeo(d).ntiles, (int64_t)sm_count() * 4);
-    k_hessian_adj_t<<<(unsigned)std::max<int64_t>(grid, 1), 256, 0, st>>>(hw, out, d, w);
+    if (offsets_fit_u32(d))
+        k_hessian_adj_t<uint32_t><<<(unsigned)std::max<int64_t>(grid, 1), 256, 0, st>>>(hw, out, d, w);
+    else
+        k_hessian_adj_t<int64_t><<<(unsigned)std::max<int64_t>(grid, 1), 256, 0, st>>>(hw, out, d, w);
     DK_LAUNCHED();
     return DECON_OK;
 }
@@ -748,8 +751,13 @@ int decon_pdhg_hess_primal(decon_pdhg* h, const float* xc, const float* aty, con
     if (!h || !xc || !aty || !y2 || !xn || !shape) return fail(DECON_ERR_NULL, "null pointer");
     W6 w;
     hessian_weights(r, w.w);
-    k_hess_primal_t<<<kPdhgGrid, 256, 0, as_stream(stream)>>>(
-        h->dev, xc, aty, y2, xn, Dims{shape[0], shape[1], shape[2]}, w, kSlotDx2, kSlotXc2, kSlotXn2);
+    const Dims d{shape[0], shape[1], shape[2]};
+    if (offsets_fit_u32(d))
+        k_hess_primal_t<uint32_t><<<kPdhgGrid, 256, 0, as_stream(stream)>>>(h->dev, xc, aty, y2, xn, d, w, kSlotDx2,
+                                                                           kSlotXc2, kSlotXn2);
+    else
+        k_hess_primal_t<int64_t><<<kPdhgGrid, 256, 0, as_stream(stream)>>>(h->dev, xc, aty, y2, xn, d, w, kSlotDx2,
+                                                                          kSlotXc2, kSlotXn2);
     DK_LAUNCHED();
     return DECON_OK;
 }
