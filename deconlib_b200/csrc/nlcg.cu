@@ -329,15 +329,16 @@ struct Fields3 {
     float a, b, c;
 };
 
+template <class IDX>
 __global__ void __launch_bounds__(256) k_nlcg_hess_gram(const float* __restrict__ f,
                                                         const float* __restrict__ sd,
                                                         const float* __restrict__ dd, Dims d, W6 w,
                                                         double* part, NlcgDev* dev) {
     double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    hess_zwalk<3>(
-        d, w, [&](int64_t i) { return Fields3{__ldg(f + i), __ldg(sd + i), __ldg(dd + i)}; },
+    hess_zwalk<IDX, 3>(
+        d, w, [&](IDX i) { return Fields3{__ldg(f + i), __ldg(sd + i), __ldg(dd + i)}; },
         [](const Fields3& r, int k) { return k == 0 ? r.a : (k == 1 ? r.b : r.c); },
-        [&](int64_t, const float (*h)[6]) {
+        [&](IDX, const float (*h)[6]) {
             // the six-component products of one voxel in FP32, the sum over
             // voxels in FP64
             float p[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -357,12 +358,13 @@ __global__ void __launch_bounds__(256) k_nlcg_hess_gram(const float* __restrict_
     fold_last<6>(v, part, &dev->ticket, dev->gram);
 }
 
+template <class IDX>
 __global__ void __launch_bounds__(256) k_nlcg_hess_energy(const float* __restrict__ f, Dims d, W6 w,
                                                           double* part, NlcgDev* dev) {
     double v[1] = {0.0};
-    hess_zwalk<1>(
-        d, w, [&](int64_t i) { return __ldg(f + i); }, [](const float& r, int) { return r; },
-        [&](int64_t, const float (*h)[6]) {
+    hess_zwalk<IDX, 1>(
+        d, w, [&](IDX i) { return __ldg(f + i); }, [](const float& r, int) { return r; },
+        [&](IDX, const float (*h)[6]) {
             float p = 0.f;
 #pragma unroll
             for (int q = 0; q < 6; ++q) p = fmaf(h[0][q], h[0][q], p);
@@ -554,8 +556,12 @@ int decon_nlcg_hess_gram(decon_nlcg* h, const float* f, const float* sd, const f
     const Dims d{shape[0], shape[1], shape[2]};
     W6 w;
     hessian_weights(r, w.w);
-    k_nlcg_hess_gram<<<hess_grid(d, (const void*)k_nlcg_hess_gram), 256, 0, as_stream(stream)>>>(
-        f, sd, dd, d, w, h->part, h->dev);
+    if (offsets_fit_u32(d))
+        k_nlcg_hess_gram<uint32_t><<<hess_grid(d, (const void*)k_nlcg_hess_gram<uint32_t>), 256, 0, as_stream(stream)>>>(
+            f, sd, dd, d, w, h->part, h->dev);
+    else
+        k_nlcg_hess_gram<int64_t><<<hess_grid(d, (const void*)k_nlcg_hess_gram<int64_t>), 256, 0, as_stream(stream)>>>(
+            f, sd, dd, d, w, h->part, h->dev);
     DK_LAUNCHED();
     return DECON_OK;
 }
@@ -566,8 +572,12 @@ int decon_nlcg_hess_energy(decon_nlcg* h, const float* f, const int64_t shape[3]
     const Dims d{shape[0], shape[1], shape[2]};
     W6 w;
     hessian_weights(r, w.w);
-    k_nlcg_hess_energy<<<hess_grid(d, (const void*)k_nlcg_hess_energy), 256, 0, as_stream(stream)>>>(
-        f, d, w, h->part, h->dev);
+    if (offsets_fit_u32(d))
+        k_nlcg_hess_energy<uint32_t><<<hess_grid(d, (const void*)k_nlcg_hess_energy<uint32_t>), 256, 0,
+                                       as_stream(stream)>>>(f, d, w, h->part, h->dev);
+    else
+        k_nlcg_hess_energy<int64_t><<<hess_grid(d, (const void*)k_nlcg_hess_energy<int64_t>), 256, 0,
+                                      as_stream(stream)>>>(f, d, w, h->part, h->dev);
     DK_LAUNCHED();
     return DECON_OK;
 }

@@ -157,12 +157,13 @@ struct Vol {
 // tile instead of once per tap and the outputs leave in rows of 32 (on the
 // B200 57 vs 107 us for a per-voxel global-memory kernel at 128x256x256,
 // bit-identical results).
+template <class IDX>
 __global__ void __launch_bounds__(256) k_hessian_fwd_z(const float* __restrict__ x, float* __restrict__ h,
                                                        Dims d, W6 w) {
-    const int64_t n = d.nz * d.ny * d.nx;
-    hess_zwalk<1>(
-        d, w, [&](int64_t i) { return __ldg(x + i); }, [](const float& r, int) { return r; },
-        [&](int64_t i, const float (*hv)[6]) {
+    const IDX n = (IDX)(d.nz * d.ny * d.nx);
+    hess_zwalk<IDX, 1>(
+        d, w, [&](IDX i) { return __ldg(x + i); }, [](const float& r, int) { return r; },
+        [&](IDX i, const float (*hv)[6]) {
 #pragma unroll
             for (int c = 0; c < 6; ++c) h[c * n + i] = hv[0][c];
         });
@@ -319,7 +320,10 @@ int decon_hessian3d_forward(const float* x, float* h, const int64_t shape[3], fl
     if (n <= 0) return DECON_OK;
     const Dims d{shape[0], shape[1], shape[2]};
     const int64_t grid = std::min<int64_t>(TileGeo(d).ntiles, (int64_t)sm_count() * 8);
-    k_hessian_fwd_z<<<(unsigned)std::max<int64_t>(grid, 1), 256, 0, as_stream(stream)>>>(x, h, d, w);
+    if (offsets_fit_u32(d))
+        k_hessian_fwd_z<uint32_t><<<(unsigned)std::max<int64_t>(grid, 1), 256, 0, as_stream(stream)>>>(x, h, d, w);
+    else
+        k_hessian_fwd_z<int64_t><<<(unsigned)std::max<int64_t>(grid, 1), 256, 0, as_stream(stream)>>>(x, h, d, w);
     DK_LAUNCHED();
     return DECON_OK;
 }

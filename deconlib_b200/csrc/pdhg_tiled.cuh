@@ -320,6 +320,7 @@ __device__ __forceinline__ void put_slot(PdhgDev* s, int slot, double v) {
 }
 
 // ||A x_new - A x||^2 and ||H (x_new - x)||^2 (z axis walked in registers).
+template <class IDX>
 __global__ void __launch_bounds__(256) k_hess_dk_r(PdhgDev* s, const float* __restrict__ axn,
                                                    const float* __restrict__ axc, int64_t m,
                                                    const float* __restrict__ xn,
@@ -332,10 +333,10 @@ __global__ void __launch_bounds__(256) k_hess_dk_r(PdhgDev* s, const float* __re
         const double dd = (double)axn[i] - (double)axc[i];
         a2 += dd * dd;
     }
-    hess_zwalk<1>(
-        d, w, [&](int64_t i) { return make_float2(__ldg(xn + i), __ldg(xc + i)); },
+    hess_zwalk<IDX, 1>(
+        d, w, [&](IDX i) { return make_float2(__ldg(xn + i), __ldg(xc + i)); },
         [](const float2& r, int) { return r.x - r.y; },
-        [&](int64_t, const float (*h)[6]) {
+        [&](IDX, const float (*h)[6]) {
             // the six squares of one voxel in FP32, the sum over voxels in FP64
             float v = 0.f;
 #pragma unroll
@@ -505,9 +506,6 @@ __device__ __forceinline__ void hess_adj_walk(const float* __restrict__ y2, cons
                                               const Body& body) {
     hess_adj_walk_c<IDX, 0>(y2, d, w, nullptr, [&](IDX i, float lt, const float*) { body(i, lt); });
 }
-
-// Element offsets fit 32 bits when all six components do.
-inline bool offsets_fit_u32(const Dims& d) { return 6 * d.nz * d.ny * d.nx < (int64_t(1) << 32); }
 
 // x_new = max(0, x - tau (A^T y1 + H^T y2)) and its FP64 sums.
 template <class IDX>

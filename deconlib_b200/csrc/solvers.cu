@@ -792,13 +792,18 @@ int decon_pdhg_hess_dk(decon_pdhg* h, const float* ax_new, const float* ax_cur, 
     hessian_weights(r, w.w);
     int per_sm = 1;
     const Dims d{shape[0], shape[1], shape[2]};
-    DK_TRY(smem_prepare((const void*)k_hess_dk_r, 0, &per_sm));
+    const bool u32 = offsets_fit_u32(d);
+    DK_TRY(smem_prepare(u32 ? (const void*)k_hess_dk_r<uint32_t> : (const void*)k_hess_dk_r<int64_t>, 0, &per_sm));
     const int grid = (int)std::min<int64_t>(kPdhgGrid, std::max<int64_t>(TileGeo(d).ntiles, 1));
     // ax_new == NULL: only ||H dx||^2 (the data term's ||A dx||^2 then comes
     // from decon_pdhg_dk with l_dx = NULL); the empty A sum goes to the spare
     // slot 7 so that the two kernels may run concurrently
-    k_hess_dk_r<<<grid, 256, 0, as_stream(stream)>>>(h->dev, ax_new, ax_cur, ax_new ? m : 0, xn, xc, d,
-                                                    w, ax_new ? kSlotDA2 : kPdhgSlots - 1, kSlotDL2);
+    if (u32)
+        k_hess_dk_r<uint32_t><<<grid, 256, 0, as_stream(stream)>>>(h->dev, ax_new, ax_cur, ax_new ? m : 0, xn, xc,
+                                                                  d, w, ax_new ? kSlotDA2 : kPdhgSlots - 1, kSlotDL2);
+    else
+        k_hess_dk_r<int64_t><<<grid, 256, 0, as_stream(stream)>>>(h->dev, ax_new, ax_cur, ax_new ? m : 0, xn, xc,
+                                                                 d, w, ax_new ? kSlotDA2 : kPdhgSlots - 1, kSlotDL2);
     DK_LAUNCHED();
     return DECON_OK;
 }

@@ -68,38 +68,53 @@ struct StageSlots {
 //   val(r, k)    -> float: field k from them
 //   body(i, h)   voxel i of the tile interior, h[k][0..6) the weighted
 //                components of field k
-template <int NF, class Raw, class Val, class Body>
+// IDX is the type of element offsets (uint32_t when every offset the
+// kernel forms fits 32 bits, which the launchers check with
+// offsets_fit_u32, else int64_t); per-tile quantities are set once per
+// tile and plane offsets advance by additions, since the walk is bound by
+// instruction issue.
+template <class IDX, int NF, class Raw, class Val, class Body>
 __device__ __forceinline__ void hess_zwalk(const Dims& d, const W6& w, const Raw& raw, const Val& val,
                                            const Body& body) {
-    using RawT = decltype(raw(int64_t(0)));
+    using RawT = decltype(raw(IDX(0)));
     __shared__ float sp[2][NF][kPL], sh[2][NF][kPL], sz[2][NF][kPL];
-    const int64_t plane = d.ny * d.nx;
+    const IDX plane = (IDX)(d.ny * d.nx);
+    const int nz = (int)d.nz;
     const TileGeo g(d);
-    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+    const int tid = threadIdx.x, tx = tid % kTX, ty = tid / kTX;
     const int c = (ty + 1) * kHX + (tx + 1);
     const int n = c - kHX, so = c + kHX, wv = c - 1, e = c + 1;
+    // this thread's two halo-window slots (the second exists for tid < kPL - 256)
+    const int q1 = tid + 256;
+    const bool ok1 = q1 < kPL;
+    const int ly0 = tid / kHX, lx0 = tid - ly0 * kHX, ly1 = q1 / kHX, lx1 = q1 - ly1 * kHX;
     int buf = 0;
     for (int64_t tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
         const int64_t bx = tile % g.ntx, r = tile / g.ntx, by = r % g.nty, bz = r / g.nty;
-        const int64_t x0 = bx * kTX, y0 = by * kTY, z0 = bz * kZChunk;
-        const int64_t z1 = min(z0 + kZChunk, d.nz);
+        const int64_t x0 = bx * kTX, y0 = by * kTY;
+        const int z0 = (int)(bz * kZChunk);
+        const int z1 = z0 + kZChunk < nz ? z0 + kZChunk : nz;
         const bool in = x0 + tx < d.nx && y0 + ty < d.ny;
-        const int64_t ipl = (y0 + ty) * d.nx + (x0 + tx);
-        const StageSlots st(x0, y0, d);
+        const IDX ipl = in ? (IDX)((y0 + ty) * d.nx + (x0 + tx)) : (IDX)0;
+        const IDX off[2] = {(IDX)(clampi(y0 - 1 + ly0, d.ny) * d.nx + clampi(x0 - 1 + lx0, d.nx)),
+                            ok1 ? (IDX)(clampi(y0 - 1 + ly1, d.ny) * d.nx + clampi(x0 - 1 + lx1, d.nx)) : (IDX)0};
+        const int q[2] = {tid, q1};
+        const bool ok[2] = {true, ok1};
         float vm[2][NF], vc[2][NF];
         RawT rq[2];
+        IDX zo = (IDX)z0 * plane;  // offset of plane z
         {
-            const int64_t zb = clampi(z0 - 1, d.nz), zq = clampi(z0 + 1, d.nz);
+            const IDX zb = (IDX)(z0 > 0 ? z0 - 1 : 0) * plane, zq = (IDX)(z0 + 1 < nz ? z0 + 1 : nz - 1) * plane;
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
-                if (st.ok[u]) {
-                    const RawT a = raw(zb * plane + st.off[u]), b = raw(z0 * plane + st.off[u]);
+                if (ok[u]) {
+                    const RawT a = raw(zb + off[u]), b = raw(zo + off[u]);
 #pragma unroll
                     for (int k = 0; k < NF; ++k) {
                         vm[u][k] = val(a, k);
                         vc[u][k] = val(b, k);
                     }
-                    rq[u] = raw(zq * plane + st.off[u]);
+                    rq[u] = raw(zq + off[u]);
                 } else {
 #pragma unroll
                     for (int k = 0; k < NF; ++k) vm[u][k] = vc[u][k] = 0.f;
@@ -107,20 +122,22 @@ __device__ __forceinline__ void hess_zwalk(const Dims& d, const W6& w, const Raw
                 }
             }
         }
-        for (int64_t z = z0; z < z1; ++z) {
+        for (int z = z0; z < z1; ++z) {
             float vp[2][NF];
-            const int64_t zq = clampi(z + 2, d.nz);
+            const IDX zi = zo;  // plane z
+            zo += plane;        // plane z + 1
+            const IDX zq = z + 2 < nz ? zo + plane : zo;  // clamp(z + 2)
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
 #pragma unroll
                 for (int k = 0; k < NF; ++k) vp[u][k] = val(rq[u], k);
-                if (st.ok[u] && z + 1 < z1) rq[u] = raw(zq * plane + st.off[u]);
-                if (st.ok[u]) {
+                if (ok[u] && z + 1 < z1) rq[u] = raw(zq + off[u]);
+                if (ok[u]) {
 #pragma unroll
                     for (int k = 0; k < NF; ++k) {
-                        sp[buf][k][st.q[u]] = vc[u][k];
-                        sh[buf][k][st.q[u]] = (vp[u][k] - vm[u][k]) / 2.f;
-                        sz[buf][k][st.q[u]] = d2v(vm[u][k], vc[u][k], vp[u][k]);
+                        sp[buf][k][q[u]] = vc[u][k];
+                        sh[buf][k][q[u]] = (vp[u][k] - vm[u][k]) / 2.f;
+                        sz[buf][k][q[u]] = d2v(vm[u][k], vc[u][k], vp[u][k]);
                     }
                 }
             }
@@ -141,7 +158,7 @@ __device__ __forceinline__ void hess_zwalk(const Dims& d, const W6& w, const Raw
                     const float dy_xm = (P[so - 1] - P[n - 1]) / 2.f;
                     h[k][5] = ((dy_xp - dy_xm) / 2.f) * w.w[5];
                 }
-                body(z * plane + ipl, h);
+                body(zi + ipl, h);
             }
             buf ^= 1;
 #pragma unroll
@@ -154,5 +171,8 @@ __device__ __forceinline__ void hess_zwalk(const Dims& d, const W6& w, const Raw
         }
     }
 }
+
+// Element offsets fit 32 bits when all six components of a Hessian do.
+inline bool offsets_fit_u32(const Dims& d) { return 6 * d.nz * d.ny * d.nx < (int64_t(1) << 32); }
 
 }  // namespace dk
