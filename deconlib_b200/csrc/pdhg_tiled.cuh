@@ -18,10 +18,14 @@
 //
 // The primal update (k_hess_primal_t: six staged y2 components, x and
 // A^T y1) keeps a one-plane register prefetch and static three-plane rings
-// (hess_adj_walk, shared with the standalone Hessian3D adjoint): two CTAs of
-// 116 registers per SM, which on the B200 measured faster than the pipelined
-// form (six deep rings cost occupancy and issue slots) and than 80- or
-// 64-register builds at three or four CTAs per SM.
+// (hess_adj_walk, shared with the standalone Hessian3D adjoint).  It is
+// bound by instruction issue, so the walk indexes with 32-bit element
+// offsets and sets everything per tile once: 64 registers, four CTAs per SM
+// (on the B200 92 us at 128x256x256 against 131 us for the same walk with
+// 64-bit indexing at 122 registers, and against 141-150 us for a form that
+// staged the operands by TMA through an mbarrier ring).  The pipelined
+// cp.async form measured slower too (six deep rings cost occupancy and
+// issue slots).
 //
 // ||H (x_new - x)||^2 (k_hess_dk_r) walks z in registers instead
 // (hess_zwalk): each thread keeps three planes of its halo positions and
